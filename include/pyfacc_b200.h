@@ -1,0 +1,179 @@
+/*
+ * pyfacc_b200.h -- C ABI of libpyfacc_b200.so, the B200 Hartree-Fock engine
+ * that stands in for PyFAcc-SCF's libscf.so.
+ *
+ * Plain C types only: host pointers unless a name says "_dev" (CUDA device
+ * memory of the device the call runs on), sizes in elements.  Matrices are
+ * nbf x nbf, row-major and symmetric.  Coordinates are in bohr, atom-major
+ * (x1 y1 z1 x2 ...), the memory order PyFAcc-SCF's Python driver hands over
+ * (src/python/helper_functions.py:110-111).
+ */
+#ifndef PYFACC_B200_H
+#define PYFACC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes returned by every int-returning entry point ---------- */
+#define PYFACC_OK                  0
+#define PYFACC_ERR_BASIS_NOT_FOUND 1  /* basis file missing                 */
+#define PYFACC_ERR_UNSUPPORTED_L   2  /* shell type other than S, P, SP     */
+#define PYFACC_ERR_NOT_CONVERGED   3  /* SCF hit max_iter                   */
+#define PYFACC_ERR_LINDEP          4  /* overlap matrix not positive        */
+#define PYFACC_ERR_CUDA            5  /* CUDA / cuBLAS / cuSOLVER failure   */
+#define PYFACC_ERR_TIMEOUT         6  /* a bounded device wait gave up      */
+#define PYFACC_ERR_INVALID         7  /* bad argument                       */
+#define PYFACC_ERR_ELEMENT         8  /* element without basis functions    */
+#define PYFACC_ERR_NO_DEVICE       9  /* no CUDA device                     */
+#define PYFACC_ERR_NOT_READY      10  /* call order (e.g. gradient before SCF) */
+
+/* ---- options ------------------------------------------------------------ */
+#define PYFACC_BOYS_ACCURATE             0 /* tabulated Taylor + asymptotic  */
+#define PYFACC_BOYS_REFERENCE_TRAPEZOID  1 /* boys.f90:9-43, used for V only */
+#define PYFACC_PRECISION_FP64            0
+#define PYFACC_PRECISION_MIXED           1 /* FP32 quartets below fp32_thresh */
+#define PYFACC_SCF_AUTO                  0 /* RHF if nalpha == nbeta          */
+#define PYFACC_SCF_RHF                   1
+#define PYFACC_SCF_UHF                   2
+
+typedef struct pyfacc_options {
+  double eps_energy;        /* |E_n - E_{n-1}| < eps_energy          (1e-10) */
+  double eps_diis;          /* max |X^T (FDS - SDF) X| < eps_diis     (1e-8)  */
+  double eps_density;       /* ||D_n - D_{n-1}||_F < eps_density; <=0 off (0) */
+  int max_iter;             /* (100)                                           */
+  int diis_size;            /* Pulay subspace; 0 = plain Roothaan     (8)     */
+  int scf_type;             /* PYFACC_SCF_*                           (AUTO)  */
+  int precision;            /* PYFACC_PRECISION_*                     (FP64)  */
+  int boys_mode;            /* PYFACC_BOYS_* for the V matrix         (ACCURATE) */
+  double schwarz_thresh;    /* skip quartets with Q_ab Q_cd D_max below (1e-12) */
+  double fp32_thresh;       /* mixed: Q_ab Q_cd below this run in FP32  (1e-5) */
+  int incremental;          /* build G[dP] and add; -1 = on for MIXED   (-1)  */
+  int rebuild_every;        /* full rebuild period of incremental builds (12) */
+  int compute_gradient;     /* fill result->gradient after the SCF      (0)   */
+  int device;               /* CUDA ordinal; -1 = current device        (-1)  */
+  int verbose;              /* iteration lines on stderr                (0)   */
+  int shard_rank;           /* J/K work shard of this process           (0)   */
+  int shard_count;          /* number of shards (1 = whole Fock build)  (1)   */
+  const char *data_dir;     /* directory holding basis_set/; NULL = search    */
+} pyfacc_options;
+
+typedef struct pyfacc_molecule {
+  int natoms;
+  const int32_t *z;         /* atomic numbers [natoms]                        */
+  const double *coords;     /* bohr, atom-major [natoms*3]                    */
+  const char *species;      /* 2*natoms chars, space padded, not NUL-terminated;
+                               NULL = derive the symbols from z              */
+  int charge;
+  int nalpha, nbeta;        /* < 0: derived as helper_functions.py:76-87     */
+  const char *basis;        /* "sto-2g" ... "sto-6g", NUL-terminated         */
+} pyfacc_molecule;
+
+typedef struct pyfacc_result {
+  double energy;            /* total energy, hartree                          */
+  double e_elec, e_nuc;
+  int converged, n_iter, scf_type, nbf, nshell, n_fock_builds;
+  double last_delta_e, last_diis_error;
+  /* caller-owned outputs, filled when non-NULL (host memory)                */
+  double *gradient;         /* [natoms*3], needs compute_gradient            */
+  double *S, *T, *V;        /* [nbf*nbf]                                     */
+  double *P;                /* total density [nbf*nbf]                       */
+  double *C_alpha, *C_beta; /* MO coefficients, column i = orbital i         */
+  double *eps_alpha, *eps_beta; /* orbital energies [nbf]                    */
+  /* statistics                                                              */
+  double ms_total, ms_one_electron, ms_fock, ms_diag, ms_gradient;
+  long long quartets_fp64, quartets_fp32;   /* contracted quartets evaluated */
+  double flops_fock;        /* algorithmic flops of all Fock builds           */
+  double flops_gradient;    /* algorithmic flops of the two-electron gradient */
+} pyfacc_result;
+
+typedef struct pyfacc_system pyfacc_system;   /* opaque, one molecule on one GPU */
+
+/* ---- drop-in entry points of PyFAcc-SCF --------------------------------- */
+
+/* src/c/scf_interface.c:9-14.  Same arguments and meaning; species is
+ * 2*natoms space-padded chars, coords atom-major bohr, basis_set_c a
+ * NUL-terminated name resolved as ./data/basis_set/<name>.txt (main.f90:33).
+ * void like the original: on failure *final_energy is NaN and the status is
+ * kept for pyfacc_last_status(). */
+void run_scf_c(int natoms, int nelectrons, int charge, int nalpha, int nbeta, const char *species,
+               double *coords, double eps_scf, int max_iter, double *final_energy,
+               const char *basis_set_c, int32_t *z_num);
+
+/* src/fortran/main.f90:15-24 (bind(C) name run_scf_interface_py): the
+ * all-by-reference form with an explicit basis-name length. */
+void run_scf_interface_py(int32_t *natoms, int32_t *nelectrons, int32_t *charge, int32_t *nalpha,
+                          int32_t *nbeta, const char *species, double *coords, double *eps_scf,
+                          int32_t *max_iter, double *final_energy, const char *basis_set_c,
+                          int32_t *len_basis_set, int32_t *z_num);
+
+/* Status of the last run_scf_c / run_scf_interface_py call on this thread
+ * (the originals return nothing; la.f90:22-25 only prints). */
+int pyfacc_last_status(void);
+const char *pyfacc_status_string(int status);
+/* Text of the most recent failure on this thread (extension). */
+const char *pyfacc_last_message(void);
+
+/* ---- extended API (no counterpart in the reference) --------------------- */
+
+void pyfacc_default_options(pyfacc_options *opt);
+
+/* One molecule: SCF (RHF/UHF per scf_type) and optionally the analytic
+ * nuclear gradient (rscf.f90:26-168 / uscf.f90:25-219 plus gradient). */
+int pyfacc_run(const pyfacc_molecule *mol, const pyfacc_options *opt, pyfacc_result *res);
+
+/* Many molecules of uneven size converged together on one GPU: batched J/K
+ * launches over all molecules' shell quartets and a batched eigensolver. */
+int pyfacc_run_batch(int nmol, const pyfacc_molecule *mols, const pyfacc_options *opt,
+                     pyfacc_result *res);
+
+/* Handle API: basis, shell pairs and Schwarz factors stay resident on the
+ * GPU between calls. */
+int pyfacc_system_create(const pyfacc_molecule *mol, const pyfacc_options *opt, pyfacc_system **sys);
+void pyfacc_system_destroy(pyfacc_system *sys);
+int pyfacc_system_info(const pyfacc_system *sys, int *nbf, int *nshell, int *natoms, int *npairs);
+/* Replace the coordinates (same atoms); pair data is rebuilt. */
+int pyfacc_system_set_coords(pyfacc_system *sys, const double *coords);
+/* S, T, V into device buffers (nbf*nbf each; any may be NULL). */
+int pyfacc_system_one_electron(pyfacc_system *sys, double *S_dev, double *T_dev, double *V_dev);
+/* J[D_j] and K[D_k] for nk in {1,2} exchange densities: J_dev = sum (mn|ls) Dj_ls,
+ * K_dev[k] = sum (ml|ns) Dk[k]_ls.  precision: PYFACC_PRECISION_*.
+ * Schwarz screening uses the density: Q_ab Q_cd max|D| < schwarz_thresh. */
+int pyfacc_system_jk(pyfacc_system *sys, const double *Dj_dev, int nk, const double *Dk_dev,
+                     double *J_dev, double *K_dev, int precision);
+/* Full (nbf^4) ERI tensor on the device, small systems only (tests). */
+int pyfacc_system_eri_tensor(pyfacc_system *sys, double *eri_dev);
+/* SCF with the system's options; res as in pyfacc_run. */
+int pyfacc_system_scf(pyfacc_system *sys, pyfacc_result *res);
+/* Analytic gradient [natoms*3] (host) of the last converged SCF. */
+int pyfacc_system_gradient(pyfacc_system *sys, double *grad);
+/* Result of the last SCF (and gradient) on this system: energies, timings,
+ * statistics and the requested output matrices, without recomputing. */
+int pyfacc_system_result(pyfacc_system *sys, pyfacc_result *res);
+/* Device pointer to the density of the last SCF (nbf*nbf; RHF total,
+ * UHF alpha). */
+int pyfacc_system_density_dev(pyfacc_system *sys, const double **P_dev);
+/* Number of kernel launches this library has issued in this process. */
+long long pyfacc_launch_count(void);
+
+#define PYFACC_BOYS_MMAX 6
+/* Boys function F_m(x), m = 0..mmax (mmax <= PYFACC_BOYS_MMAX), for n arguments (device buffers;
+ * out_dev[i*(mmax+1)+m]).  mode: PYFACC_BOYS_*; fp32 != 0 uses the
+ * single-precision path of mixed mode. */
+int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double *x_dev, double *out_dev);
+
+/* Cost-balanced split of n weighted work items into `parts` contiguous
+ * ranges: bounds[0..parts] (host only, no GPU needed). */
+int pyfacc_partition(int n, const double *cost, int parts, int *bounds);
+
+/* Sustained FP64 FMA rate of the current device, GFLOP/s (microbenchmark). */
+double pyfacc_probe_fp64_gflops(int device, double *fp32_gflops);
+
+const char *pyfacc_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PYFACC_B200_H */

@@ -803,7 +803,7 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
     }
   // two-electron term over canonical shell quartets
   std::vector<double> Q((size_t)ns * (ns + 1) / 2);
-  orc_schwarz(ns, l, atom, cen, poff, ex, co, boys_mode, Q.data());
+  orc_schwarz(ns, l, atom, cen, poff, ex, co, 0, Q.data());
   const int npair = ns * (ns + 1) / 2;
   std::vector<int> pa(npair), pb(npair);
   for (int a = 0, k = 0; a < ns; ++a)
@@ -847,11 +847,12 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
                   int lu[4] = {ls[0], ls[1], ls[2], ls[3]}, ld_[4] = {ls[0], ls[1], ls[2], ls[3]};
                   lu[ctr] += 1;
                   ld_[ctr] -= 1;
+                  // ERIs always use the exact F_m (deviation D2); boys_mode is for V
                   prim_class(lu[0], lu[1], lu[2], lu[3], e4[0], e4[1], e4[2], e4[3], cen + 3 * a, cen + 3 * b,
-                             cen + 3 * c, cen + 3 * d, boys_mode, up);
+                             cen + 3 * c, cen + 3 * d, 0, up);
                   if (ls[ctr] > 0)
                     prim_class(ld_[0], ld_[1], ld_[2], ld_[3], e4[0], e4[1], e4[2], e4[3], cen + 3 * a,
-                               cen + 3 * b, cen + 3 * c, cen + 3 * d, boys_mode, dn);
+                               cen + 3 * b, cen + 3 * c, cen + 3 * d, 0, dn);
                   const int nu4[4] = {ncart(lu[0]), ncart(lu[1]), ncart(lu[2]), ncart(lu[3])};
                   const int nd4[4] = {ncart(std::max(ld_[0], 0)), ncart(std::max(ld_[1], 0)),
                                       ncart(std::max(ld_[2], 0)), ncart(std::max(ld_[3], 0))};

@@ -280,7 +280,8 @@ def schwarz(mol: Molecule, boys_mode=0):
 
 
 def jk(mol: Molecule, dens, thresh=1e-12, boys_mode=0):
-    """J[d], K[d] for a stack of densities (nd, nbf, nbf)."""
+    """J[d], K[d] for a stack of densities (nd, nbf, nbf).  The SCF always
+    uses the exact Boys function for ERIs (deviation D2)."""
     D = np.ascontiguousarray(np.asarray(dens, dtype=np.float64))
     single = D.ndim == 2
     if single:
@@ -358,12 +359,12 @@ def scf(mol: Molecule, e_tol=1e-10, d_tol=1e-8, max_iter=200, diis_size=8, boys_
     for it in range(1, max_iter + 1):
         Pt = Ds[0] + Ds[1]
         if uhf:
-            J, K = jk(mol, np.stack(Ds), thresh, boys_mode)
+            J, K = jk(mol, np.stack(Ds), thresh)
             Jt = J[0] + J[1]
             Fs = [H + Jt - K[0], H + Jt - K[1]]
             E = 0.5 * (np.sum(Pt * H) + np.sum(Ds[0] * Fs[0]) + np.sum(Ds[1] * Fs[1]))
         else:
-            J, K = jk(mol, Pt, thresh, boys_mode)
+            J, K = jk(mol, Pt, thresh)
             Fs = [H + J - 0.5 * K]
             E = 0.5 * np.sum(Pt * (H + Fs[0]))
         errs = []

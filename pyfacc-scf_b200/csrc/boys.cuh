@@ -1,0 +1,132 @@
+// Boys function F_m(T) = int_0^1 t^(2m) exp(-T t^2) dt on the device.
+//
+// Accurate mode (default): for T < 36, an 8-term Taylor expansion of F_mmax
+// about the nearest point of a 0.1-spaced grid (|dT| <= 0.05, remainder
+// < 1e-16 relative), then the stable downward recursion
+//   F_m = (2T F_{m+1} + exp(-T)) / (2m+1);
+// for T >= 36, F_0 = sqrt(pi/T)/2 (erfc(6) ~ 2e-17) and the upward recursion
+//   F_{m+1} = ((2m+1) F_m - exp(-T)) / (2T),
+// which is stable for T > m.  The grid values are computed once on the host
+// in long double from the positive series (ensure_boys_tables, kernels.cu).
+// FP32 mode (mixed precision) uses the same grid in float with 5 Taylor terms.
+//
+// Reference mode: boys.f90:9-43 of PyFAcc-SCF -- Taylor 1/(2m+1) - x/(2m+3)
+// for x <= 1e-6, else the 1001-point trapezoid rule on [0,1].  It is used for
+// the nuclear-attraction matrix only, so that V reproduces the reference.
+#pragma once
+#include <cuda_runtime.h>
+
+#define PF_BOYS_NGRID 361
+#define PF_BOYS_STEP 0.1
+#define PF_BOYS_INV_STEP 10.0
+#define PF_BOYS_TMAX 36.0
+#define PF_BOYS_MMAX 6       // highest order needed: (pp|pp) gradient = 5
+#define PF_BOYS_NT 8         // Taylor terms, FP64
+#define PF_BOYS_NTF 5        // Taylor terms, FP32
+#define PF_BOYS_NCOL (PF_BOYS_MMAX + PF_BOYS_NT)
+
+namespace pyfacc {
+
+// Grid tables (this header is included by exactly one translation unit,
+// kernels.cu, which fills them per device with cudaMemcpyToSymbol).
+__device__ double g_boys_tab[PF_BOYS_NGRID * PF_BOYS_NCOL];
+__device__ float g_boys_tabf[PF_BOYS_NGRID * PF_BOYS_NCOL];
+
+template <int L>
+__device__ __forceinline__ void boys_fp64(double T, double* __restrict__ F) {
+  if (T < PF_BOYS_TMAX) {
+    const int k = __double2int_rn(T * PF_BOYS_INV_STEP);
+    const double x = k * PF_BOYS_STEP - T;  // F_m(T) = sum_j F_{m+j}(T_k) x^j / j!
+    const double* row = g_boys_tab + k * PF_BOYS_NCOL + L;
+    double f = __ldg(row + PF_BOYS_NT - 1);
+#pragma unroll
+    for (int j = PF_BOYS_NT - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0 / (j + 1));
+    F[L] = f;
+    if (L > 0) {
+      const double e = exp(-T);
+      const double t2 = 2.0 * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
+    }
+  } else {
+    const double rt = rsqrt(T);
+    F[0] = 0.88622692545275801365 * rt;  // sqrt(pi)/2
+    if (L > 0) {
+      const double e = exp(-T);
+      const double o2t = 0.5 * rt * rt;
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * o2t;
+    }
+  }
+}
+
+template <int L>
+__device__ __forceinline__ void boys_fp32(float T, float* __restrict__ F) {
+  if (T < (float)PF_BOYS_TMAX) {
+    const int k = __float2int_rn(T * (float)PF_BOYS_INV_STEP);
+    const float x = k * (float)PF_BOYS_STEP - T;
+    const float* row = g_boys_tabf + k * PF_BOYS_NCOL + L;
+    float f = __ldg(row + PF_BOYS_NTF - 1);
+#pragma unroll
+    for (int j = PF_BOYS_NTF - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0f / (j + 1));
+    F[L] = f;
+    if (L > 0) {
+      const float e = expf(-T);
+      const float t2 = 2.0f * T;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
+    }
+  } else {
+    const float rt = rsqrtf(T);
+    F[0] = 0.88622692545275801365f * rt;
+    if (L > 0) {
+      const float e = expf(-T);
+      const float o2t = 0.5f * rt * rt;
+#pragma unroll
+      for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * o2t;
+    }
+  }
+}
+
+template <int L, typename R> struct Boys;
+template <int L> struct Boys<L, double> {
+  __device__ static __forceinline__ void eval(double T, double* F) { boys_fp64<L>(T, F); }
+};
+template <int L> struct Boys<L, float> {
+  __device__ static __forceinline__ void eval(float T, float* F) { boys_fp32<L>(T, F); }
+};
+
+// boys.f90:9-43, literally: small-x Taylor, else 1001-point trapezoid.
+__device__ __forceinline__ double boys_trapezoid(int nu, double x) {
+  if (x <= 1.0e-6) return 1.0 / (2.0 * nu + 1.0) - x / (2.0 * nu + 3.0);
+  const int N = 1000;
+  const double dt = 1.0 / N;
+  double sum = 0.0;
+  for (int i = 0; i <= N; ++i) {
+    const double t = i * dt;
+    const double e = exp(-x * t * t);
+    double tp = 1.0;
+    for (int k = 0; k < 2 * nu; ++k) tp *= t;
+    sum += (i == 0 || i == N) ? 0.5 * tp * e : tp * e;
+  }
+  return sum * dt;
+}
+
+// F_0..F_lmax with a runtime order bound (one-electron kernels).
+__device__ __forceinline__ void boys_runtime(int mode, int lmax, double T, double* F) {
+  if (mode == 1) {
+    for (int m = 0; m <= lmax; ++m) F[m] = boys_trapezoid(m, T);
+    return;
+  }
+  switch (lmax) {
+    case 0: boys_fp64<0>(T, F); break;
+    case 1: boys_fp64<1>(T, F); break;
+    case 2: boys_fp64<2>(T, F); break;
+    case 3: boys_fp64<3>(T, F); break;
+    case 4: boys_fp64<4>(T, F); break;
+    case 5: boys_fp64<5>(T, F); break;
+    default: boys_fp64<6>(T, F); break;
+  }
+}
+
+}  // namespace pyfacc

@@ -1,0 +1,308 @@
+// C ABI of libpyfacc_b200.so (declared in include/pyfacc_b200.h).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+
+#include "engine.h"
+#include "system.h"
+
+using pyfacc::Error;
+using pyfacc::System;
+
+namespace {
+
+thread_local int g_last_status = PYFACC_OK;
+thread_local std::string g_last_message;
+
+template <typename Fn>
+int guarded(Fn&& fn) {
+  try {
+    fn();
+    return PYFACC_OK;
+  } catch (const Error& e) {
+    g_last_message = e.what();
+    if (std::getenv("PYFACC_VERBOSE")) std::fprintf(stderr, "pyfacc: %s\n", e.what());
+    return e.status;
+  } catch (const std::exception& e) {
+    g_last_message = e.what();
+    if (std::getenv("PYFACC_VERBOSE")) std::fprintf(stderr, "pyfacc: %s\n", e.what());
+    return PYFACC_ERR_INVALID;
+  }
+}
+
+int run_one(const pyfacc_molecule& m, const pyfacc_options& o, pyfacc_result* r) {
+  std::unique_ptr<System> sys(new System(m, o));
+  sys->run_scf();
+  if (o.compute_gradient) sys->gradient(nullptr);
+  if (r) sys->fill_result(r);
+  return sys->st.converged ? PYFACC_OK : PYFACC_ERR_NOT_CONVERGED;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* pyfacc_version(void) { return "pyfacc-b200 0.1 (sm_100a)"; }
+
+const char* pyfacc_status_string(int s) {
+  switch (s) {
+    case PYFACC_OK: return "ok";
+    case PYFACC_ERR_BASIS_NOT_FOUND: return "basis set file not found";
+    case PYFACC_ERR_UNSUPPORTED_L: return "unsupported shell type (s and p only)";
+    case PYFACC_ERR_NOT_CONVERGED: return "SCF not converged";
+    case PYFACC_ERR_LINDEP: return "overlap matrix not positive definite";
+    case PYFACC_ERR_CUDA: return "CUDA error";
+    case PYFACC_ERR_TIMEOUT: return "device wait timed out";
+    case PYFACC_ERR_INVALID: return "invalid argument";
+    case PYFACC_ERR_ELEMENT: return "element without basis functions";
+    case PYFACC_ERR_NO_DEVICE: return "no CUDA device";
+    case PYFACC_ERR_NOT_READY: return "call order: run the SCF first";
+    default: return "unknown status";
+  }
+}
+
+int pyfacc_last_status(void) { return g_last_status; }
+
+// Detail text of the most recent failure on this thread (extension).
+const char* pyfacc_last_message(void) { return g_last_message.c_str(); }
+
+void pyfacc_default_options(pyfacc_options* o) {
+  if (!o) return;
+  std::memset(o, 0, sizeof(*o));
+  o->eps_energy = 1e-10;
+  o->eps_diis = 1e-8;
+  o->eps_density = 0.0;
+  o->max_iter = 100;
+  o->diis_size = 8;
+  o->scf_type = PYFACC_SCF_AUTO;
+  o->precision = PYFACC_PRECISION_FP64;
+  o->boys_mode = PYFACC_BOYS_ACCURATE;
+  o->schwarz_thresh = 1e-12;
+  o->fp32_thresh = 1e-5;
+  o->incremental = -1;
+  o->rebuild_every = 12;
+  o->compute_gradient = 0;
+  o->device = -1;
+  o->verbose = 0;
+  o->shard_rank = 0;
+  o->shard_count = 1;
+  o->data_dir = nullptr;
+}
+
+// scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.
+// The Fortran side stops at max_iter and returns the last energy (rscf.f90:
+// 118-164); this engine does the same with DIIS, converging on |dE| < eps_scf
+// and ||D - D_old||_F < eps_scf as rscf.f90:152-155 does.
+void run_scf_c(int natoms, int nelectrons, int charge, int nalpha, int nbeta, const char* species, double* coords,
+               double eps_scf, int max_iter, double* final_energy, const char* basis_set_c, int32_t* z_num) {
+  (void)nelectrons;
+  pyfacc_molecule m;
+  m.natoms = natoms;
+  m.z = z_num;
+  m.coords = coords;
+  m.species = species;
+  m.charge = charge;
+  m.nalpha = nalpha;
+  m.nbeta = nbeta;
+  m.basis = basis_set_c;
+  pyfacc_options o;
+  pyfacc_default_options(&o);
+  o.eps_energy = eps_scf;
+  o.eps_density = eps_scf;
+  o.eps_diis = 1e300;  // the reference criterion is |dE| and ||dD|| only
+  o.max_iter = max_iter;
+  pyfacc_result r;
+  std::memset(&r, 0, sizeof(r));
+  int status = PYFACC_OK;
+  const int st = guarded([&] { status = run_one(m, o, &r); });
+  if (st != PYFACC_OK) status = st;
+  g_last_status = status;
+  if (final_energy) {
+    // like the reference, a run that hit max_iter still returns its energy
+    if (status == PYFACC_OK || status == PYFACC_ERR_NOT_CONVERGED) *final_energy = r.energy;
+    else *final_energy = std::numeric_limits<double>::quiet_NaN();
+  }
+}
+
+// main.f90:15-24, the bind(C) all-by-reference entry point.
+void run_scf_interface_py(int32_t* natoms, int32_t* nelectrons, int32_t* charge, int32_t* nalpha, int32_t* nbeta,
+                          const char* species, double* coords, double* eps_scf, int32_t* max_iter,
+                          double* final_energy, const char* basis_set_c, int32_t* len_basis_set, int32_t* z_num) {
+  std::string basis(basis_set_c, basis_set_c + (len_basis_set ? *len_basis_set : std::strlen(basis_set_c)));
+  while (!basis.empty() && basis.back() == ' ') basis.pop_back();
+  run_scf_c(*natoms, *nelectrons, *charge, *nalpha, *nbeta, species, coords, *eps_scf, *max_iter, final_energy,
+            basis.c_str(), z_num);
+}
+
+int pyfacc_run(const pyfacc_molecule* mol, const pyfacc_options* opt, pyfacc_result* res) {
+  if (!mol) return PYFACC_ERR_INVALID;
+  pyfacc_options o;
+  if (opt) o = *opt; else pyfacc_default_options(&o);
+  int status = PYFACC_OK;
+  const int st = guarded([&] { status = run_one(*mol, o, res); });
+  return st != PYFACC_OK ? st : status;
+}
+
+// Molecules one after another on the current GPU (the batched engine
+// replaces this loop; statuses are per molecule, the return value the worst).
+int pyfacc_run_batch(int nmol, const pyfacc_molecule* mols, const pyfacc_options* opt, pyfacc_result* res) {
+  if (nmol < 0 || (nmol > 0 && !mols)) return PYFACC_ERR_INVALID;
+  int worst = PYFACC_OK;
+  for (int i = 0; i < nmol; ++i) {
+    const int s = pyfacc_run(&mols[i], opt, res ? &res[i] : nullptr);
+    if (s != PYFACC_OK && (worst == PYFACC_OK || worst == PYFACC_ERR_NOT_CONVERGED)) worst = s;
+  }
+  return worst;
+}
+
+int pyfacc_system_create(const pyfacc_molecule* mol, const pyfacc_options* opt, pyfacc_system** out) {
+  if (!mol || !out) return PYFACC_ERR_INVALID;
+  *out = nullptr;
+  pyfacc_options o;
+  if (opt) o = *opt; else pyfacc_default_options(&o);
+  return guarded([&] {
+    std::unique_ptr<System> s(new System(*mol, o));
+    *out = new pyfacc_system{s.release()};
+  });
+}
+
+void pyfacc_system_destroy(pyfacc_system* sys) {
+  if (!sys) return;
+  delete sys->impl;
+  delete sys;
+}
+
+int pyfacc_system_info(const pyfacc_system* sys, int* nbf, int* nshell, int* natoms, int* npairs) {
+  if (!sys) return PYFACC_ERR_INVALID;
+  if (nbf) *nbf = sys->impl->nbf;
+  if (nshell) *nshell = sys->impl->ns;
+  if (natoms) *natoms = sys->impl->natoms;
+  if (npairs) *npairs = sys->impl->pd.npair;
+  return PYFACC_OK;
+}
+
+int pyfacc_system_set_coords(pyfacc_system* sys, const double* coords) {
+  if (!sys || !coords) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    PF_CUDA(cudaSetDevice(sys->impl->device));
+    sys->impl->set_coords(coords);
+  });
+}
+
+int pyfacc_system_one_electron(pyfacc_system* sys, double* S_dev, double* T_dev, double* V_dev) {
+  if (!sys) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    System& s = *sys->impl;
+    PF_CUDA(cudaSetDevice(s.device));
+    s.one_electron();
+    const size_t b = (size_t)s.nbf * s.nbf * sizeof(double);
+    if (S_dev) PF_CUDA(cudaMemcpyAsync(S_dev, s.S, b, cudaMemcpyDeviceToDevice, s.stream));
+    if (T_dev) PF_CUDA(cudaMemcpyAsync(T_dev, s.T, b, cudaMemcpyDeviceToDevice, s.stream));
+    if (V_dev) PF_CUDA(cudaMemcpyAsync(V_dev, s.Vm, b, cudaMemcpyDeviceToDevice, s.stream));
+    PF_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int pyfacc_system_jk(pyfacc_system* sys, const double* Dj_dev, int nk, const double* Dk_dev, double* J_dev,
+                     double* K_dev, int precision) {
+  if (!sys || !Dj_dev || !Dk_dev || !J_dev || !K_dev || nk < 1 || nk > 2) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    System& s = *sys->impl;
+    PF_CUDA(cudaSetDevice(s.device));
+    const size_t n2 = (size_t)s.nbf * s.nbf;
+    const double* Dk[2] = {Dk_dev, Dk_dev + n2};
+    double* Ko[2] = {K_dev, K_dev + n2};
+    s.jk(Dj_dev, nk, Dk, J_dev, Ko, precision);
+    PF_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int pyfacc_system_eri_tensor(pyfacc_system* sys, double* eri_dev) {
+  if (!sys || !eri_dev) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    System& s = *sys->impl;
+    if (s.nbf > 64) throw Error(PYFACC_ERR_INVALID, "ERI tensor limited to nbf <= 64");
+    PF_CUDA(cudaSetDevice(s.device));
+    s.eri_tensor(eri_dev);
+    PF_CUDA(cudaStreamSynchronize(s.stream));
+  });
+}
+
+int pyfacc_system_scf(pyfacc_system* sys, pyfacc_result* res) {
+  if (!sys) return PYFACC_ERR_INVALID;
+  int status = PYFACC_OK;
+  const int st = guarded([&] {
+    System& s = *sys->impl;
+    PF_CUDA(cudaSetDevice(s.device));
+    s.run_scf();
+    if (s.opt.compute_gradient) s.gradient(nullptr);
+    if (res) s.fill_result(res);
+    status = s.st.converged ? PYFACC_OK : PYFACC_ERR_NOT_CONVERGED;
+  });
+  return st != PYFACC_OK ? st : status;
+}
+
+int pyfacc_system_gradient(pyfacc_system* sys, double* grad) {
+  if (!sys) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    System& s = *sys->impl;
+    PF_CUDA(cudaSetDevice(s.device));
+    s.gradient(grad);
+  });
+}
+
+int pyfacc_system_result(pyfacc_system* sys, pyfacc_result* res) {
+  if (!sys || !res) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    System& s = *sys->impl;
+    if (!s.st.done) throw Error(PYFACC_ERR_NOT_READY, "no SCF has run on this system");
+    PF_CUDA(cudaSetDevice(s.device));
+    s.fill_result(res);
+  });
+}
+
+long long pyfacc_launch_count(void) { return pyfacc::launch_count(); }
+
+int pyfacc_system_density_dev(pyfacc_system* sys, const double** P_dev) {
+  if (!sys || !P_dev) return PYFACC_ERR_INVALID;
+  *P_dev = sys->impl->P[0];
+  return PYFACC_OK;
+}
+
+int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double* x_dev, double* out_dev) {
+  if (mmax < 0 || mmax > PYFACC_BOYS_MMAX || n < 0 || (n > 0 && (!x_dev || !out_dev))) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    int dev = 0;
+    PF_CUDA(cudaGetDevice(&dev));
+    pyfacc::ensure_boys_tables(dev);
+    pyfacc::launch_boys_test(mode, fp32, mmax, n, x_dev, out_dev, 0);
+    PF_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+int pyfacc_partition(int n, const double* cost, int parts, int* bounds) {
+  if (n < 0 || parts < 1 || !bounds || (n > 0 && !cost)) return PYFACC_ERR_INVALID;
+  double total = 0.0;
+  for (int i = 0; i < n; ++i) total += cost[i] > 0 ? cost[i] : 0.0;
+  bounds[0] = 0;
+  double acc = 0.0;
+  int k = 1;
+  for (int i = 0; i < n && k < parts; ++i) {
+    acc += cost[i] > 0 ? cost[i] : 0.0;
+    // close part k-1 once its cumulative share is reached
+    while (k < parts && acc >= total * k / parts) bounds[k++] = i + 1;
+  }
+  while (k <= parts) bounds[k++] = n;
+  return PYFACC_OK;
+}
+
+double pyfacc_probe_fp64_gflops(int device, double* fp32_gflops) {
+  double r = -1.0;
+  guarded([&] { r = pyfacc::probe_fp64(device, fp32_gflops); });
+  return r;
+}
+
+}  // extern "C"

@@ -1,0 +1,438 @@
+// Host side of the B200 Hartree-Fock engine: one molecule on one GPU.
+//
+// SCF (rscf.f90:26-168 / uscf.f90:25-219 of PyFAcc-SCF, with the intended
+// semantics: every 8-fold ERI image, RHF/UHF dispatch on n_alpha == n_beta,
+// Pulay DIIS, convergence on |dE|, the DIIS commutator and optionally
+// ||dD||_F):
+//   S, T, V on the GPU; X = U s^-1/2 (la.f90:28-57, canonical, no
+//   eigenvalue dropping) from cuSOLVER once; core guess; then per iteration
+//   J/K digestion kernels (FP64, or mixed FP64/FP32 with incremental dP
+//   builds), F = H + J - K/2 (RHF) or H + J - K_s (UHF), energy and DIIS
+//   error reduced on the device, F' = X^T F X and C = X C' by cuBLAS DGEMM,
+//   eigenvectors by cuSOLVER DSYEVD, D = 2 C_occ C_occ^T (RHF).
+// Gradient: one- and two-electron derivative kernels contracted with P and
+// W = sum_occ eps_i c_i c_i^T on the device, nuclear repulsion on the host.
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+#include "engine.h"
+#include "system.h"
+
+namespace pyfacc {
+
+void DeviceBuf::ensure(size_t b) {
+  if (b <= bytes) return;
+  release();
+  PF_CUDA(cudaMalloc(&p, b));
+  bytes = b;
+}
+void DeviceBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+#define PF_CUBLAS(x)                                                                    \
+  do {                                                                                  \
+    cublasStatus_t s_ = (x);                                                            \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                                    \
+      throw Error(PYFACC_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); \
+  } while (0)
+#define PF_CUSOLVER(x)                                                                  \
+  do {                                                                                  \
+    cusolverStatus_t s_ = (x);                                                          \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                  \
+      throw Error(PYFACC_ERR_CUDA, std::string(#x) + ": cuSOLVER status " + std::to_string((int)s_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ setup
+System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
+  if (m.natoms <= 0 || !m.z || !m.coords || !m.basis) throw Error(PYFACC_ERR_INVALID, "empty molecule");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(PYFACC_ERR_NO_DEVICE, "no CUDA device");
+  if (opt.device >= 0) {
+    device = opt.device;
+    PF_CUDA(cudaSetDevice(device));
+  } else {
+    PF_CUDA(cudaGetDevice(&device));
+  }
+  cudaDeviceProp prop;
+  PF_CUDA(cudaGetDeviceProperties(&prop, device));
+  num_sms = prop.multiProcessorCount;
+  ensure_boys_tables(device);
+  PF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  PF_CUBLAS(cublasCreate(&cublas));
+  PF_CUBLAS(cublasSetStream(cublas, stream));
+  PF_CUSOLVER(cusolverDnCreate(&cusolver));
+  PF_CUSOLVER(cusolverDnSetStream(cusolver, stream));
+  PF_CUDA(cudaEventCreate(&ev0));
+  PF_CUDA(cudaEventCreate(&ev1));
+
+  natoms = m.natoms;
+  Z.assign(m.z, m.z + natoms);
+  xyz.assign(m.coords, m.coords + 3 * natoms);
+  species.resize(natoms);
+  for (int a = 0; a < natoms; ++a) {
+    if (m.species) {
+      std::string s(m.species + 2 * a, 2);
+      while (!s.empty() && (s.back() == ' ' || s.back() == '\0')) s.pop_back();
+      species[a] = s;
+    } else {
+      species[a] = element_symbol(Z[a]);
+    }
+    if (species[a].empty() || element_z(species[a]) == 0)
+      throw Error(PYFACC_ERR_ELEMENT, "unknown element at atom " + std::to_string(a));
+  }
+  charge = m.charge;
+  if (m.nalpha >= 0 && m.nbeta >= 0) {
+    nalpha = m.nalpha;
+    nbeta = m.nbeta;
+  } else {
+    spin_electrons(species, charge, &nalpha, &nbeta);
+  }
+  basis_name = m.basis;
+  basis_file = resolve_basis_file(basis_name, opt.data_dir);
+  basis = build_basis(basis_file, species, xyz);
+  nbf = basis.nbf;
+  ns = (int)basis.shells.size();
+  uhf = (opt.scf_type == PYFACC_SCF_UHF) || (opt.scf_type == PYFACC_SCF_AUTO && nalpha != nbeta);
+  e_nuc = nuclear_repulsion();
+  upload_shells();
+  build_pairs();
+  alloc_matrices();
+}
+
+System::~System() {
+  cudaSetDevice(device);
+  if (cublas) cublasDestroy(cublas);
+  if (cusolver) cusolverDnDestroy(cusolver);
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
+  release_extra();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// helper_functions.py:58-87: multiplicity 1 or 2, O2 -> 3, N2 -> 4.
+void System::spin_electrons(const std::vector<std::string>& sp, int chg, int* na, int* nb) {
+  int total = -chg;
+  for (auto& s : sp) total += element_z(s);
+  int mult = (total % 2 == 0) ? 1 : 2;
+  bool all_same = std::all_of(sp.begin(), sp.end(), [&](const std::string& s) { return s == sp[0]; });
+  if (all_same && sp.size() == 2 && sp[0] == "O") mult = 3;
+  if (all_same && sp.size() == 2 && sp[0] == "N") mult = 4;
+  const int twoS = mult - 1;
+  if ((total + twoS) % 2 != 0) throw Error(PYFACC_ERR_INVALID, "Inconsistent electron count and spin state.");
+  *na = (total + twoS) / 2;
+  *nb = total - *na;
+}
+
+// molecule.f90:31-52: sum_{i<j} Z_i Z_j / R_ij, pairs with R <= 1e-10 skipped.
+double System::nuclear_repulsion() const {
+  double e = 0.0;
+  for (int i = 0; i < natoms; ++i)
+    for (int j = i + 1; j < natoms; ++j) {
+      double d2 = 0;
+      for (int x = 0; x < 3; ++x) d2 += (xyz[3 * i + x] - xyz[3 * j + x]) * (xyz[3 * i + x] - xyz[3 * j + x]);
+      const double r = std::sqrt(d2);
+      if (r > 1.0e-10) e += (double)Z[i] * Z[j] / r;
+    }
+  return e;
+}
+
+void System::nuclear_repulsion_gradient(double* g) const {
+  for (int i = 0; i < natoms; ++i)
+    for (int j = 0; j < natoms; ++j) {
+      if (i == j) continue;
+      double d[3], r2 = 0;
+      for (int x = 0; x < 3; ++x) {
+        d[x] = xyz[3 * i + x] - xyz[3 * j + x];
+        r2 += d[x] * d[x];
+      }
+      const double r = std::sqrt(r2);
+      if (r <= 1.0e-10) continue;
+      for (int x = 0; x < 3; ++x) g[3 * i + x] -= (double)Z[i] * Z[j] * d[x] / (r2 * r);
+    }
+}
+
+void System::upload_shells() {
+  std::vector<double4> cen(ns);
+  std::vector<int4> desc(ns);
+  std::vector<int> np(ns), nf(ns);
+  std::vector<double> ex, co;
+  std::vector<int> bfo(ns + 1);
+  for (int s = 0; s < ns; ++s) {
+    const Shell& sh = basis.shells[s];
+    cen[s] = make_double4(sh.c[0], sh.c[1], sh.c[2], 0.0);
+    desc[s] = make_int4(sh.l, sh.atom, basis.bf_off[s], (int)ex.size());
+    np[s] = (int)sh.ex.size();
+    nf[s] = (sh.l + 1) * (sh.l + 2) / 2;
+    ex.insert(ex.end(), sh.ex.begin(), sh.ex.end());
+    co.insert(co.end(), sh.co.begin(), sh.co.end());
+    bfo[s] = basis.bf_off[s];
+  }
+  bfo[ns] = nbf;
+  std::vector<double4> atoms(natoms);
+  for (int a = 0; a < natoms; ++a) atoms[a] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], (double)Z[a]);
+  // 1e pair list: (a, b) with a <= b, the upper triangle of S_overlap (overlap.f90:292-329)
+  std::vector<int2> p1;
+  for (int a = 0; a < ns; ++a)
+    for (int b = a; b < ns; ++b) p1.push_back(make_int2(a, b));
+  n1e = (int)p1.size();
+  const size_t nex = std::max<size_t>(ex.size(), 1);
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_cen = carve(ns * sizeof(double4)), o_desc = carve(ns * sizeof(int4)), o_np = carve(ns * sizeof(int)),
+               o_ex = carve(nex * sizeof(double)), o_co = carve(nex * sizeof(double)),
+               o_atoms = carve(natoms * sizeof(double4)), o_p1 = carve(n1e * sizeof(int2)),
+               o_bfo = carve((ns + 1) * sizeof(int)), o_nf = carve(ns * sizeof(int));
+  shd.buf.ensure(off);
+  char* base = shd.buf.as<char>();
+  shd.ns = ns;
+  shd.cen = reinterpret_cast<double4*>(base + o_cen);
+  shd.desc = reinterpret_cast<int4*>(base + o_desc);
+  shd.nprim = reinterpret_cast<int*>(base + o_np);
+  shd.ex = reinterpret_cast<double*>(base + o_ex);
+  shd.co = reinterpret_cast<double*>(base + o_co);
+  atoms_dev = reinterpret_cast<double4*>(base + o_atoms);
+  pairs1e = reinterpret_cast<int2*>(base + o_p1);
+  bf_off_dev = reinterpret_cast<int*>(base + o_bfo);
+  nfun_dev = reinterpret_cast<int*>(base + o_nf);
+  PF_CUDA(cudaMemcpyAsync(shd.cen, cen.data(), ns * sizeof(double4), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(shd.desc, desc.data(), ns * sizeof(int4), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(shd.nprim, np.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(shd.ex, ex.data(), ex.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(shd.co, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(atoms_dev, atoms.data(), natoms * sizeof(double4), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(pairs1e, p1.data(), n1e * sizeof(int2), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(bf_off_dev, bfo.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(nfun_dev, nf.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Canonical shell pairs grouped by class, Schwarz factors on the GPU, then
+// sorted by Q (descending) inside each class; pairs that cannot reach the
+// threshold against the largest Q are dropped.  Task lists per class pair.
+void System::build_pairs() {
+  std::vector<int4> pl0[NCLASS];
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j <= i; ++j) {
+      int a = i, b = j;
+      if (basis.shells[a].l < basis.shells[b].l) std::swap(a, b);
+      const int c = basis.shells[a].l + basis.shells[b].l;
+      pl0[c].push_back(make_int4(a, b, 0, 0));
+    }
+  std::vector<int4> all0, all1;
+  int off[NCLASS + 1] = {0, 0, 0, 0};
+  int nprim_tot = 0;
+  for (int c = 0; c < NCLASS; ++c) {
+    off[c + 1] = off[c] + (int)pl0[c].size();
+    for (auto p : pl0[c]) {
+      p.z = nprim_tot;
+      nprim_tot += (int)(basis.shells[p.x].ex.size() * basis.shells[p.y].ex.size());
+      all0.push_back(p);
+      all1.push_back(make_int4(0, nbf, 0, 0));
+    }
+  }
+  const int np_all = off[NCLASS];
+  // scratch: unsorted records
+  size_t o = 0;
+  auto carve = [&](size_t bytes) {
+    size_t r = o;
+    o += (bytes + 255) / 256 * 256;
+    return r;
+  };
+  const size_t s_pl0 = carve(np_all * sizeof(int4)), s_pl1 = carve(np_all * sizeof(int4)),
+               s_i0 = carve(np_all * sizeof(int4)), s_i1 = carve(np_all * sizeof(int4)),
+               s_i2 = carve(np_all * sizeof(int4)), s_g = carve(np_all * sizeof(double4)),
+               s_pr = carve((size_t)std::max(nprim_tot, 1) * 3 * sizeof(double4)), s_q = carve(np_all * sizeof(double)),
+               s_perm = carve(np_all * sizeof(int)), s_ps = carve(np_all * sizeof(int));
+  DeviceBuf scratch;
+  scratch.ensure(o);
+  char* sb = scratch.as<char>();
+  int4* d_pl0 = reinterpret_cast<int4*>(sb + s_pl0);
+  int4* d_pl1 = reinterpret_cast<int4*>(sb + s_pl1);
+  PairData tmp;
+  tmp.info0 = reinterpret_cast<int4*>(sb + s_i0);
+  tmp.info1 = reinterpret_cast<int4*>(sb + s_i1);
+  tmp.info2 = reinterpret_cast<int4*>(sb + s_i2);
+  tmp.geom = reinterpret_cast<double4*>(sb + s_g);
+  tmp.prim = reinterpret_cast<double4*>(sb + s_pr);
+  double* d_q = reinterpret_cast<double*>(sb + s_q);
+  int* d_perm = reinterpret_cast<int*>(sb + s_perm);
+  int* d_ps = reinterpret_cast<int*>(sb + s_ps);
+  PF_CUDA(cudaMemcpyAsync(d_pl0, all0.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(d_pl1, all1.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
+  launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, stream);
+  launch_schwarz(tmp, off, d_q, stream);
+  std::vector<double> q(np_all);
+  PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  const double qmax = np_all ? *std::max_element(q.begin(), q.end()) : 0.0;
+  const double thr = opt.schwarz_thresh;
+  std::vector<int> perm, new_ps;
+  pd.class_off[0] = 0;
+  int nprim_new = 0;
+  pd.q_host.clear();
+  pd.cls_host.clear();
+  for (int c = 0; c < NCLASS; ++c) {
+    std::vector<int> idx;
+    for (int k = off[c]; k < off[c + 1]; ++k)
+      if (thr <= 0 || q[k] * qmax >= thr) idx.push_back(k);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return q[x] > q[y]; });
+    for (int k : idx) {
+      perm.push_back(k);
+      new_ps.push_back(nprim_new);
+      nprim_new += (int)(basis.shells[all0[k].x].ex.size() * basis.shells[all0[k].y].ex.size());
+      pd.q_host.push_back(q[k]);
+      pd.cls_host.push_back(c);
+    }
+    pd.class_off[c + 1] = (int)perm.size();
+  }
+  pd.npair = (int)perm.size();
+  pd.nprim = nprim_new;
+  // final records
+  o = 0;
+  const size_t f_i0 = carve(pd.npair * sizeof(int4)), f_i1 = carve(pd.npair * sizeof(int4)),
+               f_i2 = carve(pd.npair * sizeof(int4)), f_g = carve(pd.npair * sizeof(double4)),
+               f_pr = carve((size_t)std::max(nprim_new, 1) * 3 * sizeof(double4));
+  pd.buf.ensure(std::max<size_t>(o, 256));
+  char* pb = pd.buf.as<char>();
+  pd.info0 = reinterpret_cast<int4*>(pb + f_i0);
+  pd.info1 = reinterpret_cast<int4*>(pb + f_i1);
+  pd.info2 = reinterpret_cast<int4*>(pb + f_i2);
+  pd.geom = reinterpret_cast<double4*>(pb + f_g);
+  pd.prim = reinterpret_cast<double4*>(pb + f_pr);
+  if (pd.npair > 0) {
+    PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
+    PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
+    launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, pd.info0,
+                        pd.info1, pd.info2, pd.geom, nullptr, pd.prim, nullptr, stream);
+  }
+  PF_CUDA(cudaStreamSynchronize(stream));
+  build_tasks();
+}
+
+// Ket ranges per bra: kets are the pairs of the ket class, sorted by Q; a
+// bra reaches the prefix with Q_bra Q_ket >= thresh (and, in mixed mode, the
+// FP64 part is the prefix with Q_bra Q_ket >= fp32_thresh).  For equal
+// classes only kets up to the bra itself are canonical.
+void System::build_tasks() {
+  std::vector<int> hostbuf;
+  struct Pending { int bc, kc, prec; size_t off; int nbra; };
+  std::vector<Pending> pend;
+  const double thr = std::max(opt.schwarz_thresh, 0.0);
+  const double t32 = opt.fp32_thresh;
+  quartets_total = 0;
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
+      const int nk = pd.class_off[kc + 1] - pd.class_off[kc];
+      const double* qb = pd.q_host.data() + pd.class_off[bc];
+      const double* qk = pd.q_host.data() + pd.class_off[kc];
+      auto prefix = [&](double qbra, double t) {
+        if (t <= 0) return nk;
+        // number of kets with qbra * qk[j] >= t (qk descending)
+        int lo = 0, hi = nk;
+        while (lo < hi) {
+          int mid = (lo + hi) / 2;
+          if (qbra * qk[mid] >= t) lo = mid + 1; else hi = mid;
+        }
+        return lo;
+      };
+      for (int prec = 0; prec < 3; ++prec) {
+        Pending p{bc, kc, prec, hostbuf.size(), nb};
+        std::vector<int> toff(nb + 1), lo(nb), hi(nb);
+        long long quart = 0;
+        int ntask = 0;
+        for (int i = 0; i < nb; ++i) {
+          int m = prefix(qb[i], thr);
+          if (bc == kc) m = std::min(m, i + 1);
+          int m64 = std::min(prefix(qb[i], t32), m);
+          int l = 0, h = m;
+          if (prec == 1) h = m64;
+          if (prec == 2) l = m64;
+          lo[i] = l;
+          hi[i] = h;
+          toff[i] = ntask;
+          ntask += (h - l + TASK_WIDTH - 1) / TASK_WIDTH;
+          quart += h - l;
+        }
+        toff[nb] = ntask;
+        if (prec == 0) quartets_total += quart;
+        TaskList& tl = tasks[bc][kc][prec];
+        tl.nbra = nb;
+        tl.ntasks = ntask;
+        tl.nquartets = quart;
+        hostbuf.insert(hostbuf.end(), toff.begin(), toff.end());
+        hostbuf.insert(hostbuf.end(), lo.begin(), lo.end());
+        hostbuf.insert(hostbuf.end(), hi.begin(), hi.end());
+        pend.push_back(p);
+      }
+    }
+  task_buf.ensure(std::max<size_t>(hostbuf.size() * sizeof(int), 256));
+  int* d = task_buf.as<int>();
+  PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  for (auto& p : pend) {
+    TaskList& tl = tasks[p.bc][p.kc][p.prec];
+    tl.task_off = d + p.off;
+    tl.ket_lo = d + p.off + p.nbra + 1;
+    tl.ket_hi = d + p.off + 2 * p.nbra + 1;
+  }
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+void System::alloc_matrices() {
+  const size_t n2 = (size_t)nbf * nbf;
+  const int nmat = 24 + 4 * std::max(opt.diis_size, 1);
+  mats.ensure(nmat * n2 * sizeof(double) + 64 * sizeof(double) + ns * ns * sizeof(float) + 1024);
+  double* m = mats.as<double>();
+  auto take = [&]() { double* r = m; m += n2; return r; };
+  S = take(); T = take(); Vm = take(); H = take(); X = take();
+  F[0] = take(); F[1] = take(); J = take(); K[0] = take(); K[1] = take();
+  P[0] = take(); P[1] = take(); Pbuilt[0] = take(); Pbuilt[1] = take(); Pold[0] = take(); Pold[1] = take();
+  W1 = take(); W2 = take(); W3 = take(); Err[0] = take(); Err[1] = take(); Cm[0] = take(); Cm[1] = take();
+  Wm = take();
+  const int nd = std::max(opt.diis_size, 1);
+  for (int i = 0; i < nd; ++i) {
+    diis_F.push_back(m); m += 2 * n2;
+    diis_E.push_back(m); m += 2 * n2;
+  }
+  small = m; m += 64;
+  dmax = reinterpret_cast<float*>(m);
+  PF_CUDA(cudaMalloc(&eps_dev, 2 * nbf * sizeof(double)));
+  PF_CUDA(cudaMalloc(&info_dev, sizeof(int)));
+  PF_CUDA(cudaMalloc(&stats_dev, sizeof(JkStats)));
+  PF_CUDA(cudaMalloc(&ptrs_dev, 64 * sizeof(double*)));
+  PF_CUDA(cudaMalloc(&grad_dev, 3 * natoms * sizeof(double)));
+  int lwork = 0;
+  PF_CUSOLVER(cusolverDnDsyevd_bufferSize(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W1, nbf,
+                                          eps_dev, &lwork));
+  syev_work.ensure(std::max<size_t>((size_t)lwork * sizeof(double), 256));
+  syev_lwork = lwork;
+}
+
+void System::release_extra() {
+  if (eps_dev) cudaFree(eps_dev);
+  if (info_dev) cudaFree(info_dev);
+  if (stats_dev) cudaFree(stats_dev);
+  if (ptrs_dev) cudaFree(ptrs_dev);
+  if (grad_dev) cudaFree(grad_dev);
+  eps_dev = nullptr;
+  info_dev = nullptr;
+  stats_dev = nullptr;
+  ptrs_dev = nullptr;
+  grad_dev = nullptr;
+}
+
+}  // namespace pyfacc

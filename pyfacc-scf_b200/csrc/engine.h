@@ -1,0 +1,213 @@
+// Internal declarations of the B200 Hartree-Fock engine.
+//
+// Device data layout (one molecule, or a batch of molecules packed together):
+//  * shells       SoA: centre (double4), l, atom, bf offset, primitive range
+//  * shell pairs  canonical pairs (a, b) with l_a >= l_b, grouped by class
+//                 ss | ps | pp and sorted by Schwarz factor Q_ab (descending)
+//                 inside a class:  info0 = {bf_a, bf_b, prim_start, n_prim},
+//                 info1 = {shell_a, shell_b, atom_a, atom_b},
+//                 info2 = {matrix offset (lo, hi), ld, molecule},
+//                 geom = {A-B, Q_ab}
+//  * prim pairs   3 x double4 per primitive pair:
+//                 {p, 1/(2p), K, alpha}, {P, 0}, {P-A, 0} with
+//                 K = c_a c_b N_a N_b exp(-alpha beta/p |AB|^2) sqrt(2) pi^(5/4) / p
+//                 so that a primitive quartet prefactor is K_ab K_cd / sqrt(p+q);
+//                 a float copy serves the FP32 quartets of mixed precision.
+//  * tasks        per (bra class, ket class, precision): for bra pair i the
+//                 ket range [ket_lo[i], ket_hi[i]) in chunks of 32 (one warp,
+//                 one ket per lane); task_off is the exclusive prefix sum.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include "pyfacc_b200.h"
+
+namespace pyfacc {
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+#define PF_CUDA(x)                                                                          \
+  do {                                                                                      \
+    cudaError_t e_ = (x);                                                                   \
+    if (e_ != cudaSuccess)                                                                  \
+      throw ::pyfacc::Error(PYFACC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr int NCLASS = 3;        // ss, ps, pp
+constexpr int NQCLASS = 6;       // (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|pp)
+constexpr int TASK_WIDTH = 32;   // kets per task = lanes per warp
+
+// ---------------------------------------------------------------- host basis
+struct Shell {
+  int l = 0, atom = 0;
+  double c[3] = {0, 0, 0};
+  std::vector<double> ex, co;
+};
+
+struct Basis {
+  std::vector<Shell> shells;
+  std::vector<int> bf_off;  // nshell + 1
+  int nbf = 0;
+};
+
+// basis.cpp
+const char* element_symbol(int z);
+int element_z(const std::string& sym);
+std::string resolve_basis_file(const std::string& name, const char* data_dir);
+// Shells in the order of basis.f90:9-190 for the given atoms.
+Basis build_basis(const std::string& basis_file, const std::vector<std::string>& species,
+                  const std::vector<double>& xyz);
+
+// --------------------------------------------------------- device structures
+struct DeviceBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  void ensure(size_t b);
+  void release();
+  ~DeviceBuf() { release(); }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct TaskList {
+  int nbra = 0;
+  long long nquartets = 0;
+  int ntasks = 0;
+  int* task_off = nullptr;  // device, nbra + 1
+  int* ket_lo = nullptr;    // device, nbra
+  int* ket_hi = nullptr;    // device, nbra
+};
+
+// Packed pair data of one molecule or of a batch (every pair stores the
+// offset and leading dimension of its molecule's matrices).
+struct PairData {
+  int npair = 0;
+  int class_off[NCLASS + 1] = {0, 0, 0, 0};
+  int nprim = 0;
+  int4* info0 = nullptr;     // {bf_a, bf_b, prim_start, n_prim}
+  int4* info1 = nullptr;     // {shell_a, shell_b, atom_a, atom_b}
+  int4* info2 = nullptr;     // {mat_off lo, mat_off hi, ld, molecule}
+  double4* geom = nullptr;   // {ABx, ABy, ABz, Q}
+  float4* geomf = nullptr;
+  double4* prim = nullptr;   // 3 per primitive pair
+  float4* primf = nullptr;
+  std::vector<double> q_host;   // Q of the sorted pairs
+  std::vector<int> cls_host;    // class of the sorted pairs
+  std::vector<int> mol_host;    // molecule of the sorted pairs
+  DeviceBuf buf;
+};
+
+struct JkStats {
+  unsigned long long quartets[2][NQCLASS];  // [fp64, fp32][class]
+  unsigned long long prims[2][NQCLASS];
+};
+
+// Algorithmic flop counts of the generated class routines (eri_classes.cuh).
+struct ClassFlops { int L, nout, vrr, hrr, grad; };
+const ClassFlops& class_flops(int qclass);
+// Flops charged per primitive quartet outside the VRR (prefactors + Boys)
+// and per contracted quartet for the J/K digestion.
+double prim_overhead_flops(int qclass, bool fp32);
+double digest_flops(int qclass, int nk);
+
+// ------------------------------------------------------------- launchers
+// Every kernel launch of this library is counted (pyfacc_launch_count).
+void count_launch();
+long long launch_count();
+void ensure_boys_tables(int device);
+void launch_boys_test(int mode, int fp32, int mmax, int n, const double* x, double* out, cudaStream_t s);
+
+struct ShellDev {  // device copies of the shells (packed over a batch)
+  int ns = 0;
+  double4* cen = nullptr;   // {x, y, z, 0}
+  int4* desc = nullptr;     // {l, atom, bf_off, prim_start}
+  int* nprim = nullptr;
+  double* ex = nullptr;
+  double* co = nullptr;
+  DeviceBuf buf;
+};
+
+// Pair construction: canonical pair list -> records, then Schwarz factors.
+void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const int4* pl1, int4* info0,
+                        int4* info1, int4* info2, double4* geom, double4* prim, cudaStream_t s);
+void launch_schwarz(const PairData& pd, int npair_class_begin[NCLASS + 1], double* q, cudaStream_t s);
+void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
+                         const int4* i2, const double4* g, const double4* pr, const double* q, int4* o0,
+                         int4* o1, int4* o2, double4* og, float4* ogf, double4* opr, float4* oprf,
+                         cudaStream_t s);
+
+struct JkArgs {
+  const double* Dj;      // density for J
+  const double* Dk0;     // densities for K
+  const double* Dk1;
+  double* J;
+  double* K0;
+  double* K1;
+  const float* dmax;     // shell-block max |D|, ns x ns (or null)
+  int ns_ld;             // leading dimension of dmax
+  double thresh;         // density-weighted Schwarz threshold
+  unsigned long long* stats;  // JkStats layout (device) or null
+};
+void launch_jk(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, int nk,
+               const JkArgs& a, int num_sms, cudaStream_t s);
+
+struct GradArgs {
+  const double* Pt;
+  const double* Pa;
+  const double* Pb;
+  const float* dmax;
+  int ns_ld;
+  double thresh;
+  int uhf;
+  double* grad;  // natoms*3 (packed over a batch via the pair's atom index)
+};
+void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, const GradArgs& a,
+                   int num_sms, cudaStream_t s);
+
+void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, int nbf,
+                       double* eri, cudaStream_t s);
+
+// One-electron integrals over canonical shell pairs of the shells in sh.
+struct OneEArgs {
+  int natoms;
+  const double4* atoms;  // {x, y, z, Z}
+  int boys_mode;
+  double* S;
+  double* T;
+  double* V;
+  int nbf;
+};
+void launch_one_electron(const ShellDev& sh, int npair, const int2* pairs, const OneEArgs& a, cudaStream_t s);
+
+struct OneEGradArgs {
+  int natoms;
+  const double4* atoms;
+  int boys_mode;
+  const double* P;
+  const double* W;
+  int nbf;
+  double* grad;
+};
+void launch_grad1e(const ShellDev& sh, int npair, const int2* pairs, const OneEGradArgs& a, cudaStream_t s);
+
+// Small dense helpers.
+void launch_symmetrize_add(int n, double* A, cudaStream_t s);             // A = A + A^T
+void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
+void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
+                 cudaStream_t s);                                          // F = H + J - kf K
+void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s);
+void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb,
+                       const double* Fa, const double* Fb, const double* Ea, const double* Eb,
+                       const double* Pa_old, const double* Pb_old, double* out, cudaStream_t s);
+void launch_scale_columns(int n, double* U, const double* sv, cudaStream_t s);  // U[:,j] /= sqrt(s_j)
+void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
+                 const double* C, float* dmax, cudaStream_t s);
+void launch_zero(void* p, size_t bytes, cudaStream_t s);
+
+double probe_fp64(int device, double* fp32);
+
+}  // namespace pyfacc

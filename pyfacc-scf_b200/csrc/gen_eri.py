@@ -1,0 +1,300 @@
+#!/usr/bin/env python3
+"""Generate eri_classes.cuh: straight-line Obara-Saika / Head-Gordon-Pople
+code for every s/p shell-quartet class of STO-nG bases.
+
+For a class (la lb|lc ld) with la >= lb, lc >= ld the generator emits
+
+* ``vrr``  : one primitive quartet, [e0|f0]^(0) for l(e) in [la, la+lb],
+             l(f) in [lc, lc+ld] built from I_m = pref*F_m(T) by the OS
+             vertical recursion, added into the contracted accumulators;
+* ``hrr``  : the horizontal recursion (a b| = (a+1_i b-1_i| + AB_i (a b-1_i|
+             on the contracted accumulators, bra then ket, giving (ab|cd);
+* ``grad`` : one primitive quartet of the nuclear-gradient contraction
+             sum_abcd Gamma_abcd d(ab|cd)/dX for the centres A, B, C
+             (D follows from translational invariance), using
+             d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}.
+
+It also emits the algorithmic FP operation count (each + - * is one flop)
+of every routine; the kernels multiply them by the number of primitive and
+contracted quartets they evaluate to report FLOP/s.
+
+The recursions are the textbook ones (Obara & Saika, J. Chem. Phys. 84,
+3963 (1986); Head-Gordon & Pople, J. Chem. Phys. 89, 5777 (1988)), the same
+algorithm the reference delegates to Libint 2.11.1 (libint_f.f90:303-625).
+Cartesian components follow cartesian.f90:7-23 (x descending, then y).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+AX = 'xyz'
+
+
+def comps(l):
+    out = []
+    for ax in range(l, -1, -1):
+        for ay in range(l - ax, -1, -1):
+            out.append((ax, ay, l - ax - ay))
+    return out
+
+
+def lsum(c):
+    return c[0] + c[1] + c[2]
+
+
+def first_axis(c):
+    for i in range(3):
+        if c[i] > 0:
+            return i
+    return -1
+
+
+def up(c, i):
+    c = list(c)
+    c[i] += 1
+    return tuple(c)
+
+
+def down(c, i):
+    c = list(c)
+    c[i] -= 1
+    return tuple(c)
+
+
+def cname(c):
+    return f"{c[0]}{c[1]}{c[2]}"
+
+
+class Emitter:
+    def __init__(self):
+        self.lines = []
+        self.flops = 0
+        self.n = 0
+
+    def tmp(self, expr, flops):
+        name = f"t{self.n}"
+        self.n += 1
+        self.lines.append(f"    const R {name} = {expr};")
+        self.flops += flops
+        return name
+
+
+class Vrr:
+    """Symbolic OS VRR on one primitive quartet."""
+
+    def __init__(self, em: Emitter, L: int):
+        self.em = em
+        self.L = L
+        self.memo = {}
+
+    def V(self, e, f, m):
+        key = (e, f, m)
+        if key in self.memo:
+            return self.memo[key]
+        em = self.em
+        if lsum(e) == 0 and lsum(f) == 0:
+            r = f"I[{m}]"
+        elif lsum(f) == 0:
+            i = first_axis(e)
+            e1 = down(e, i)
+            terms, fl = [f"PA[{i}] * {self.V(e1, f, m)}", f"WP[{i}] * {self.V(e1, f, m + 1)}"], 3
+            if e1[i] > 0:
+                e2 = down(e1, i)
+                c = f"{e1[i]}.0 * " if e1[i] > 1 else ""
+                terms.append(f"{c}o2p * ({self.V(e2, f, m)} - rp * {self.V(e2, f, m + 1)})")
+                fl += 4 + (1 if e1[i] > 1 else 0)
+            r = em.tmp(" + ".join(terms), fl)
+        else:
+            i = first_axis(f)
+            f1 = down(f, i)
+            terms, fl = [f"QC[{i}] * {self.V(e, f1, m)}", f"WQ[{i}] * {self.V(e, f1, m + 1)}"], 3
+            if f1[i] > 0:
+                f2 = down(f1, i)
+                c = f"{f1[i]}.0 * " if f1[i] > 1 else ""
+                terms.append(f"{c}o2q * ({self.V(e, f2, m)} - rq * {self.V(e, f2, m + 1)})")
+                fl += 4 + (1 if f1[i] > 1 else 0)
+            if e[i] > 0:
+                c = f"{e[i]}.0 * " if e[i] > 1 else ""
+                terms.append(f"{c}o2pq * {self.V(down(e, i), f1, m + 1)}")
+                fl += 2 + (1 if e[i] > 1 else 0)
+            r = em.tmp(" + ".join(terms), fl)
+        self.memo[key] = r
+        return r
+
+
+class Hrr:
+    """Symbolic HGP HRR.  base(e, f) gives the name of [e0|f0]."""
+
+    def __init__(self, em: Emitter, base):
+        self.em = em
+        self.base = base
+        self.mb = {}
+        self.mk = {}
+
+    def bra(self, a, b, f):
+        key = (a, b, f)
+        if key in self.mb:
+            return self.mb[key]
+        if lsum(b) == 0:
+            r = self.base(a, f)
+        else:
+            i = first_axis(b)
+            r = self.em.tmp(f"{self.bra(up(a, i), down(b, i), f)} + AB[{i}] * {self.bra(a, down(b, i), f)}", 2)
+        self.mb[key] = r
+        return r
+
+    def full(self, a, b, c, d):
+        key = (a, b, c, d)
+        if key in self.mk:
+            return self.mk[key]
+        if lsum(d) == 0:
+            r = self.bra(a, b, c)
+        else:
+            i = first_axis(d)
+            r = self.em.tmp(f"{self.full(a, b, up(c, i), down(d, i))} + CD[{i}] * {self.full(a, b, c, down(d, i))}", 2)
+        self.mk[key] = r
+        return r
+
+
+def ecomps(lo, hi):
+    out = []
+    for l in range(max(lo, 0), hi + 1):
+        out.extend(comps(l))
+    return out
+
+
+def gen_class(la, lb, lc, ld):
+    L = la + lb + lc + ld
+    E = ecomps(la, la + lb)
+    F = ecomps(lc, lc + ld)
+    acc_index = {}
+    for e in E:
+        for f in F:
+            acc_index[(e, f)] = len(acc_index)
+    nacc = len(acc_index)
+    nout = len(comps(la)) * len(comps(lb)) * len(comps(lc)) * len(comps(ld))
+    tag = f"{la}{lb}{lc}{ld}"
+    src = []
+    src.append(f"template <typename R> struct EriClass<R, {la}, {lb}, {lc}, {ld}> {{")
+    src.append(f"  static constexpr int L = {L};")
+    src.append(f"  static constexpr int NACC = {nacc};")
+    src.append(f"  static constexpr int NOUT = {nout};")
+    # --- vrr
+    em = Emitter()
+    v = Vrr(em, L)
+    acc_lines = []
+    for (e, f), k in acc_index.items():
+        acc_lines.append(f"    acc[{k}] += {v.V(e, f, 0)};")
+        em.flops += 1
+    vrr_flops = em.flops
+    src.append("  __device__ static __forceinline__ void vrr(const R* __restrict__ I, const R* __restrict__ PA,")
+    src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
+    src.append("      R o2q, R rq, R o2pq, R* __restrict__ acc) {")
+    src.extend(em.lines)
+    src.extend(acc_lines)
+    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+    src.append("  }")
+    # --- hrr
+    em = Emitter()
+    h = Hrr(em, lambda e, f: f"acc[{acc_index[(e, f)]}]")
+    out_lines = []
+    k = 0
+    for a in comps(la):
+        for b in comps(lb):
+            for c in comps(lc):
+                for d in comps(ld):
+                    out_lines.append(f"    out[{k}] = {h.full(a, b, c, d)};")
+                    k += 1
+    hrr_flops = em.flops
+    src.append("  __device__ static __forceinline__ void hrr(const R* __restrict__ acc, const R* __restrict__ AB,")
+    src.append("      const R* __restrict__ CD, R* __restrict__ out) {")
+    src.extend(em.lines)
+    src.extend(out_lines)
+    src.append("    (void)AB; (void)CD;")
+    src.append("  }")
+    # --- gradient (primitive level, contracted with gam)
+    em = Emitter()
+    v = Vrr(em, L + 1)
+    h = Hrr(em, lambda e, f: v.V(e, f, 0))
+    ls = [la, lb, lc, ld]
+    g_lines = []
+    for ctr in range(3):
+        for x in range(3):
+            up_terms, dn_terms = [], []
+            k = 0
+            for a in comps(la):
+                for b in comps(lb):
+                    for c in comps(lc):
+                        for d in comps(ld):
+                            q = [a, b, c, d]
+                            qu = list(q)
+                            qu[ctr] = up(q[ctr], x)
+                            up_terms.append(f"gam[{k}] * {h.full(*qu)}")
+                            cnt = q[ctr][x]
+                            if cnt > 0:
+                                qd = list(q)
+                                qd[ctr] = down(q[ctr], x)
+                                cc = f"{cnt}.0 * " if cnt > 1 else ""
+                                dn_terms.append(f"{cc}gam[{k}] * {h.full(*qd)}")
+                            k += 1
+            su = em.tmp(" + ".join(up_terms), 2 * len(up_terms) - 1)
+            expr = f"tw[{ctr}] * {su}"
+            fl = 2
+            if dn_terms:
+                sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
+                expr += f" - {sd}"
+                fl += 1
+            g_lines.append(f"    g[{3 * ctr + x}] += w * ({expr});")
+            em.flops += fl + 1
+    grad_flops = em.flops
+    src.append("  // tw[c] = 2 * exponent of centre c (A, B, C); w = primitive weight")
+    src.append("  __device__ static __forceinline__ void grad(const R* __restrict__ I, const R* __restrict__ PA,")
+    src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
+    src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+    src.append("      const R* __restrict__ tw, R w, const R* __restrict__ gam, R* __restrict__ g) {")
+    src.extend(em.lines)
+    src.extend(g_lines)
+    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+    src.append("    (void)AB; (void)CD;")
+    src.append("  }")
+    src.append(f"  static constexpr int VRR_FLOPS = {vrr_flops};")
+    src.append(f"  static constexpr int HRR_FLOPS = {hrr_flops};")
+    src.append(f"  static constexpr int GRAD_FLOPS = {grad_flops};")
+    src.append("};")
+    return "\n".join(src), dict(tag=tag, L=L, nacc=nacc, nout=nout, vrr=vrr_flops, hrr=hrr_flops, grad=grad_flops)
+
+
+CLASSES = [(0, 0, 0, 0), (1, 0, 0, 0), (1, 0, 1, 0), (1, 1, 0, 0), (1, 1, 1, 0), (1, 1, 1, 1)]
+
+
+def generate() -> str:
+    parts = ["// Generated by gen_eri.py -- do not edit by hand.",
+             "// Obara-Saika VRR / Head-Gordon-Pople HRR for s/p shell quartets.",
+             "#pragma once", "",
+             "template <typename R, int LA, int LB, int LC, int LD> struct EriClass;", ""]
+    table = []
+    for cl in CLASSES:
+        s, info = gen_class(*cl)
+        parts.append(s)
+        parts.append("")
+        table.append(info)
+    parts.append("// class | L | accumulators | outputs | vrr flops/prim | hrr flops/contr | grad flops/prim")
+    for t in table:
+        parts.append(f"//  {t['tag']}  | {t['L']} | {t['nacc']:3d} | {t['nout']:3d} | {t['vrr']:5d} | {t['hrr']:4d} | {t['grad']:6d}")
+    return "\n".join(parts) + "\n"
+
+
+def main(out_path=None):
+    here = os.path.dirname(os.path.abspath(__file__))
+    out_path = out_path or os.path.join(here, "eri_classes.cuh")
+    text = generate()
+    old = open(out_path).read() if os.path.exists(out_path) else None
+    if old != text:
+        with open(out_path, "w") as fh:
+            fh.write(text)
+    return out_path
+
+
+if __name__ == "__main__":
+    print(main(sys.argv[1] if len(sys.argv) > 1 else None))

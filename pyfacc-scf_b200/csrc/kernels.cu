@@ -1,0 +1,1279 @@
+// Device code of the B200 Hartree-Fock engine (sm_100a).
+//
+//  * Boys tables (boys.cuh)
+//  * shell-pair construction, Schwarz factors, sorted gather
+//  * J/K digestion: one warp per task = one bra shell pair x 32 ket pairs,
+//    one contracted shell quartet per lane, OS/HGP class code from
+//    eri_classes.cuh, J_ab reduced across the warp with shuffles, the other
+//    J/K blocks added with FP64 atomics; the ERI tensor is never stored
+//  * nuclear-gradient two-electron kernel with the same task layout
+//  * one-electron S/T/V and their derivatives (the reference's formulas,
+//    overlap.f90 / kinetic.f90 / nuclear.f90, evaluated per shell pair)
+//  * dense helpers for the SCF step and an FP64 peak probe
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "boys.cuh"
+#include "engine.h"
+#include "eri_classes.cuh"
+
+namespace pyfacc {
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+// ===========================================================================
+// Boys tables: F_m(T_k), T_k = 0.1 k, from the positive series in long double
+// ===========================================================================
+static long double boys_series_ld(int m, long double x) {
+  if (x <= 0.0L) return 1.0L / (2 * m + 1);
+  long double term = 1.0L / (2 * m + 1), sum = term;
+  for (int k = 1; k < 2000; ++k) {
+    term *= 2.0L * x / (2 * m + 2 * k + 1);
+    sum += term;
+    if (term < sum * 1e-22L) break;
+  }
+  return expl(-x) * sum;
+}
+
+void ensure_boys_tables(int device) {
+  static std::mutex mu;
+  static std::vector<double> tab;
+  static std::vector<float> tabf;
+  static std::vector<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (tab.empty()) {
+    tab.resize(PF_BOYS_NGRID * PF_BOYS_NCOL);
+    tabf.resize(tab.size());
+    for (int k = 0; k < PF_BOYS_NGRID; ++k)
+      for (int m = 0; m < PF_BOYS_NCOL; ++m) {
+        long double v = boys_series_ld(m, (long double)k * 0.1L);
+        tab[k * PF_BOYS_NCOL + m] = (double)v;
+        tabf[k * PF_BOYS_NCOL + m] = (float)v;
+      }
+  }
+  if ((int)done.size() <= device) done.resize(device + 1, 0);
+  if (!done[device]) {
+    PF_CUDA(cudaMemcpyToSymbol(g_boys_tab, tab.data(), tab.size() * sizeof(double)));
+    PF_CUDA(cudaMemcpyToSymbol(g_boys_tabf, tabf.data(), tabf.size() * sizeof(float)));
+    done[device] = 1;
+  }
+}
+
+__global__ void boys_test_kernel(int mode, int fp32, int mmax, int n, const double* __restrict__ x,
+                                 double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double F[PF_BOYS_MMAX + 1];
+  if (fp32) {
+    float Ff[PF_BOYS_MMAX + 1];
+    float T = (float)x[i];
+    switch (mmax) {
+      case 0: boys_fp32<0>(T, Ff); break;
+      case 1: boys_fp32<1>(T, Ff); break;
+      case 2: boys_fp32<2>(T, Ff); break;
+      case 3: boys_fp32<3>(T, Ff); break;
+      case 4: boys_fp32<4>(T, Ff); break;
+      case 5: boys_fp32<5>(T, Ff); break;
+      default: boys_fp32<6>(T, Ff); break;
+    }
+    for (int m = 0; m <= mmax; ++m) F[m] = Ff[m];
+  } else {
+    boys_runtime(mode, mmax, x[i], F);
+  }
+  for (int m = 0; m <= mmax; ++m) out[(size_t)i * (mmax + 1) + m] = F[m];
+}
+
+void launch_boys_test(int mode, int fp32, int mmax, int n, const double* x, double* out, cudaStream_t s) {
+  if (n <= 0) return;
+  boys_test_kernel<<<(n + 127) / 128, 128, 0, s>>>(mode, fp32, mmax, n, x, out);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// Shell pairs
+// ===========================================================================
+__device__ __forceinline__ double prim_norm(int l, double a) {
+  // gaussian.f90:80-98 for l <= 1 (the (2a_x-1)!! product is 1 for s and p)
+  double n = pow(2.0 * a * 0.31830988618379067154, 0.75);
+  return l == 0 ? n : n * 2.0 * sqrt(a);
+}
+
+// pl0 = {shell a, shell b, prim_start, 0}, pl1 = {mat_off, ld, molecule, 0}
+__global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, const int4* __restrict__ desc,
+                                   const int* __restrict__ nprim, const double* __restrict__ ex,
+                                   const double* __restrict__ co, const int4* __restrict__ pl0,
+                                   const int4* __restrict__ pl1, int4* __restrict__ info0,
+                                   int4* __restrict__ info1, int4* __restrict__ info2,
+                                   double4* __restrict__ geom, double4* __restrict__ prim) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npair) return;
+  const int4 p0 = pl0[i];
+  const int a = p0.x, b = p0.y, ps = p0.z;
+  const int4 da = desc[a], db = desc[b];
+  const int na = nprim[a], nb = nprim[b];
+  const double4 A = cen[a], B = cen[b];
+  const double ABx = A.x - B.x, ABy = A.y - B.y, ABz = A.z - B.z;
+  const double ab2 = ABx * ABx + ABy * ABy + ABz * ABz;
+  info0[i] = make_int4(da.z, db.z, ps, na * nb);
+  info1[i] = make_int4(a, b, da.y, db.y);
+  info2[i] = pl1[i];
+  geom[i] = make_double4(ABx, ABy, ABz, 0.0);
+  const double c0 = 1.4142135623730950488 * 4.1748047532602143;  // sqrt(2) * pi^(5/4)
+  for (int ka = 0; ka < na; ++ka) {
+    const double al = ex[da.w + ka], ca = co[da.w + ka] * prim_norm(da.x, ex[da.w + ka]);
+    for (int kb = 0; kb < nb; ++kb) {
+      const double be = ex[db.w + kb], cb = co[db.w + kb] * prim_norm(db.x, ex[db.w + kb]);
+      const double p = al + be, op = 1.0 / p;
+      const double K = ca * cb * exp(-al * be * op * ab2) * c0 * op;
+      const double Px = (al * A.x + be * B.x) * op, Py = (al * A.y + be * B.y) * op, Pz = (al * A.z + be * B.z) * op;
+      double4* r = prim + 3 * (size_t)(ps + ka * nb + kb);
+      r[0] = make_double4(p, 0.5 * op, K, al);
+      r[1] = make_double4(Px, Py, Pz, 0.0);
+      r[2] = make_double4(Px - A.x, Py - A.y, Pz - A.z, 0.0);
+    }
+  }
+}
+
+void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const int4* pl1, int4* info0,
+                        int4* info1, int4* info2, double4* geom, double4* prim, cudaStream_t s) {
+  if (npair <= 0) return;
+  build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, pl0, pl1,
+                                                         info0, info1, info2, geom, prim);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ---------------------------------------------------------------------------
+// One primitive quartet: prefactors, Boys, VRR (shared by J/K, Schwarz,
+// gradient and tensor kernels).
+// ---------------------------------------------------------------------------
+template <typename R>
+struct PrimGeo {
+  R I[PF_BOYS_MMAX + 1];
+  R WP[3], WQ[3];
+  R o2p, rp, o2q, rq, o2pq;
+};
+
+// bra record b0..b2 and ket record k0..k2 (double4 x 3 each)
+template <typename R, int LM>
+__device__ __forceinline__ void prim_setup(const double4& b0, const double4& b1, const double4& k0,
+                                           const double4& k1, PrimGeo<R>& g) {
+  const R p = (R)b0.x, q = (R)k0.x;
+  const R PQx = (R)(b1.x - k1.x), PQy = (R)(b1.y - k1.y), PQz = (R)(b1.z - k1.z);
+  const R zeta = p + q;
+  R rs, oz;
+  if constexpr (sizeof(R) == 8) {
+    rs = rsqrt((double)zeta);
+  } else {
+    rs = rsqrtf((float)zeta);
+  }
+  oz = rs * rs;
+  const R rho = p * q * oz;
+  const R T = rho * (PQx * PQx + PQy * PQy + PQz * PQz);
+  const R pref = (R)b0.z * (R)k0.z * rs;
+  R F[LM + 1];
+  Boys<LM, R>::eval(T, F);
+#pragma unroll
+  for (int m = 0; m <= LM; ++m) g.I[m] = pref * F[m];
+  const R qz = q * oz, pz = p * oz;
+  g.WP[0] = -qz * PQx; g.WP[1] = -qz * PQy; g.WP[2] = -qz * PQz;
+  g.WQ[0] = pz * PQx;  g.WQ[1] = pz * PQy;  g.WQ[2] = pz * PQz;
+  g.o2p = (R)b0.y;
+  g.o2q = (R)k0.y;
+  g.rp = qz;  // rho / p
+  g.rq = pz;  // rho / q
+  g.o2pq = (R)0.5 * oz;
+}
+
+template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
+
+// Contracted (ab|cd) for one bra pair and one ket pair.
+template <typename R, int LA, int LB, int LC, int LD>
+__device__ __forceinline__ void contracted_quartet(const double4* __restrict__ prim, int4 bi0, int4 ki0,
+                                                   const double4& bgeo, const double4& kgeo,
+                                                   R out[EriClass<R, LA, LB, LC, LD>::NOUT]) {
+  using C = EriClass<R, LA, LB, LC, LD>;
+  R acc[C::NACC];
+#pragma unroll
+  for (int i = 0; i < C::NACC; ++i) acc[i] = (R)0;
+  for (int kq = 0; kq < ki0.w; ++kq) {
+    const double4* kr = prim + 3 * (size_t)(ki0.z + kq);
+    const double4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+    for (int kp = 0; kp < bi0.w; ++kp) {
+      const double4* br = prim + 3 * (size_t)(bi0.z + kp);
+      const double4 b0 = br[0], b1 = br[1], b2 = br[2];
+      const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
+      PrimGeo<R> g;
+      prim_setup<R, C::L>(b0, b1, k0, k1, g);
+      C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.rp, g.o2q, g.rq, g.o2pq, acc);
+    }
+  }
+  const R AB[3] = {(R)bgeo.x, (R)bgeo.y, (R)bgeo.z};
+  const R CD[3] = {(R)kgeo.x, (R)kgeo.y, (R)kgeo.z};
+  C::hrr(acc, AB, CD, out);
+}
+
+// Schwarz factor of every pair of one class: Q = sqrt(max |(ab|ab)|).
+template <int LA, int LB>
+__global__ void schwarz_kernel(int begin, int end, const int4* __restrict__ info0, const double4* __restrict__ geom,
+                               const double4* __restrict__ prim, double* __restrict__ q) {
+  int i = begin + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= end) return;
+  using C = EriClass<double, LA, LB, LA, LB>;
+  double out[C::NOUT];
+  const int4 i0 = info0[i];
+  const double4 g = geom[i];
+  contracted_quartet<double, LA, LB, LA, LB>(prim, i0, i0, g, g, out);
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
+  double mx = 0.0;
+#pragma unroll
+  for (int a = 0; a < NA; ++a)
+#pragma unroll
+    for (int b = 0; b < NB; ++b) mx = fmax(mx, fabs(out[((a * NB + b) * NA + a) * NB + b]));
+  q[i] = sqrt(mx);
+}
+
+void launch_schwarz(const PairData& pd, int off[NCLASS + 1], double* q, cudaStream_t s) {
+  for (int c = 0; c < NCLASS; ++c) {
+    int n = off[c + 1] - off[c];
+    if (n <= 0) continue;
+    dim3 grid((n + 63) / 64), block(64);
+    if (c == 0) schwarz_kernel<0, 0><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    if (c == 1) schwarz_kernel<1, 0><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    if (c == 2) schwarz_kernel<1, 1><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    PF_CUDA(cudaGetLastError());
+  count_launch();
+  }
+}
+
+__global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, const int* __restrict__ new_ps,
+                                    const int4* __restrict__ i0, const int4* __restrict__ i1,
+                                    const int4* __restrict__ i2, const double4* __restrict__ g,
+                                    const double4* __restrict__ pr, const double* __restrict__ q,
+                                    int4* __restrict__ o0, int4* __restrict__ o1, int4* __restrict__ o2,
+                                    double4* __restrict__ og, double4* __restrict__ opr) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= npair) return;
+  const int j = perm[i];
+  int4 a = i0[j];
+  const int old_ps = a.z;
+  a.z = new_ps[i];
+  o0[i] = a;
+  o1[i] = i1[j];
+  o2[i] = i2[j];
+  double4 gg = g[j];
+  gg.w = q[j];
+  og[i] = gg;
+  for (int k = 0; k < 3 * a.w; ++k) opr[3 * (size_t)a.z + k] = pr[3 * (size_t)old_ps + k];
+}
+
+void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
+                         const int4* i2, const double4* g, const double4* pr, const double* q, int4* o0,
+                         int4* o1, int4* o2, double4* og, float4*, double4* opr, float4*, cudaStream_t s) {
+  if (npair <= 0) return;
+  gather_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, perm, new_pstart, i0, i1, i2, g, pr, q, o0, o1, o2,
+                                                          og, opr);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// J/K digestion
+// ===========================================================================
+__device__ __forceinline__ int find_bra(const int* __restrict__ task_off, int nbra, int t) {
+  int lo = 0, hi = nbra;  // task_off[lo] <= t < task_off[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(task_off + mid) <= t) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float dmax_bound(const float* __restrict__ dm, int ld, int a, int b, int c, int d) {
+  float m = 2.0f * fmaxf(__ldg(dm + a * ld + b), __ldg(dm + c * ld + d));
+  m = fmaxf(m, __ldg(dm + a * ld + c));
+  m = fmaxf(m, __ldg(dm + a * ld + d));
+  m = fmaxf(m, __ldg(dm + b * ld + c));
+  m = fmaxf(m, __ldg(dm + b * ld + d));
+  return m;
+}
+
+struct JkKernelArgs {
+  JkArgs a;
+  const int4* info0;
+  const int4* info1;
+  const int4* info2;
+  const double4* geom;
+  const double4* prim;
+  const int* task_off;
+  const int* ket_lo;
+  const int* ket_hi;
+  int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec;
+};
+
+template <typename R, int LA, int LB, int LC, int LD, int NK>
+__global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
+  using C = EriClass<R, LA, LB, LC, LD>;
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v, NCc = NC<LC>::v, ND = NC<LD>::v;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const JkArgs& A = args.a;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+    const int ib = find_bra(args.task_off, args.nbra, t);
+    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
+    const int bp = args.bra_base + ib;
+    const int kp = args.ket_base + ket;
+    bool active = ket < __ldg(args.ket_hi + ib);
+    const int4 bi0 = args.info0[bp], bi1 = args.info1[bp], bi2 = args.info2[bp];
+    const double4 bg = args.geom[bp];
+    int4 ki0 = bi0, ki1 = bi1;
+    double4 kg = bg;
+    if (active) {
+      ki0 = args.info0[kp];
+      ki1 = args.info1[kp];
+      kg = args.geom[kp];
+      if (A.dmax) {
+        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        active = bound >= (float)A.thresh;
+      }
+    }
+    const unsigned amask = __ballot_sync(0xffffffffu, active);
+    if (amask == 0u) continue;
+    if (A.stats && lane == 0) {
+      atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
+      atomicAdd(A.stats + (2 + args.prec) * NQCLASS + args.qclass,
+                (unsigned long long)__popc(amask) * (unsigned long long)(bi0.w * ki0.w));
+    }
+    R out[C::NOUT];
+    if (active) {
+      contracted_quartet<R, LA, LB, LC, LD>(args.prim, bi0, ki0, bg, kg, out);
+    } else {
+#pragma unroll
+      for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
+    }
+    // degeneracy factor of the canonical quartet
+    double fac = active ? 1.0 : 0.0;
+    if (bi1.x == bi1.y) fac *= 0.5;
+    if (ki1.x == ki1.y) fac *= 0.5;
+    if (args.same_class && bp == kp) fac *= 0.5;
+    const size_t mo = (size_t)bi2.x;
+    const int ld = bi2.y;
+    const int ma = bi0.x, mb = bi0.y, mc = ki0.x, md = ki0.y;
+    // ---- Coulomb
+    double Dab[NA * NB], Dcd[NCc * ND];
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b) Dab[a * NB + b] = __ldg(A.Dj + mo + (size_t)(ma + a) * ld + mb + b);
+#pragma unroll
+    for (int c = 0; c < NCc; ++c)
+#pragma unroll
+      for (int d = 0; d < ND; ++d)
+        Dcd[c * ND + d] = active ? __ldg(A.Dj + mo + (size_t)(mc + c) * ld + md + d) : 0.0;
+    double jab[NA * NB], jcd[NCc * ND];
+#pragma unroll
+    for (int i = 0; i < NA * NB; ++i) jab[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < NCc * ND; ++i) jcd[i] = 0.0;
+#pragma unroll
+    for (int a = 0; a < NA; ++a)
+#pragma unroll
+      for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (int c = 0; c < NCc; ++c)
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            const double v = fac * (double)out[((a * NB + b) * NCc + c) * ND + d];
+            jab[a * NB + b] += v * Dcd[c * ND + d];
+            jcd[c * ND + d] += v * Dab[a * NB + b];
+          }
+#pragma unroll
+    for (int i = 0; i < NA * NB; ++i) {
+      const double s = warp_sum(jab[i]);
+      if (lane == 0 && s != 0.0) atomicAdd(A.J + mo + (size_t)(ma + i / NB) * ld + mb + i % NB, 2.0 * s);
+    }
+    if (active) {
+#pragma unroll
+      for (int c = 0; c < NCc; ++c)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) atomicAdd(A.J + mo + (size_t)(mc + c) * ld + md + d, 2.0 * jcd[c * ND + d]);
+    }
+    // ---- exchange, one or two densities
+    if (active) {
+#pragma unroll
+      for (int k = 0; k < NK; ++k) {
+        const double* Dk = (k == 0) ? A.Dk0 : A.Dk1;
+        double* Kk = (k == 0) ? A.K0 : A.K1;
+        double kac[NA * NCc], kad[NA * ND], kbc[NB * NCc], kbd[NB * ND];
+#pragma unroll
+        for (int i = 0; i < NA * NCc; ++i) kac[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NA * ND; ++i) kad[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NB * NCc; ++i) kbc[i] = 0.0;
+#pragma unroll
+        for (int i = 0; i < NB * ND; ++i) kbd[i] = 0.0;
+        double Dbd[NB * ND], Dbc[NB * NCc], Dad[NA * ND], Dac[NA * NCc];
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+          for (int d = 0; d < ND; ++d) Dbd[b * ND + d] = __ldg(Dk + mo + (size_t)(mb + b) * ld + md + d);
+#pragma unroll
+          for (int c = 0; c < NCc; ++c) Dbc[b * NCc + c] = __ldg(Dk + mo + (size_t)(mb + b) * ld + mc + c);
+        }
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+#pragma unroll
+          for (int d = 0; d < ND; ++d) Dad[a * ND + d] = __ldg(Dk + mo + (size_t)(ma + a) * ld + md + d);
+#pragma unroll
+          for (int c = 0; c < NCc; ++c) Dac[a * NCc + c] = __ldg(Dk + mo + (size_t)(ma + a) * ld + mc + c);
+        }
+#pragma unroll
+        for (int a = 0; a < NA; ++a)
+#pragma unroll
+          for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int c = 0; c < NCc; ++c)
+#pragma unroll
+              for (int d = 0; d < ND; ++d) {
+                const double v = fac * (double)out[((a * NB + b) * NCc + c) * ND + d];
+                kac[a * NCc + c] += v * Dbd[b * ND + d];
+                kad[a * ND + d] += v * Dbc[b * NCc + c];
+                kbc[b * NCc + c] += v * Dad[a * ND + d];
+                kbd[b * ND + d] += v * Dac[a * NCc + c];
+              }
+#pragma unroll
+        for (int a = 0; a < NA; ++a) {
+#pragma unroll
+          for (int c = 0; c < NCc; ++c) atomicAdd(Kk + mo + (size_t)(ma + a) * ld + mc + c, kac[a * NCc + c]);
+#pragma unroll
+          for (int d = 0; d < ND; ++d) atomicAdd(Kk + mo + (size_t)(ma + a) * ld + md + d, kad[a * ND + d]);
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+          for (int c = 0; c < NCc; ++c) atomicAdd(Kk + mo + (size_t)(mb + b) * ld + mc + c, kbc[b * NCc + c]);
+#pragma unroll
+          for (int d = 0; d < ND; ++d) atomicAdd(Kk + mo + (size_t)(mb + b) * ld + md + d, kbd[b * ND + d]);
+        }
+      }
+    }
+  }
+}
+
+static int qclass_of(int bc, int kc) {
+  // (ss|ss)=0 (ps|ss)=1 (ps|ps)=2 (pp|ss)=3 (pp|ps)=4 (pp|pp)=5
+  static const int tab[3][3] = {{0, -1, -1}, {1, 2, -1}, {3, 4, 5}};
+  return tab[bc][kc];
+}
+
+template <typename R, int LA, int LB, int LC, int LD>
+static void jk_dispatch_nk(int nk, dim3 grid, dim3 block, cudaStream_t s, const JkKernelArgs& k) {
+  if (nk == 1) jk_kernel<R, LA, LB, LC, LD, 1><<<grid, block, 0, s>>>(k);
+  else jk_kernel<R, LA, LB, LC, LD, 2><<<grid, block, 0, s>>>(k);
+}
+
+template <typename R>
+static void jk_dispatch(int qc, int nk, dim3 grid, dim3 block, cudaStream_t s, const JkKernelArgs& k) {
+  switch (qc) {
+    case 0: jk_dispatch_nk<R, 0, 0, 0, 0>(nk, grid, block, s, k); break;
+    case 1: jk_dispatch_nk<R, 1, 0, 0, 0>(nk, grid, block, s, k); break;
+    case 2: jk_dispatch_nk<R, 1, 0, 1, 0>(nk, grid, block, s, k); break;
+    case 3: jk_dispatch_nk<R, 1, 1, 0, 0>(nk, grid, block, s, k); break;
+    case 4: jk_dispatch_nk<R, 1, 1, 1, 0>(nk, grid, block, s, k); break;
+    default: jk_dispatch_nk<R, 1, 1, 1, 1>(nk, grid, block, s, k); break;
+  }
+}
+
+static int grid_for(int ntasks, int num_sms) {
+  long long warps_needed = ntasks;
+  long long blocks = (warps_needed + 3) / 4;
+  long long cap = (long long)num_sms * 16;
+  return (int)std::max(1LL, std::min(blocks, cap));
+}
+
+void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32, int nk, const JkArgs& a,
+               int num_sms, cudaStream_t s) {
+  if (tl.ntasks <= 0) return;
+  JkKernelArgs k;
+  k.a = a;
+  k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
+  k.geom = pd.geom; k.prim = pd.prim;
+  k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
+  k.nbra = tl.nbra; k.ntasks = tl.ntasks;
+  k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  k.same_class = (bc == kc);
+  k.qclass = qclass_of(bc, kc);
+  k.prec = fp32 ? 1 : 0;
+  dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
+  if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, s, k);
+  else jk_dispatch<double>(k.qclass, nk, grid, block, s, k);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// Nuclear gradient, two-electron part
+// ===========================================================================
+struct GradKernelArgs {
+  GradArgs a;
+  const int4* info0;
+  const int4* info1;
+  const int4* info2;
+  const double4* geom;
+  const double4* prim;
+  const int* task_off;
+  const int* ket_lo;
+  const int* ket_hi;
+  int nbra, ntasks, bra_base, ket_base, same_class;
+};
+
+template <int LA, int LB, int LC, int LD>
+__global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) {
+  using C = EriClass<double, LA, LB, LC, LD>;
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v, NCc = NC<LC>::v, ND = NC<LD>::v;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  const GradArgs& A = args.a;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+    const int ib = find_bra(args.task_off, args.nbra, t);
+    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
+    const int bp = args.bra_base + ib;
+    const int kp = args.ket_base + ket;
+    bool active = ket < __ldg(args.ket_hi + ib);
+    const int4 bi0 = args.info0[bp], bi1 = args.info1[bp], bi2 = args.info2[bp];
+    const double4 bg = args.geom[bp];
+    int4 ki0 = bi0, ki1 = bi1;
+    double4 kg = bg;
+    if (active) {
+      ki0 = args.info0[kp];
+      ki1 = args.info1[kp];
+      kg = args.geom[kp];
+      if (A.dmax) {
+        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        active = bound >= (float)A.thresh;
+      }
+    }
+    if (__ballot_sync(0xffffffffu, active) == 0u) continue;
+    double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (active) {
+      const size_t mo = (size_t)bi2.x;
+      const int ld = bi2.y;
+      const int ma = bi0.x, mb = bi0.y, mc = ki0.x, md = ki0.y;
+      double gam[C::NOUT];
+#pragma unroll
+      for (int a = 0; a < NA; ++a)
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int c = 0; c < NCc; ++c)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+              const size_t mu = ma + a, nu = mb + b, la = mc + c, si = md + d;
+              const double* Pt = A.Pt + mo;
+              double v = __ldg(Pt + mu * ld + nu) * __ldg(Pt + la * ld + si);
+              if (A.uhf) {
+                const double* Pa = A.Pa + mo;
+                const double* Pb = A.Pb + mo;
+                v -= 0.5 * (__ldg(Pa + mu * ld + la) * __ldg(Pa + nu * ld + si) +
+                            __ldg(Pa + mu * ld + si) * __ldg(Pa + nu * ld + la));
+                v -= 0.5 * (__ldg(Pb + mu * ld + la) * __ldg(Pb + nu * ld + si) +
+                            __ldg(Pb + mu * ld + si) * __ldg(Pb + nu * ld + la));
+              } else {
+                v -= 0.25 * (__ldg(Pt + mu * ld + la) * __ldg(Pt + nu * ld + si) +
+                             __ldg(Pt + mu * ld + si) * __ldg(Pt + nu * ld + la));
+              }
+              gam[((a * NB + b) * NCc + c) * ND + d] = v;
+            }
+      const double AB[3] = {bg.x, bg.y, bg.z};
+      const double CD[3] = {kg.x, kg.y, kg.z};
+      for (int kq = 0; kq < ki0.w; ++kq) {
+        const double4* kr = args.prim + 3 * (size_t)(ki0.z + kq);
+        const double4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
+        const double QC[3] = {k2.x, k2.y, k2.z};
+        for (int kpp = 0; kpp < bi0.w; ++kpp) {
+          const double4* br = args.prim + 3 * (size_t)(bi0.z + kpp);
+          const double4 b0 = br[0], b1 = br[1], b2 = br[2];
+          const double PA[3] = {b2.x, b2.y, b2.z};
+          PrimGeo<double> pg;
+          prim_setup<double, C::L + 1>(b0, b1, k0, k1, pg);
+          const double tw[3] = {2.0 * b0.w, 2.0 * (b0.x - b0.w), 2.0 * k0.w};
+          C::grad(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, tw, 1.0, gam, g);
+        }
+      }
+      double fac = 4.0;
+      if (bi1.x == bi1.y) fac *= 0.5;
+      if (ki1.x == ki1.y) fac *= 0.5;
+      if (args.same_class && bp == kp) fac *= 0.5;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) g[i] *= fac;
+    }
+    // centre A and B are the bra's, uniform across the warp
+    double* G = A.grad;
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const double sa = warp_sum(g[x]);
+      const double sb = warp_sum(g[3 + x]);
+      if (lane == 0) {
+        atomicAdd(G + 3 * bi1.z + x, sa);
+        atomicAdd(G + 3 * bi1.w + x, sb);
+      }
+    }
+    if (active) {
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        atomicAdd(G + 3 * ki1.z + x, g[6 + x]);
+        atomicAdd(G + 3 * ki1.w + x, -(g[x] + g[3 + x] + g[6 + x]));
+      }
+    }
+  }
+}
+
+void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, const GradArgs& a, int num_sms,
+                   cudaStream_t s) {
+  if (tl.ntasks <= 0) return;
+  GradKernelArgs k;
+  k.a = a;
+  k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
+  k.geom = pd.geom; k.prim = pd.prim;
+  k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
+  k.nbra = tl.nbra; k.ntasks = tl.ntasks;
+  k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  k.same_class = (bc == kc);
+  dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
+  switch (qclass_of(bc, kc)) {
+    case 0: grad2e_kernel<0, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 1: grad2e_kernel<1, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 2: grad2e_kernel<1, 0, 1, 0><<<grid, block, 0, s>>>(k); break;
+    case 3: grad2e_kernel<1, 1, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 4: grad2e_kernel<1, 1, 1, 0><<<grid, block, 0, s>>>(k); break;
+    default: grad2e_kernel<1, 1, 1, 1><<<grid, block, 0, s>>>(k); break;
+  }
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// Full ERI tensor (small systems, tests): every canonical quartet writes its
+// eight images.
+// ===========================================================================
+template <int LA, int LB, int LC, int LD>
+__global__ void eri_tensor_kernel(const JkKernelArgs args, int n, double* __restrict__ eri) {
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v, NCc = NC<LC>::v, ND = NC<LD>::v;
+  using C = EriClass<double, LA, LB, LC, LD>;
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+    const int ib = find_bra(args.task_off, args.nbra, t);
+    const int ket = args.ket_lo[ib] + (t - args.task_off[ib]) * TASK_WIDTH + lane;
+    if (ket >= args.ket_hi[ib]) continue;
+    const int bp = args.bra_base + ib, kp = args.ket_base + ket;
+    const int4 bi0 = args.info0[bp], ki0 = args.info0[kp];
+    double out[C::NOUT];
+    contracted_quartet<double, LA, LB, LC, LD>(args.prim, bi0, ki0, args.geom[bp], args.geom[kp], out);
+    for (int a = 0; a < NA; ++a)
+      for (int b = 0; b < NB; ++b)
+        for (int c = 0; c < NCc; ++c)
+          for (int d = 0; d < ND; ++d) {
+            const size_t i = bi0.x + a, j = bi0.y + b, k = ki0.x + c, l = ki0.y + d;
+            const double v = out[((a * NB + b) * NCc + c) * ND + d];
+            const size_t N = n;
+            eri[((i * N + j) * N + k) * N + l] = v;
+            eri[((j * N + i) * N + k) * N + l] = v;
+            eri[((i * N + j) * N + l) * N + k] = v;
+            eri[((j * N + i) * N + l) * N + k] = v;
+            eri[((k * N + l) * N + i) * N + j] = v;
+            eri[((l * N + k) * N + i) * N + j] = v;
+            eri[((k * N + l) * N + j) * N + i] = v;
+            eri[((l * N + k) * N + j) * N + i] = v;
+          }
+  }
+}
+
+void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bc, int kc, int nbf, double* eri,
+                       cudaStream_t s) {
+  if (tl.ntasks <= 0) return;
+  JkKernelArgs k{};
+  k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
+  k.geom = pd.geom; k.prim = pd.prim;
+  k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
+  k.nbra = tl.nbra; k.ntasks = tl.ntasks;
+  k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  dim3 grid((tl.ntasks + 3) / 4), block(128);
+  switch (qclass_of(bc, kc)) {
+    case 0: eri_tensor_kernel<0, 0, 0, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
+    case 1: eri_tensor_kernel<1, 0, 0, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
+    case 2: eri_tensor_kernel<1, 0, 1, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
+    case 3: eri_tensor_kernel<1, 1, 0, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
+    case 4: eri_tensor_kernel<1, 1, 1, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
+    default: eri_tensor_kernel<1, 1, 1, 1><<<grid, block, 0, s>>>(k, nbf, eri); break;
+  }
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// One-electron integrals: the reference's formulas per primitive pair
+// (overlap.f90:121-174 OS overlap, overlap.f90:24-60 + kinetic.f90:20-54
+// binomial kinetic, nuclear.f90:19-136 Cook/THO nuclear attraction).
+// ===========================================================================
+__device__ __forceinline__ double ipowd(double x, int n) {
+  double r = 1.0;
+  for (int i = 0; i < n; ++i) r *= x;
+  return r;
+}
+__device__ __forceinline__ double factd(int n) {
+  double r = 1.0;
+  for (int i = 2; i <= n; ++i) r *= i;
+  return r;
+}
+__device__ __forceinline__ double fact2d(int n) {
+  double r = 1.0;
+  for (int i = n; i > 1; i -= 2) r *= i;
+  return r;
+}
+__device__ __forceinline__ double binomd(int n, int k) { return factd(n) / (factd(k) * factd(n - k)); }
+
+// 1-D overlap S(a,b) by the recursion of overlap.f90:121-145 (with the
+// Gaussian factor sqrt(pi/p) exp(-ab/p X^2) of S00 included).
+__device__ double sij_1d(int a, int b, double aa, double bb, double Ra, double Rb, double Rp) {
+  if (a < 0 || b < 0) return 0.0;
+  double S[6][6];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) S[i][j] = 0.0;
+  const double p = aa + bb;
+  S[1][1] = sqrt(3.14159265358979323846 / p) * exp(-(aa * bb) / p * (Ra - Rb) * (Ra - Rb));
+  const double o2p = 1.0 / (2.0 * p);
+  for (int i = 0; i <= a; ++i)
+    for (int j = 0; j <= b; ++j) {
+      if (i + 1 <= a) S[i + 2][j + 1] = (Rp - Ra) * S[i + 1][j + 1] + o2p * (i * S[i][j + 1] + j * S[i + 1][j]);
+      if (j + 1 <= b) S[i + 1][j + 2] = (Rp - Rb) * S[i + 1][j + 1] + o2p * (i * S[i][j + 1] + j * S[i + 1][j]);
+    }
+  return S[a + 1][b + 1];
+}
+
+// Binomial 1-D overlap Si of overlap.f90:24-60 (no Gaussian factor).
+__device__ double si_binom(int a, int b, double aa, double bb, double Ra, double Rb, double R) {
+  double s = 0.0;
+  for (int i = 0; i <= a; ++i)
+    for (int j = 0; j <= b; ++j)
+      if (((i + j) & 1) == 0) {
+        double t = binomd(a, i) * binomd(b, j) * fact2d(i + j - 1);
+        t *= ipowd(R - Ra, a - i);
+        t *= ipowd(R - Rb, b - j);
+        t /= pow(2.0 * (aa + bb), (i + j) / 2.0);
+        s += t;
+      }
+  return s;
+}
+
+__device__ double ki_term(int ac, int a1, int a2, int bc, int b1, int b2, double aa, double bb, double Ra, double Rb,
+                          double Ra1, double Rb1, double Ra2, double Rb2, double Rc, double R1, double R2, double cp) {
+  double k = 0.0;
+  k += ac * bc * si_binom(ac - 1, bc - 1, aa, bb, Ra, Rb, Rc);
+  k -= 2.0 * aa * bc * si_binom(ac + 1, bc - 1, aa, bb, Ra, Rb, Rc);
+  k -= 2.0 * ac * bb * si_binom(ac - 1, bc + 1, aa, bb, Ra, Rb, Rc);
+  k += 4.0 * aa * bb * si_binom(ac + 1, bc + 1, aa, bb, Ra, Rb, Rc);
+  k *= 0.5;
+  double v = cp * pow(3.14159265358979323846 / (aa + bb), 1.5) * k;
+  v *= si_binom(a1, b1, aa, bb, Ra1, Rb1, R1);
+  v *= si_binom(a2, b2, aa, bb, Ra2, Rb2, R2);
+  return v;
+}
+
+struct Prim1e {
+  double aa, bb, p, cp;
+  double A[3], B[3], P[3];
+};
+
+__device__ __forceinline__ bool valid3(const int* a) { return a[0] >= 0 && a[1] >= 0 && a[2] >= 0; }
+
+__device__ double overlap_u(const int* a, const int* b, const Prim1e& g) {
+  if (!valid3(a) || !valid3(b)) return 0.0;
+  double s = 1.0;
+  for (int x = 0; x < 3; ++x) s *= sij_1d(a[x], b[x], g.aa, g.bb, g.A[x], g.B[x], g.P[x]);
+  return s;
+}
+
+__device__ double kinetic_u(const int* a, const int* b, const Prim1e& g) {
+  if (!valid3(a) || !valid3(b)) return 0.0;
+  const double *A = g.A, *B = g.B, *P = g.P;
+  double k = ki_term(a[0], a[1], a[2], b[0], b[1], b[2], g.aa, g.bb, A[0], B[0], A[1], B[1], A[2], B[2], P[0], P[1], P[2], g.cp);
+  k += ki_term(a[1], a[2], a[0], b[1], b[2], b[0], g.aa, g.bb, A[1], B[1], A[2], B[2], A[0], B[0], P[1], P[2], P[0], g.cp);
+  k += ki_term(a[2], a[0], a[1], b[2], b[0], b[1], g.aa, g.bb, A[2], B[2], A[0], B[0], A[1], B[1], P[2], P[0], P[1], g.cp);
+  return k;
+}
+
+__device__ double fcoefd(int j, int l, int m, double a, double b) {
+  double r = 0.0;
+  for (int k = max(0, j - m); k <= min(j, l); ++k) r += binomd(l, k) * binomd(m, j - k) * ipowd(a, l - k) * ipowd(b, m + k - j);
+  return r;
+}
+__device__ double afac(int l, int r, int i, int l1, int l2, double Ra, double Rb, double Rc, double Rp, double eps) {
+  double a = (l & 1) ? -1.0 : 1.0;
+  a *= fcoefd(l, l1, l2, Rp - Ra, Rp - Rb);
+  a *= (i & 1) ? -1.0 : 1.0;
+  a *= factd(l);
+  a *= ipowd(Rp - Rc, l - 2 * r - 2 * i);
+  a *= ipowd(eps, r + i);
+  a /= factd(r) * factd(i) * factd(l - 2 * r - 2 * i);
+  return a;
+}
+
+// <a| 1/|r-C| |b> (unnormalised) * 2 pi / p * K_AB given F_0..F_{la+lb}.
+__device__ double nuclear_u(const int* a, const int* b, const Prim1e& g, const double* C, const double* F) {
+  if (!valid3(a) || !valid3(b)) return 0.0;
+  const double eps = 1.0 / (4.0 * g.p);
+  double v = 0.0;
+  for (int l = 0; l <= a[0] + b[0]; ++l)
+    for (int r = 0; r <= l / 2; ++r)
+      for (int i = 0; i <= (l - 2 * r) / 2; ++i) {
+        const double Ax = afac(l, r, i, a[0], b[0], g.A[0], g.B[0], C[0], g.P[0], eps);
+        for (int m = 0; m <= a[1] + b[1]; ++m)
+          for (int s = 0; s <= m / 2; ++s)
+            for (int j = 0; j <= (m - 2 * s) / 2; ++j) {
+              const double Ay = afac(m, s, j, a[1], b[1], g.A[1], g.B[1], C[1], g.P[1], eps);
+              for (int n = 0; n <= a[2] + b[2]; ++n)
+                for (int t = 0; t <= n / 2; ++t)
+                  for (int k = 0; k <= (n - 2 * t) / 2; ++k) {
+                    const double Az = afac(n, t, k, a[2], b[2], g.A[2], g.B[2], C[2], g.P[2], eps);
+                    v += Ax * Ay * Az * F[l + m + n - 2 * (r + s + t) - (i + j + k)];
+                  }
+            }
+      }
+  return v * g.cp * 2.0 * 3.14159265358979323846 / g.p;
+}
+
+__device__ __forceinline__ void cart_comp(int l, int k, int* c) {
+  // x descending, then y (cartesian.f90:7-23), l <= 2
+  if (l == 0) { c[0] = c[1] = c[2] = 0; return; }
+  if (l == 1) { c[0] = (k == 0); c[1] = (k == 1); c[2] = (k == 2); return; }
+  const int t[6][3] = {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}};
+  c[0] = t[k][0]; c[1] = t[k][1]; c[2] = t[k][2];
+}
+
+__device__ __forceinline__ double norm_comp(const int* c, double a) {
+  const int l = c[0] + c[1] + c[2];
+  double n = pow(2.0 * a * 0.31830988618379067154, 0.75) * pow(4.0 * a, 0.5 * l);
+  return n / sqrt(fact2d(2 * c[0] - 1) * fact2d(2 * c[1] - 1) * fact2d(2 * c[2] - 1));
+}
+
+__device__ __forceinline__ void prim1e_setup(double aa, double bb, const double4& A, const double4& B, Prim1e& g) {
+  g.aa = aa; g.bb = bb; g.p = aa + bb;
+  g.A[0] = A.x; g.A[1] = A.y; g.A[2] = A.z;
+  g.B[0] = B.x; g.B[1] = B.y; g.B[2] = B.z;
+  double ab2 = 0.0;
+  for (int x = 0; x < 3; ++x) {
+    g.P[x] = (aa * g.A[x] + bb * g.B[x]) / g.p;
+    ab2 += (g.A[x] - g.B[x]) * (g.A[x] - g.B[x]);
+  }
+  g.cp = exp(-aa * bb / g.p * ab2);
+}
+
+// One warp per shell pair (a <= b): lanes share the (primitive pair, atom)
+// combinations; S and T use the primitive pairs only.
+__global__ void one_electron_kernel(int npair, const int2* __restrict__ pairs, const double4* __restrict__ cen,
+                                    const int4* __restrict__ desc, const int* __restrict__ nprim,
+                                    const double* __restrict__ ex, const double* __restrict__ co, OneEArgs args) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= npair) return;
+  const int2 pr = pairs[w];
+  const int4 da = desc[pr.x], db = desc[pr.y];
+  const int la = da.x, lb = db.x, na = nprim[pr.x], nb = nprim[pr.y];
+  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
+  const double4 A = cen[pr.x], B = cen[pr.y];
+  double s[9], t[9], v[9];
+  for (int i = 0; i < 9; ++i) s[i] = t[i] = v[i] = 0.0;
+  const int npp = na * nb;
+  const int work = npp * args.natoms;
+  for (int idx = lane; idx < work; idx += 32) {
+    const int pp = idx % npp, c = idx / npp;
+    const int ka = pp / nb, kb = pp % nb;
+    const double aa = ex[da.w + ka], bb = ex[db.w + kb];
+    Prim1e g;
+    prim1e_setup(aa, bb, A, B, g);
+    const double4 Cn = args.atoms[c];
+    const double C[3] = {Cn.x, Cn.y, Cn.z};
+    double pc2 = 0.0;
+    for (int x = 0; x < 3; ++x) pc2 += (g.P[x] - C[x]) * (g.P[x] - C[x]);
+    double F[PF_BOYS_MMAX + 1];
+    boys_runtime(args.boys_mode, la + lb, g.p * pc2, F);
+    const double cc = co[da.w + ka] * co[db.w + kb];
+    for (int ia = 0; ia < nca; ++ia)
+      for (int ib = 0; ib < ncb; ++ib) {
+        int ca[3], cb[3];
+        cart_comp(la, ia, ca);
+        cart_comp(lb, ib, cb);
+        const double w2 = cc * norm_comp(ca, aa) * norm_comp(cb, bb);
+        if (c == 0) {
+          s[ia * 3 + ib] += w2 * overlap_u(ca, cb, g);
+          t[ia * 3 + ib] += w2 * kinetic_u(ca, cb, g);
+        }
+        v[ia * 3 + ib] += w2 * (-Cn.w) * nuclear_u(ca, cb, g, C, F);
+      }
+  }
+  for (int i = 0; i < 9; ++i) {
+    s[i] = warp_sum(s[i]);
+    t[i] = warp_sum(t[i]);
+    v[i] = warp_sum(v[i]);
+  }
+  if (lane == 0) {
+    const int n = args.nbf;
+    for (int ia = 0; ia < nca; ++ia)
+      for (int ib = 0; ib < ncb; ++ib) {
+        const size_t mu = da.z + ia, nu = db.z + ib;
+        const int k = ia * 3 + ib;
+        if (args.S) { args.S[mu * n + nu] = s[k]; args.S[nu * n + mu] = s[k]; }
+        if (args.T) { args.T[mu * n + nu] = t[k]; args.T[nu * n + mu] = t[k]; }
+        if (args.V) { args.V[mu * n + nu] = v[k]; args.V[nu * n + mu] = v[k]; }
+      }
+  }
+}
+
+void launch_one_electron(const ShellDev& sh, int npair, const int2* pairs, const OneEArgs& a, cudaStream_t s) {
+  if (npair <= 0) return;
+  one_electron_kernel<<<(npair + 3) / 4, 128, 0, s>>>(npair, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// Gradient of the one-electron energy over canonical shell pairs (a <= b):
+//   sum P (dT + dV) - sum W dS, d/dB = -d/dA for the two-centre S and T,
+//   d/dC V^C = -(d/dA + d/dB) V^C for every nucleus C.
+__global__ void grad1e_kernel(int npair, const int2* __restrict__ pairs, const double4* __restrict__ cen,
+                              const int4* __restrict__ desc, const int* __restrict__ nprim,
+                              const double* __restrict__ ex, const double* __restrict__ co, OneEGradArgs args) {
+  const int lane = threadIdx.x & 31;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= npair) return;
+  const int2 pr = pairs[w];
+  const int4 da = desc[pr.x], db = desc[pr.y];
+  const int la = da.x, lb = db.x, na = nprim[pr.x], nb = nprim[pr.y];
+  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
+  const double4 A = cen[pr.x], B = cen[pr.y];
+  const double wgt = (pr.x == pr.y) ? 1.0 : 2.0;
+  const int n = args.nbf;
+  double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
+  const int npp = na * nb;
+  const int work = npp * args.natoms;
+  for (int idx = lane; idx < work; idx += 32) {
+    const int pp = idx % npp, c = idx / npp;
+    const int ka = pp / nb, kb = pp % nb;
+    const double aa = ex[da.w + ka], bb = ex[db.w + kb];
+    Prim1e g;
+    prim1e_setup(aa, bb, A, B, g);
+    const double4 Cn = args.atoms[c];
+    const double C[3] = {Cn.x, Cn.y, Cn.z};
+    double pc2 = 0.0;
+    for (int x = 0; x < 3; ++x) pc2 += (g.P[x] - C[x]) * (g.P[x] - C[x]);
+    double F[PF_BOYS_MMAX + 1];
+    boys_runtime(args.boys_mode, la + lb + 1, g.p * pc2, F);
+    const double cc = co[da.w + ka] * co[db.w + kb];
+    double gC[3] = {0, 0, 0};
+    for (int ia = 0; ia < nca; ++ia)
+      for (int ib = 0; ib < ncb; ++ib) {
+        int ca[3], cb[3];
+        cart_comp(la, ia, ca);
+        cart_comp(lb, ib, cb);
+        const size_t mu = da.z + ia, nu = db.z + ib;
+        const double pw = wgt * cc * norm_comp(ca, aa) * norm_comp(cb, bb);
+        const double P = args.P[mu * n + nu] * pw, W = args.W[mu * n + nu] * pw;
+        for (int x = 0; x < 3; ++x) {
+          int up[3] = {ca[0], ca[1], ca[2]}, dn[3] = {ca[0], ca[1], ca[2]};
+          int bu[3] = {cb[0], cb[1], cb[2]}, bd[3] = {cb[0], cb[1], cb[2]};
+          up[x] += 1; dn[x] -= 1; bu[x] += 1; bd[x] -= 1;
+          double va = 2.0 * aa * nuclear_u(up, cb, g, C, F) - ca[x] * nuclear_u(dn, cb, g, C, F);
+          double vb = 2.0 * bb * nuclear_u(ca, bu, g, C, F) - cb[x] * nuclear_u(ca, bd, g, C, F);
+          va *= -Cn.w * P;
+          vb *= -Cn.w * P;
+          gA[x] += va;
+          gB[x] += vb;
+          gC[x] -= va + vb;
+          if (c == 0) {
+            const double ds = 2.0 * aa * overlap_u(up, cb, g) - ca[x] * overlap_u(dn, cb, g);
+            const double dt = 2.0 * aa * kinetic_u(up, cb, g) - ca[x] * kinetic_u(dn, cb, g);
+            const double d = P * dt - W * ds;
+            gA[x] += d;
+            gB[x] -= d;
+          }
+        }
+      }
+    for (int x = 0; x < 3; ++x) atomicAdd(args.grad + 3 * c + x, gC[x]);
+  }
+  for (int x = 0; x < 3; ++x) {
+    const double sa = warp_sum(gA[x]), sb = warp_sum(gB[x]);
+    if (lane == 0) {
+      atomicAdd(args.grad + 3 * da.y + x, sa);
+      atomicAdd(args.grad + 3 * db.y + x, sb);
+    }
+  }
+}
+
+void launch_grad1e(const ShellDev& sh, int npair, const int2* pairs, const OneEGradArgs& a, cudaStream_t s) {
+  if (npair <= 0) return;
+  grad1e_kernel<<<(npair + 3) / 4, 128, 0, s>>>(npair, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ===========================================================================
+// Dense helpers
+// ===========================================================================
+__global__ void symmetrize_add_kernel(int n, double* A) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || j > i) return;
+  const double s = A[(size_t)i * n + j] + A[(size_t)j * n + i];
+  A[(size_t)i * n + j] = s;
+  A[(size_t)j * n + i] = s;
+}
+void launch_symmetrize_add(int n, double* A, cudaStream_t s) {
+  dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
+  symmetrize_add_kernel<<<g, b, 0, s>>>(n, A);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+__global__ void axpby_kernel(long long n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s) {
+  int g = (int)std::min<long long>((n + 255) / 256, 4096);
+  axpby_kernel<<<std::max(g, 1), 256, 0, s>>>(n, a, x, b, y);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+__global__ void fock_kernel(long long n, const double* __restrict__ H, const double* __restrict__ J, double kf,
+                            const double* __restrict__ K, double* __restrict__ F) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    F[i] = H[i] + J[i] - kf * K[i];
+}
+void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
+                 cudaStream_t s) {
+  int g = (int)std::min<long long>((n + 255) / 256, 4096);
+  fock_kernel<<<std::max(g, 1), 256, 0, s>>>(n, H, J, kf, K, F);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = (threadIdx.x < (blockDim.x >> 5)) ? sh[threadIdx.x] : 0.0;
+  if (w == 0) v = warp_sum(v);
+  __syncthreads();
+  return v;
+}
+
+// out[j] = <x, ys[j]>, one block per j (deterministic order).
+__global__ void dot_many_kernel(long long n, const double* __restrict__ x, const double* const* ys, double* out) {
+  __shared__ double sh[32];
+  const double* y = ys[blockIdx.x];
+  double acc = 0.0;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) acc += x[i] * y[i];
+  acc = block_sum(acc, sh);
+  if (threadIdx.x == 0) out[blockIdx.x] = acc;
+}
+void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s) {
+  if (m <= 0) return;
+  dot_many_kernel<<<m, 512, 0, s>>>(n, x, ys, out);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// One block: out[0] = sum Pt H + sum Pa Fa + sum Pb Fb (x 1/2 applied by the
+// caller), out[1] = max |Ea|,|Eb|, out[2] = ||dP||_F^2.
+__global__ void scf_reduce_kernel(long long n, int uhf, const double* __restrict__ H, const double* __restrict__ Pa,
+                                  const double* __restrict__ Pb, const double* __restrict__ Fa,
+                                  const double* __restrict__ Fb, const double* __restrict__ Ea,
+                                  const double* __restrict__ Eb, const double* __restrict__ Pa_old,
+                                  const double* __restrict__ Pb_old, double* out) {
+  __shared__ double sh[32];
+  double e = 0.0, dp = 0.0;
+  double emx = 0.0;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+    if (uhf) {
+      e += (Pa[i] + Pb[i]) * H[i] + Pa[i] * Fa[i] + Pb[i] * Fb[i];
+      emx = fmax(emx, fmax(fabs(Ea[i]), fabs(Eb[i])));
+      if (Pa_old) {
+        const double d1 = Pa[i] - Pa_old[i], d2 = Pb[i] - Pb_old[i];
+        dp += d1 * d1 + d2 * d2;
+      }
+    } else {
+      e += Pa[i] * (H[i] + Fa[i]);
+      emx = fmax(emx, fabs(Ea[i]));
+      if (Pa_old) {
+        const double d1 = Pa[i] - Pa_old[i];
+        dp += d1 * d1;
+      }
+    }
+  }
+  e = block_sum(e, sh);
+  dp = block_sum(dp, sh);
+  // max reduction
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) emx = fmax(emx, __shfl_xor_sync(0xffffffffu, emx, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = emx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmax(m, sh[k]);
+    out[0] = e;
+    out[1] = m;
+    out[2] = dp;
+  }
+}
+void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb, const double* Fa,
+                       const double* Fb, const double* Ea, const double* Eb, const double* Pa_old,
+                       const double* Pb_old, double* out, cudaStream_t s) {
+  scf_reduce_kernel<<<1, 1024, 0, s>>>(n, uhf, H, Pa, Pb, Fa, Fb, Ea, Eb, Pa_old, Pb_old, out);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+__global__ void scale_columns_kernel(int n, double* U, const double* s) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || j >= n) return;
+  U[(size_t)j * n + i] *= rsqrt(s[j]);  // column-major: column j
+}
+void launch_scale_columns(int n, double* U, const double* s, cudaStream_t st) {
+  dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
+  scale_columns_kernel<<<g, b, 0, st>>>(n, U, s);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// dmax[a][b] = max |A|, |B| over the (a, b) shell block.
+__global__ void dmax_kernel(int ns, const int* __restrict__ bf_off, const int* __restrict__ nfun, int nbf,
+                            const double* __restrict__ A, const double* __restrict__ B,
+                            const double* __restrict__ Cc, float* __restrict__ dm) {
+  const int a = blockIdx.y * blockDim.y + threadIdx.y, b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= ns || b >= ns) return;
+  double m = 0.0;
+  for (int i = 0; i < nfun[a]; ++i)
+    for (int j = 0; j < nfun[b]; ++j) {
+      const size_t k = (size_t)(bf_off[a] + i) * nbf + bf_off[b] + j;
+      m = fmax(m, fabs(A[k]));
+      if (B) m = fmax(m, fabs(B[k]));
+      if (Cc) m = fmax(m, fabs(Cc[k]));
+    }
+  dm[(size_t)a * ns + b] = (float)m;
+}
+void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
+                 const double* C, float* dmax, cudaStream_t s) {
+  dim3 b(16, 16), g((ns + 15) / 16, (ns + 15) / 16);
+  dmax_kernel<<<g, b, 0, s>>>(ns, bf_off, nfun, nbf, A, B, C, dmax);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+void launch_zero(void* p, size_t bytes, cudaStream_t s) { PF_CUDA(cudaMemsetAsync(p, 0, bytes, s)); }
+
+// ===========================================================================
+// FP64 / FP32 FMA throughput probe: independent FMA chains per thread.
+// ===========================================================================
+template <typename R>
+__global__ void fma_probe_kernel(R* out, int iters, R a, R b) {
+  R x0 = threadIdx.x * (R)1e-3, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6,
+    x7 = x0 + 7;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      x0 = x0 * a + b; x1 = x1 * a + b; x2 = x2 * a + b; x3 = x3 * a + b;
+      x4 = x4 * a + b; x5 = x5 * a + b; x6 = x6 * a + b; x7 = x7 * a + b;
+    }
+  }
+  R s = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+  if (s == (R)-12345.678) out[0] = s;  // keep the chains alive
+}
+
+double probe_fp64(int device, double* fp32) {
+  PF_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  PF_CUDA(cudaGetDeviceProperties(&prop, device));
+  double* d = nullptr;
+  PF_CUDA(cudaMalloc(&d, 64));
+  cudaEvent_t e0, e1;
+  PF_CUDA(cudaEventCreate(&e0));
+  PF_CUDA(cudaEventCreate(&e1));
+  const int blocks = prop.multiProcessorCount * 8, threads = 256, iters = 4096;
+  double best64 = 0.0, best32 = 0.0;
+  for (int rep = 0; rep < 4; ++rep) {
+    PF_CUDA(cudaEventRecord(e0));
+    fma_probe_kernel<double><<<blocks, threads>>>(d, iters, 0.999999, 1e-7);
+    PF_CUDA(cudaEventRecord(e1));
+    PF_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    if (rep > 0) best64 = std::max(best64, flops / (ms * 1e-3) / 1e9);
+    PF_CUDA(cudaEventRecord(e0));
+    fma_probe_kernel<float><<<blocks, threads>>>(reinterpret_cast<float*>(d), iters * 2, 0.999999f, 1e-7f);
+    PF_CUDA(cudaEventRecord(e1));
+    PF_CUDA(cudaEventSynchronize(e1));
+    PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (rep > 0) best32 = std::max(best32, 2.0 * flops / (ms * 1e-3) / 1e9);
+  }
+  PF_CUDA(cudaEventDestroy(e0));
+  PF_CUDA(cudaEventDestroy(e1));
+  PF_CUDA(cudaFree(d));
+  if (fp32) *fp32 = best32;
+  return best64;
+}
+
+}  // namespace pyfacc
+
+namespace pyfacc {
+
+// ---------------------------------------------------------------------------
+// Algorithmic flop counts (from the generated class routines)
+// ---------------------------------------------------------------------------
+const ClassFlops& class_flops(int qc) {
+  using C0 = EriClass<double, 0, 0, 0, 0>;
+  using C1 = EriClass<double, 1, 0, 0, 0>;
+  using C2 = EriClass<double, 1, 0, 1, 0>;
+  using C3 = EriClass<double, 1, 1, 0, 0>;
+  using C4 = EriClass<double, 1, 1, 1, 0>;
+  using C5 = EriClass<double, 1, 1, 1, 1>;
+  static const ClassFlops tab[NQCLASS] = {
+      {C0::L, C0::NOUT, C0::VRR_FLOPS, C0::HRR_FLOPS, C0::GRAD_FLOPS},
+      {C1::L, C1::NOUT, C1::VRR_FLOPS, C1::HRR_FLOPS, C1::GRAD_FLOPS},
+      {C2::L, C2::NOUT, C2::VRR_FLOPS, C2::HRR_FLOPS, C2::GRAD_FLOPS},
+      {C3::L, C3::NOUT, C3::VRR_FLOPS, C3::HRR_FLOPS, C3::GRAD_FLOPS},
+      {C4::L, C4::NOUT, C4::VRR_FLOPS, C4::HRR_FLOPS, C4::GRAD_FLOPS},
+      {C5::L, C5::NOUT, C5::VRR_FLOPS, C5::HRR_FLOPS, C5::GRAD_FLOPS},
+  };
+  return tab[qc];
+}
+
+// Per primitive quartet outside the VRR: P-Q (3), T (6), prefactor (2),
+// zeta/rho/W terms (12), Boys (Taylor 2*8 + downward recursion 4L), I_m (L+1).
+double prim_overhead_flops(int qc, bool) {
+  const int L = class_flops(qc).L;
+  return 3 + 6 + 2 + 12 + 16 + 4 * L + (L + 1);
+}
+
+// Digestion per contracted quartet: J (4 flops per integral) and K (8 per
+// integral and exchange density).
+double digest_flops(int qc, int nk) { return (double)class_flops(qc).nout * (4.0 + 8.0 * nk); }
+
+}  // namespace pyfacc

@@ -1,0 +1,509 @@
+// SCF step of the B200 engine: Fock builds, DIIS, diagonalisation, density,
+// energy and the analytic gradient (see engine.cpp for the overview).
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "engine.h"
+#include "system.h"
+
+namespace pyfacc {
+
+#define PF_CUBLAS(x)                                                                    \
+  do {                                                                                  \
+    cublasStatus_t s_ = (x);                                                            \
+    if (s_ != CUBLAS_STATUS_SUCCESS)                                                    \
+      throw Error(PYFACC_ERR_CUDA, std::string(#x) + ": cuBLAS status " + std::to_string((int)s_)); \
+  } while (0)
+#define PF_CUSOLVER(x)                                                                  \
+  do {                                                                                  \
+    cusolverStatus_t s_ = (x);                                                          \
+    if (s_ != CUSOLVER_STATUS_SUCCESS)                                                  \
+      throw Error(PYFACC_ERR_CUDA, std::string(#x) + ": cuSOLVER status " + std::to_string((int)s_)); \
+  } while (0)
+
+float System::elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  PF_CUDA(cudaEventElapsedTime(&ms, a, b));
+  return ms;
+}
+
+void System::one_electron() {
+  OneEArgs a;
+  a.natoms = natoms;
+  a.atoms = atoms_dev;
+  a.boys_mode = opt.boys_mode;
+  a.S = S;
+  a.T = T;
+  a.V = Vm;
+  a.nbf = nbf;
+  launch_one_electron(shd, n1e, pairs1e, a, stream);
+  launch_axpby((long long)nbf * nbf, 1.0, T, 0.0, H, stream);
+  launch_axpby((long long)nbf * nbf, 1.0, Vm, 1.0, H, stream);
+  one_e_done = true;
+}
+
+// One Fock build: zero the outputs, shell-block density maxima for the
+// density-weighted Schwarz test, the six class kernels (FP64 task lists, or
+// the FP64 and FP32 halves of the mixed lists), then J = Jh + Jh^T.
+void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision) {
+  const size_t n2 = (size_t)nbf * nbf;
+  launch_zero(Jo, n2 * sizeof(double), stream);
+  for (int k = 0; k < nk; ++k) launch_zero(Ko[k], n2 * sizeof(double), stream);
+  launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Dj, Dk[0], nk > 1 ? Dk[1] : nullptr, dmax, stream);
+  JkArgs a;
+  a.Dj = Dj;
+  a.Dk0 = Dk[0];
+  a.Dk1 = nk > 1 ? Dk[1] : Dk[0];
+  a.J = Jo;
+  a.K0 = Ko[0];
+  a.K1 = nk > 1 ? Ko[1] : Ko[0];
+  a.dmax = (opt.schwarz_thresh > 0) ? dmax : nullptr;
+  a.ns_ld = ns;
+  a.thresh = opt.schwarz_thresh;
+  a.stats = stats_dev;
+  for (int bc = NCLASS - 1; bc >= 0; --bc)
+    for (int kc = bc; kc >= 0; --kc) {
+      if (precision == PYFACC_PRECISION_MIXED) {
+        launch_jk(pd, tasks[bc][kc][1], bc, kc, false, nk, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, nk, a, num_sms, stream);
+      } else {
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, nk, a, num_sms, stream);
+      }
+    }
+  launch_symmetrize_add(nbf, Jo, stream);
+  for (int k = 0; k < nk; ++k) launch_symmetrize_add(nbf, Ko[k], stream);
+  st.n_fock++;
+}
+
+void System::eri_tensor(double* eri) {
+  const size_t n = nbf;
+  launch_zero(eri, n * n * n * n * sizeof(double), stream);
+  // unscreened canonical quartets: use a system-local zero-threshold task set
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) launch_eri_tensor(pd, tasks[bc][kc][0], bc, kc, nbf, eri, stream);
+}
+
+// X = U s^-1/2 from S (la.f90:28-57).  cuSOLVER works column-major; S is
+// symmetric, and U comes back with eigenvector j in column j.
+void System::orthogonalizer() {
+  const size_t n2 = (size_t)nbf * nbf;
+  PF_CUDA(cudaMemcpyAsync(X, S, n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  PF_CUSOLVER(cusolverDnDsyevd(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, X, nbf, eps_dev,
+                               syev_work.as<double>(), syev_lwork, info_dev));
+  std::vector<double> s(nbf);
+  int info = 0;
+  PF_CUDA(cudaMemcpyAsync(s.data(), eps_dev, nbf * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaMemcpyAsync(&info, info_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  if (info != 0) throw Error(PYFACC_ERR_CUDA, "overlap diagonalisation failed");
+  if (!(s[0] > 0.0)) throw Error(PYFACC_ERR_LINDEP, "overlap matrix is not positive definite");
+  if (s[0] < 1.0e-8 && opt.verbose)
+    std::fprintf(stderr, "pyfacc: small overlap eigenvalue %g\n", s[0]);  // la.f90:40-44
+  launch_scale_columns(nbf, X, eps_dev, stream);
+}
+
+// F' = X^T F X, eigenpairs, C = X C' (all column-major).
+void System::diagonalize(const double* Fm, double* C, double* eps) {
+  const double one = 1.0, zero = 0.0;
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, W2, nbf));
+  PF_CUSOLVER(cusolverDnDsyevd(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W2, nbf, eps,
+                               syev_work.as<double>(), syev_lwork, info_dev));
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W2, nbf, &zero, C, nbf));
+}
+
+// P = scale * C_occ C_occ^T
+void System::density_from(const double* C, int nocc, double scale, double* Pm) {
+  const double zero = 0.0;
+  if (nocc <= 0) {
+    launch_zero(Pm, (size_t)nbf * nbf * sizeof(double), stream);
+    return;
+  }
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nocc, &scale, C, nbf, C, nbf, &zero, Pm, nbf));
+}
+
+static bool solve_small(int m, std::vector<double> A, std::vector<double> b, std::vector<double>& x) {
+  // Gaussian elimination with partial pivoting on an m x m system.
+  for (int c = 0; c < m; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < m; ++r)
+      if (std::fabs(A[r * m + c]) > std::fabs(A[piv * m + c])) piv = r;
+    if (std::fabs(A[piv * m + c]) < 1e-300) return false;
+    if (piv != c) {
+      for (int k = 0; k < m; ++k) std::swap(A[c * m + k], A[piv * m + k]);
+      std::swap(b[c], b[piv]);
+    }
+    for (int r = c + 1; r < m; ++r) {
+      const double f = A[r * m + c] / A[c * m + c];
+      for (int k = c; k < m; ++k) A[r * m + k] -= f * A[c * m + k];
+      b[r] -= f * b[c];
+    }
+  }
+  x.assign(m, 0.0);
+  for (int r = m - 1; r >= 0; --r) {
+    double s = b[r];
+    for (int k = r + 1; k < m; ++k) s -= A[r * m + k] * x[k];
+    x[r] = s / A[r * m + r];
+  }
+  for (double v : x)
+    if (!std::isfinite(v)) return false;
+  return true;
+}
+
+void System::run_scf() {
+  const size_t n2 = (size_t)nbf * nbf;
+  const int nsp = uhf ? 2 : 1;
+  const int nocc[2] = {uhf ? nalpha : (nalpha + nbeta + 1) / 2, uhf ? nbeta : 0};  // rscf.f90:54-55
+  const double pscale = uhf ? 1.0 : 2.0;
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+  const bool incremental = opt.incremental < 0 ? mixed : (opt.incremental != 0);
+  st = ScfState();
+  PF_CUDA(cudaMemsetAsync(stats_dev, 0, sizeof(JkStats), stream));
+  cudaEvent_t t0, t1, a0, a1;
+  PF_CUDA(cudaEventCreate(&t0));
+  PF_CUDA(cudaEventCreate(&t1));
+  PF_CUDA(cudaEventCreate(&a0));
+  PF_CUDA(cudaEventCreate(&a1));
+  PF_CUDA(cudaEventRecord(t0, stream));
+  PF_CUDA(cudaEventRecord(a0, stream));
+  one_electron();
+  PF_CUDA(cudaEventRecord(a1, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  st.ms_1e = elapsed(a0, a1);
+  orthogonalizer();
+  // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144)
+  diagonalize(H, Cm[0], eps_dev);
+  for (int s = 0; s < nsp; ++s) {
+    if (s == 1) PF_CUDA(cudaMemcpyAsync(Cm[1], Cm[0], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    density_from(Cm[s], nocc[s], pscale, P[s]);
+  }
+  for (int s = 0; s < nsp; ++s) launch_zero(Pbuilt[s], n2 * sizeof(double), stream);
+  launch_zero(J, n2 * sizeof(double), stream);
+  for (int s = 0; s < nsp; ++s) launch_zero(K[s], n2 * sizeof(double), stream);
+
+  const int ndiis = std::max(opt.diis_size, 0);
+  for (int k = 0; k < ndiis; ++k) {
+    launch_zero(diis_F[k], 2 * n2 * sizeof(double), stream);
+    launch_zero(diis_E[k], 2 * n2 * sizeof(double), stream);
+  }
+  int nhist = 0, head = 0;
+  std::vector<double> Bm;  // DIIS overlap matrix of the stored error vectors
+  const int cap = std::max(ndiis, 1);
+  Bm.assign(cap * cap, 0.0);
+  std::vector<int> slot_age(cap, -1);
+  double E_old = 0.0;
+  double ms_fock = 0.0, ms_diag = 0.0;
+  int since_full = 0;
+  const double* Pspin[2] = {P[0], P[1]};
+  for (int it = 1; it <= opt.max_iter; ++it) {
+    st.n_iter = it;
+    // ---- Fock build
+    PF_CUDA(cudaEventRecord(a0, stream));
+    const bool full = !incremental || it == 1 || since_full + 1 >= std::max(opt.rebuild_every, 1);
+    double* Kp[2] = {K[0], K[1]};
+    if (full) {
+      if (uhf) {
+        launch_axpby((long long)n2, 1.0, P[0], 0.0, W3, stream);
+        launch_axpby((long long)n2, 1.0, P[1], 1.0, W3, stream);
+        jk(W3, 2, Pspin, J, Kp, opt.precision);
+      } else {
+        jk(P[0], 1, Pspin, J, Kp, opt.precision);
+      }
+      since_full = 0;
+    } else {
+      // dP = P - P_built; J += J[dP], K += K[dP]
+      double* dP[2] = {Err[0], Err[1]};
+      for (int s = 0; s < nsp; ++s) {
+        launch_axpby((long long)n2, 1.0, P[s], 0.0, dP[s], stream);
+        launch_axpby((long long)n2, -1.0, Pbuilt[s], 1.0, dP[s], stream);
+      }
+      double* dK[2] = {W2, W3};
+      const double* dPc[2] = {dP[0], dP[1]};
+      if (uhf) {
+        launch_axpby((long long)n2, 1.0, dP[0], 0.0, Wm, stream);
+        launch_axpby((long long)n2, 1.0, dP[1], 1.0, Wm, stream);
+        jk(Wm, 2, dPc, W1, dK, opt.precision);
+      } else {
+        jk(dP[0], 1, dPc, W1, dK, opt.precision);
+      }
+      launch_axpby((long long)n2, 1.0, W1, 1.0, J, stream);
+      for (int s = 0; s < nsp; ++s) launch_axpby((long long)n2, 1.0, dK[s], 1.0, K[s], stream);
+      since_full++;
+    }
+    for (int s = 0; s < nsp; ++s)
+      PF_CUDA(cudaMemcpyAsync(Pbuilt[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    for (int s = 0; s < nsp; ++s) launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
+    PF_CUDA(cudaEventRecord(a1, stream));
+    // ---- DIIS error X^T (F P S - S P F) X and energy
+    const double one = 1.0, zero = 0.0, mone = -1.0;
+    for (int s = 0; s < nsp; ++s) {
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, F[s], nbf, P[s], nbf, &zero, W1, nbf));
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, W1, nbf, S, nbf, &zero, W2, nbf));
+      PF_CUBLAS(cublasDgeam(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, &one, W2, nbf, &mone, W2, nbf, W1, nbf));
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, W1, nbf, X, nbf, &zero, W2, nbf));
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W2, nbf, &zero, Err[s], nbf));
+    }
+    launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Err[0],
+                      uhf ? Err[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, stream);
+    // ---- DIIS bookkeeping: store F and the error vector, overlaps with the stored errors
+    int slot = -1;
+    if (ndiis > 0) {
+      slot = head;
+      head = (head + 1) % ndiis;
+      for (int s = 0; s < nsp; ++s) {
+        PF_CUDA(cudaMemcpyAsync(diis_F[slot] + s * n2, F[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        PF_CUDA(cudaMemcpyAsync(diis_E[slot] + s * n2, Err[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+      }
+      std::vector<const double*> ys(ndiis);
+      for (int k = 0; k < ndiis; ++k) ys[k] = diis_E[k];
+      PF_CUDA(cudaMemcpyAsync(ptrs_dev, ys.data(), ndiis * sizeof(double*), cudaMemcpyHostToDevice, stream));
+      launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, stream);
+    }
+    double red[8 + 64];
+    PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    ms_fock += elapsed(a0, a1);
+    const double E = 0.5 * red[0];
+    const double err = red[1];
+    const double dD = std::sqrt(red[2]);
+    const double dE = std::fabs(E - E_old);
+    st.last_de = dE;
+    st.last_err = err;
+    st.e_elec = E;
+    st.energy = E + e_nuc;
+    if (opt.verbose)
+      std::fprintf(stderr, "pyfacc iter %3d  E = %.12f  dE = %.3e  err = %.3e  |dD| = %.3e\n", it, E + e_nuc, dE,
+                   err, dD);
+    bool conv = dE < opt.eps_energy && err < opt.eps_diis;
+    if (opt.eps_density > 0) conv = conv && it > 1 && dD < opt.eps_density;
+    if (conv) {
+      st.converged = true;
+      break;
+    }
+    E_old = E;
+    for (int s = 0; s < nsp; ++s)
+      PF_CUDA(cudaMemcpyAsync(Pold[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    // ---- extrapolate
+    const double* Fuse[2] = {F[0], F[1]};
+    if (ndiis > 0) {
+      slot_age[slot] = it;
+      for (int k = 0; k < ndiis; ++k) {
+        Bm[slot * cap + k] = red[8 + k];
+        Bm[k * cap + slot] = red[8 + k];
+      }
+      nhist = std::min(nhist + 1, ndiis);
+      if (nhist >= 2) {
+        std::vector<int> use;
+        for (int k = 0; k < ndiis; ++k)
+          if (slot_age[k] >= 0) use.push_back(k);
+        // drop the oldest vectors until the system is solvable
+        while (use.size() >= 2) {
+          const int m = (int)use.size();
+          std::vector<double> A((m + 1) * (m + 1), 0.0), b(m + 1, 0.0), x;
+          double scl = 0.0;
+          for (int i = 0; i < m; ++i) scl = std::max(scl, std::fabs(Bm[use[i] * cap + use[i]]));
+          scl = scl > 0 ? 1.0 / scl : 1.0;
+          for (int i = 0; i < m; ++i) {
+            for (int j = 0; j < m; ++j) A[i * (m + 1) + j] = Bm[use[i] * cap + use[j]] * scl;
+            A[i * (m + 1) + m] = -1.0;
+            A[m * (m + 1) + i] = -1.0;
+          }
+          b[m] = -1.0;
+          if (solve_small(m + 1, A, b, x)) {
+            // F_diis = sum c_i F_i  (into W3 / Wm as the stacked spins)
+            double* Fd = W3;
+            launch_zero(Fd, n2 * sizeof(double), stream);
+            if (uhf) launch_zero(Wm, n2 * sizeof(double), stream);
+            for (int i = 0; i < m; ++i) {
+              launch_axpby((long long)n2, x[i], diis_F[use[i]], 1.0, Fd, stream);
+              if (uhf) launch_axpby((long long)n2, x[i], diis_F[use[i]] + n2, 1.0, Wm, stream);
+            }
+            Fuse[0] = Fd;
+            Fuse[1] = Wm;
+            break;
+          }
+          int oldest = 0;
+          for (int i = 1; i < (int)use.size(); ++i)
+            if (slot_age[use[i]] < slot_age[use[oldest]]) oldest = i;
+          slot_age[use[oldest]] = -1;
+          use.erase(use.begin() + oldest);
+        }
+      }
+    }
+    // ---- diagonalise and rebuild the density
+    PF_CUDA(cudaEventRecord(a0, stream));
+    for (int s = 0; s < nsp; ++s) {
+      diagonalize(Fuse[s], Cm[s], eps_dev + s * nbf);
+      density_from(Cm[s], nocc[s], pscale, P[s]);
+    }
+    PF_CUDA(cudaEventRecord(a1, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    ms_diag += elapsed(a0, a1);
+  }
+  // orbitals of the final Fock matrix (for W and the outputs)
+  for (int s = 0; s < nsp; ++s) diagonalize(F[s], Cm[s], eps_dev + s * nbf);
+  PF_CUDA(cudaEventRecord(t1, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  st.ms_total = elapsed(t0, t1);
+  st.ms_fock = ms_fock;
+  st.ms_diag = ms_diag;
+  JkStats js;
+  PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
+  st.quartets[0] = st.quartets[1] = 0;
+  st.flops_fock = 0.0;
+  const int nk = uhf ? 2 : 1;
+  for (int p = 0; p < 2; ++p)
+    for (int q = 0; q < NQCLASS; ++q) {
+      st.quartets[p] += js.quartets[p][q];
+      const ClassFlops& cf = class_flops(q);
+      st.flops_fock += (double)js.prims[p][q] * (cf.vrr + prim_overhead_flops(q, p == 1)) +
+                       (double)js.quartets[p][q] * (cf.hrr + digest_flops(q, nk));
+    }
+  st.done = true;
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  cudaEventDestroy(a0);
+  cudaEventDestroy(a1);
+}
+
+// Analytic gradient of the converged SCF:
+//   dE/dR = sum P dH - sum W dS + 1/2 sum Gamma d(mn|ls) + dV_nn
+void System::gradient(double* g_host) {
+  if (!st.done) throw Error(PYFACC_ERR_NOT_READY, "gradient requested before the SCF");
+  const size_t n2 = (size_t)nbf * nbf;
+  const double one = 1.0, zero = 0.0;
+  cudaEvent_t a0, a1;
+  PF_CUDA(cudaEventCreate(&a0));
+  PF_CUDA(cudaEventCreate(&a1));
+  PF_CUDA(cudaEventRecord(a0, stream));
+  // W = sum_s sum_occ eps_i c_i c_i^T (x2 for RHF)
+  const int nsp = uhf ? 2 : 1;
+  const int nocc[2] = {uhf ? nalpha : (nalpha + nbeta + 1) / 2, uhf ? nbeta : 0};
+  launch_zero(Wm, n2 * sizeof(double), stream);
+  for (int s = 0; s < nsp; ++s) {
+    if (nocc[s] <= 0) continue;
+    PF_CUDA(cudaMemcpyAsync(W1, Cm[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    PF_CUBLAS(cublasDdgmm(cublas, CUBLAS_SIDE_RIGHT, nbf, nocc[s], Cm[s], nbf, eps_dev + s * nbf, 1, W1, nbf));
+    const double f = uhf ? 1.0 : 2.0;
+    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nocc[s], &f, W1, nbf, Cm[s], nbf, &one, Wm, nbf));
+  }
+  (void)zero;
+  // total density and spin densities of the final orbitals
+  double* Pt = W2;
+  double* Ps[2] = {Pbuilt[0], Pbuilt[1]};
+  if (uhf) {
+    density_from(Cm[0], nocc[0], 1.0, Ps[0]);
+    density_from(Cm[1], nocc[1], 1.0, Ps[1]);
+    launch_axpby((long long)n2, 1.0, Ps[0], 0.0, Pt, stream);
+    launch_axpby((long long)n2, 1.0, Ps[1], 1.0, Pt, stream);
+  } else {
+    density_from(Cm[0], nocc[0], 2.0, Pt);
+  }
+  launch_zero(grad_dev, 3 * natoms * sizeof(double), stream);
+  OneEGradArgs g1;
+  g1.natoms = natoms;
+  g1.atoms = atoms_dev;
+  g1.boys_mode = opt.boys_mode;
+  g1.P = Pt;
+  g1.W = Wm;
+  g1.nbf = nbf;
+  g1.grad = grad_dev;
+  launch_grad1e(shd, n1e, pairs1e, g1, stream);
+  launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Pt, nullptr, nullptr, dmax, stream);
+  GradArgs g2;
+  g2.Pt = Pt;
+  g2.Pa = uhf ? Ps[0] : Pt;
+  g2.Pb = uhf ? Ps[1] : Pt;
+  g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
+  g2.ns_ld = ns;
+  g2.thresh = opt.schwarz_thresh;
+  g2.uhf = uhf ? 1 : 0;
+  g2.grad = grad_dev;
+  st.flops_grad = 0.0;
+  for (int bc = NCLASS - 1; bc >= 0; --bc)
+    for (int kc = bc; kc >= 0; --kc) {
+      launch_grad2e(pd, tasks[bc][kc][0], bc, kc, g2, num_sms, stream);
+      const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
+      // every pair of STO-nG shells has K^2 primitive pairs
+      const double k2 = basis.shells.empty() ? 1.0 : (double)basis.shells[0].ex.size() * basis.shells[0].ex.size();
+      st.flops_grad += (double)tasks[bc][kc][0].nquartets * k2 * k2 *
+                       (class_flops(qc).grad + prim_overhead_flops(qc, false));
+    }
+  PF_CUDA(cudaEventRecord(a1, stream));
+  std::vector<double> g(3 * natoms, 0.0);
+  PF_CUDA(cudaMemcpyAsync(g.data(), grad_dev, 3 * natoms * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  st.ms_grad = elapsed(a0, a1);
+  nuclear_repulsion_gradient(g.data());
+  grad_host = g;
+  if (g_host) std::memcpy(g_host, g.data(), g.size() * sizeof(double));
+  cudaEventDestroy(a0);
+  cudaEventDestroy(a1);
+}
+
+static void copy_out(cudaStream_t s, double* host, const double* dev, size_t n) {
+  if (host) PF_CUDA(cudaMemcpyAsync(host, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+}
+
+// Device matrices are symmetric (layout-free) except C, which is
+// column-major (orbital j = column j) and is returned as such.
+void System::fill_result(pyfacc_result* r) {
+  const size_t n2 = (size_t)nbf * nbf;
+  r->energy = st.energy;
+  r->e_elec = st.e_elec;
+  r->e_nuc = e_nuc;
+  r->converged = st.converged ? 1 : 0;
+  r->n_iter = st.n_iter;
+  r->scf_type = uhf ? PYFACC_SCF_UHF : PYFACC_SCF_RHF;
+  r->nbf = nbf;
+  r->nshell = ns;
+  r->n_fock_builds = st.n_fock;
+  r->last_delta_e = st.last_de;
+  r->last_diis_error = st.last_err;
+  copy_out(stream, r->S, S, n2);
+  copy_out(stream, r->T, T, n2);
+  copy_out(stream, r->V, Vm, n2);
+  if (r->P) {
+    if (uhf) {
+      launch_axpby((long long)n2, 1.0, P[0], 0.0, W1, stream);
+      launch_axpby((long long)n2, 1.0, P[1], 1.0, W1, stream);
+      copy_out(stream, r->P, W1, n2);
+    } else {
+      copy_out(stream, r->P, P[0], n2);
+    }
+  }
+  copy_out(stream, r->C_alpha, Cm[0], n2);
+  copy_out(stream, r->C_beta, Cm[uhf ? 1 : 0], n2);
+  copy_out(stream, r->eps_alpha, eps_dev, nbf);
+  copy_out(stream, r->eps_beta, eps_dev + (uhf ? nbf : 0), nbf);
+  PF_CUDA(cudaStreamSynchronize(stream));
+  if (r->gradient && !grad_host.empty()) std::memcpy(r->gradient, grad_host.data(), grad_host.size() * sizeof(double));
+  r->ms_total = st.ms_total;
+  r->ms_one_electron = st.ms_1e;
+  r->ms_fock = st.ms_fock;
+  r->ms_diag = st.ms_diag;
+  r->ms_gradient = st.ms_grad;
+  r->quartets_fp64 = (long long)st.quartets[0];
+  r->quartets_fp32 = (long long)st.quartets[1];
+  r->flops_fock = st.flops_fock;
+  r->flops_gradient = st.flops_grad;
+}
+
+void System::set_coords(const double* coords) {
+  xyz.assign(coords, coords + 3 * natoms);
+  for (auto& sh : basis.shells)
+    for (int x = 0; x < 3; ++x) sh.c[x] = xyz[3 * sh.atom + x];
+  e_nuc = nuclear_repulsion();
+  upload_shells();
+  build_pairs();
+  st = ScfState();
+  one_e_done = false;
+  grad_host.clear();
+}
+
+}  // namespace pyfacc

@@ -1,0 +1,110 @@
+// The opaque pyfacc_system of the C ABI: one molecule resident on one GPU.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace pyfacc {
+
+struct ScfState {
+  bool done = false;
+  bool converged = false;
+  int n_iter = 0;
+  int n_fock = 0;
+  double energy = 0.0, e_elec = 0.0;
+  double last_de = 0.0, last_err = 0.0;
+  double ms_total = 0, ms_1e = 0, ms_fock = 0, ms_diag = 0, ms_grad = 0;
+  unsigned long long quartets[2] = {0, 0};
+  double flops_fock = 0.0, flops_grad = 0.0;
+};
+
+struct System {
+  System(const pyfacc_molecule& m, const pyfacc_options& o);
+  ~System();
+  System(const System&) = delete;
+  System& operator=(const System&) = delete;
+
+  // ---- configuration and molecule
+  pyfacc_options opt;
+  int device = 0, num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int natoms = 0, charge = 0, nalpha = 0, nbeta = 0;
+  bool uhf = false;
+  std::vector<int> Z;
+  std::vector<double> xyz;
+  std::vector<std::string> species;
+  std::string basis_name, basis_file;
+  Basis basis;
+  int nbf = 0, ns = 0;
+  double e_nuc = 0.0;
+
+  // ---- device data
+  ShellDev shd;
+  double4* atoms_dev = nullptr;
+  int2* pairs1e = nullptr;
+  int n1e = 0;
+  int* bf_off_dev = nullptr;
+  int* nfun_dev = nullptr;
+  PairData pd;
+  TaskList tasks[NCLASS][NCLASS][3];  // [bra class][ket class][full fp64 | mixed fp64 | mixed fp32]
+  DeviceBuf task_buf;
+  long long quartets_total = 0;
+
+  DeviceBuf mats;
+  double *S = nullptr, *T = nullptr, *Vm = nullptr, *H = nullptr, *X = nullptr;
+  double *F[2] = {nullptr, nullptr}, *J = nullptr, *K[2] = {nullptr, nullptr};
+  double *P[2] = {nullptr, nullptr}, *Pbuilt[2] = {nullptr, nullptr}, *Pold[2] = {nullptr, nullptr};
+  double *W1 = nullptr, *W2 = nullptr, *W3 = nullptr, *Err[2] = {nullptr, nullptr};
+  double *Cm[2] = {nullptr, nullptr}, *Wm = nullptr, *small = nullptr;
+  float* dmax = nullptr;
+  std::vector<double*> diis_F, diis_E;
+  double* eps_dev = nullptr;
+  int* info_dev = nullptr;
+  unsigned long long* stats_dev = nullptr;
+  const double** ptrs_dev = nullptr;
+  double* grad_dev = nullptr;
+  DeviceBuf syev_work;
+  int syev_lwork = 0;
+
+  ScfState st;
+  bool one_e_done = false;
+  std::vector<double> grad_host;
+
+  // ---- setup (engine.cpp)
+  static void spin_electrons(const std::vector<std::string>& sp, int chg, int* na, int* nb);
+  double nuclear_repulsion() const;
+  void nuclear_repulsion_gradient(double* g) const;
+  void upload_shells();
+  void build_pairs();
+  void build_tasks();
+  void alloc_matrices();
+  void release_extra();
+  void set_coords(const double* coords);
+
+  // ---- operations (scf.cpp)
+  void one_electron();
+  // J = J[Dj], K[k] = K[Dk[k]] (precision 0 = fp64, 1 = mixed); screening by
+  // Q_ab Q_cd max|D| with the density(ies) given.
+  void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision);
+  void eri_tensor(double* eri);
+  void orthogonalizer();
+  void diagonalize(const double* Fm, double* C, double* eps);
+  void density_from(const double* C, int nocc, double scale, double* Pm);
+  void run_scf();
+  void gradient(double* g_host);
+  void fill_result(pyfacc_result* r);
+  float elapsed(cudaEvent_t a, cudaEvent_t b);
+};
+
+}  // namespace pyfacc
+
+struct pyfacc_system {
+  pyfacc::System* impl;
+};

@@ -1,0 +1,48 @@
+"""Regenerates the golden fixtures of tests/golden/.
+
+* boys_mpmath.json -- F_m(x) from mpmath's 1F1 (independent of this repo):
+  F_m(x) = 1F1(m+1/2; m+3/2; -x) / (2m+1)
+* h2o_sto3g.json   -- the oracle's converged H2O/STO-3G energy (data/molecules/
+  h2o.xyz) and its V matrix with the reference's trapezoid Boys function.
+
+    python tests/golden/make_golden.py
+"""
+import json
+import os
+import sys
+
+import mpmath
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def boys_values():
+    mpmath.mp.dps = 40
+    xs = [0.0, 1e-12, 1e-7, 1e-3, 0.05, 0.3, 1.0, 2.5, 5.0, 9.9, 14.0, 20.0, 27.5, 35.9, 36.1, 45.0, 80.0,
+          250.0, 1e4, 1e6]
+    out = []
+    for m in range(0, 7):
+        for x in xs:
+            v = mpmath.hyp1f1(m + 0.5, m + 1.5, -x) / (2 * m + 1)
+            out.append([m, x, float(v)])
+    return out
+
+
+def main():
+    with open(os.path.join(HERE, "boys_mpmath.json"), "w") as fh:
+        json.dump({"source": "mpmath.hyp1f1, 40 digits", "values": boys_values()}, fh, indent=0)
+    import oracle as O
+    n, c, s = O.read_xyz(os.path.join(ROOT, "pyfacc-scf_b200", "data", "molecules", "h2o.xyz"))
+    mol = O.molecule(s, c.T, os.path.join(ROOT, "pyfacc-scf_b200", "data", "basis_set", "sto-3g.txt"))
+    r = O.scf(mol)
+    S, T, V = O.one_electron(mol, boys_mode=1)
+    with open(os.path.join(HERE, "h2o_sto3g.json"), "w") as fh:
+        json.dump({"source": "oracle, h2o.xyz, STO-3G, dE<1e-10, DIIS err<1e-8", "energy": r.energy,
+                   "S": S.tolist(), "T": T.tolist(), "V_trapezoid": V.tolist()}, fh)
+
+
+if __name__ == "__main__":
+    main()
