@@ -125,7 +125,7 @@ __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, c
   info1[i] = make_int4(a, b, da.y, db.y);
   info2[i] = pl1[i];
   geom[i] = make_double4(ABx, ABy, ABz, 0.0);
-  const double c0 = 1.4142135623730950488 * 4.1748047532602143;  // sqrt(2) * pi^(5/4)
+  const double c0 = 5.9149671727956128778;  // sqrt(2) * pi^(5/4)
   for (int ka = 0; ka < na; ++ka) {
     const double al = ex[da.w + ka], ca = co[da.w + ka] * prim_norm(da.x, ex[da.w + ka]);
     for (int kb = 0; kb < nb; ++kb) {
