@@ -173,6 +173,21 @@ double pyfacc_probe_fp64_gflops(int device, double *fp32_gflops);
 
 const char *pyfacc_version(void);
 
+/* J[D] and K[D] of one molecule for a density already in device memory,
+ * with no device allocation at all.  No counterpart in the reference: it is
+ * for programs whose device memory belongs to their own allocator (a
+ * framework's caching allocator, a pool sized once at start-up), where a
+ * library cudaMalloc would fail or fragment the pool.  D_dev, J_dev, K_dev are
+ * nbf*nbf device buffers owned by the caller (J, K are overwritten); every
+ * intermediate lives in a 64 MiB array reserved statically on each GPU that
+ * loads the library, and a molecule that needs more is rejected with
+ * PYFACC_ERR_INVALID (pyfacc_last_message() gives the size).  The first call
+ * on a device sets that device up and should precede any stream capture.
+ * Calls share the array; calls from one process are serialised and return
+ * after their kernels finish. */
+int pyfacc_jk_noalloc(const pyfacc_molecule *mol, const char *data_dir, double schwarz_thresh,
+                      const double *D_dev, double *J_dev, double *K_dev);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,10 @@ int run_one(const pyfacc_molecule& m, const pyfacc_options& o, pyfacc_result* r)
 
 }  // namespace
 
+namespace pyfacc {
+void set_last_message(const std::string& m) { g_last_message = m; }
+}  // namespace pyfacc
+
 extern "C" {
 
 const char* pyfacc_version(void) { return "pyfacc-b200 0.1 (sm_100a)"; }

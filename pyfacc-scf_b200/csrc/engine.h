@@ -210,4 +210,7 @@ void launch_zero(void* p, size_t bytes, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
 
+// Detail text returned by pyfacc_last_message() (capi.cpp).
+void set_last_message(const std::string& m);
+
 }  // namespace pyfacc

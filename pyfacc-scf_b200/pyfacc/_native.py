@@ -99,6 +99,7 @@ SIGNATURES = {
     "pyfacc_partition": (c_int, [c_int, P_double, c_int, ctypes.POINTER(c_int)]),
     "pyfacc_probe_fp64_gflops": (c_double, [c_int, P_double]),
     "pyfacc_version": (c_char_p, []),
+    "pyfacc_jk_noalloc": (c_int, [ctypes.POINTER(MoleculeC), c_char_p, c_double, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None
