@@ -180,11 +180,16 @@ void System::upload_shells() {
   bfo[ns] = nbf;
   std::vector<double4> atoms(natoms);
   for (int a = 0; a < natoms; ++a) atoms[a] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], (double)Z[a]);
-  // 1e pair list: (a, b) with a <= b, the upper triangle of S_overlap (overlap.f90:292-329)
-  std::vector<int2> p1;
+  // 1e pair lists: every pair a <= b of the upper triangle of S_overlap
+  // (overlap.f90:292-329), per class, ordered so that l_a >= l_b
+  std::vector<int2> p1[NCLASS];
   for (int a = 0; a < ns; ++a)
-    for (int b = a; b < ns; ++b) p1.push_back(make_int2(a, b));
-  n1e = (int)p1.size();
+    for (int b = a; b < ns; ++b) {
+      int x = a, y = b;
+      if (basis.shells[x].l < basis.shells[y].l) std::swap(x, y);
+      p1[basis.shells[x].l + basis.shells[y].l].push_back(make_int2(x, y));
+    }
+  for (int c = 0; c < NCLASS; ++c) n1e[c] = (int)p1[c].size();
   const size_t nex = std::max<size_t>(ex.size(), 1);
   size_t off = 0;
   auto carve = [&](size_t bytes) {
@@ -194,7 +199,7 @@ void System::upload_shells() {
   };
   const size_t o_cen = carve(ns * sizeof(double4)), o_desc = carve(ns * sizeof(int4)), o_np = carve(ns * sizeof(int)),
                o_ex = carve(nex * sizeof(double)), o_co = carve(nex * sizeof(double)),
-               o_atoms = carve(natoms * sizeof(double4)), o_p1 = carve(n1e * sizeof(int2)),
+               o_atoms = carve(natoms * sizeof(double4)), o_p1 = carve((n1e[0] + n1e[1] + n1e[2] + 3) * sizeof(int2)),
                o_bfo = carve((ns + 1) * sizeof(int)), o_nf = carve(ns * sizeof(int));
   shd.buf.ensure(off);
   char* base = shd.buf.as<char>();
@@ -205,7 +210,9 @@ void System::upload_shells() {
   shd.ex = reinterpret_cast<double*>(base + o_ex);
   shd.co = reinterpret_cast<double*>(base + o_co);
   atoms_dev = reinterpret_cast<double4*>(base + o_atoms);
-  pairs1e = reinterpret_cast<int2*>(base + o_p1);
+  pairs1e[0] = reinterpret_cast<int2*>(base + o_p1);
+  pairs1e[1] = pairs1e[0] + n1e[0];
+  pairs1e[2] = pairs1e[1] + n1e[1];
   bf_off_dev = reinterpret_cast<int*>(base + o_bfo);
   nfun_dev = reinterpret_cast<int*>(base + o_nf);
   PF_CUDA(cudaMemcpyAsync(shd.cen, cen.data(), ns * sizeof(double4), cudaMemcpyHostToDevice, stream));
@@ -214,7 +221,8 @@ void System::upload_shells() {
   PF_CUDA(cudaMemcpyAsync(shd.ex, ex.data(), ex.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(shd.co, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(atoms_dev, atoms.data(), natoms * sizeof(double4), cudaMemcpyHostToDevice, stream));
-  PF_CUDA(cudaMemcpyAsync(pairs1e, p1.data(), n1e * sizeof(int2), cudaMemcpyHostToDevice, stream));
+  for (int c = 0; c < NCLASS; ++c)
+    if (n1e[c]) PF_CUDA(cudaMemcpyAsync(pairs1e[c], p1[c].data(), n1e[c] * sizeof(int2), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(bf_off_dev, bfo.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(nfun_dev, nf.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
@@ -394,7 +402,7 @@ void System::build_tasks() {
 
 void System::alloc_matrices() {
   const size_t n2 = (size_t)nbf * nbf;
-  const int nmat = 24 + 4 * std::max(opt.diis_size, 1);
+  const int nmat = 27 + 4 * std::max(opt.diis_size, 1);
   mats.ensure(nmat * n2 * sizeof(double) + 64 * sizeof(double) + ns * ns * sizeof(float) + 1024);
   double* m = mats.as<double>();
   auto take = [&]() { double* r = m; m += n2; return r; };
@@ -403,12 +411,14 @@ void System::alloc_matrices() {
   P[0] = take(); P[1] = take(); Pbuilt[0] = take(); Pbuilt[1] = take(); Pold[0] = take(); Pold[1] = take();
   W1 = take(); W2 = take(); W3 = take(); Err[0] = take(); Err[1] = take(); Cm[0] = take(); Cm[1] = take();
   Wm = take();
+  Pu[0] = take(); Pu[1] = take(); Pu[2] = take();
   const int nd = std::max(opt.diis_size, 1);
   for (int i = 0; i < nd; ++i) {
     diis_F.push_back(m); m += 2 * n2;
     diis_E.push_back(m); m += 2 * n2;
   }
-  small = m; m += 64;
+  small = m; m += 48;
+  pstate = m; m += 16;
   dmax = reinterpret_cast<float*>(m);
   PF_CUDA(cudaMalloc(&eps_dev, 2 * nbf * sizeof(double)));
   PF_CUDA(cudaMalloc(&info_dev, sizeof(int)));

@@ -181,7 +181,9 @@ struct OneEArgs {
   double* V;
   int nbf;
 };
-void launch_one_electron(const ShellDev& sh, int npair, const int2* pairs, const OneEArgs& a, cudaStream_t s);
+// pairs[c]: the shell pairs (a, b) of class c = l_a + l_b with l_a >= l_b.
+void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEArgs& a,
+                         cudaStream_t s);
 
 struct OneEGradArgs {
   int natoms;
@@ -192,7 +194,8 @@ struct OneEGradArgs {
   int nbf;
   double* grad;
 };
-void launch_grad1e(const ShellDev& sh, int npair, const int2* pairs, const OneEGradArgs& a, cudaStream_t s);
+void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEGradArgs& a,
+                   int num_sms, cudaStream_t s);
 
 // Small dense helpers.
 void launch_symmetrize_add(int n, double* A, cudaStream_t s);             // A = A + A^T
@@ -207,6 +210,10 @@ void launch_scale_columns(int n, double* U, const double* sv, cudaStream_t s);  
 void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
                  const double* C, float* dmax, cudaStream_t s);
 void launch_zero(void* p, size_t bytes, cudaStream_t s);
+// TC2 purification helpers (state: l_min, l_max, Tr X, Tr X^2, converged, steps)
+void launch_gersh(int n, const double* F, double* state, cudaStream_t s);
+void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s);
+void launch_tc2_step(int n, double nocc, double* X, const double* X2, double* state, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
 

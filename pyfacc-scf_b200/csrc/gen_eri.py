@@ -213,13 +213,14 @@ def gen_class(la, lb, lc, ld):
     src.extend(out_lines)
     src.append("    (void)AB; (void)CD;")
     src.append("  }")
-    # --- gradient (primitive level, contracted with gam)
-    em = Emitter()
-    v = Vrr(em, L + 1)
-    h = Hrr(em, lambda e, f: v.V(e, f, 0))
-    ls = [la, lb, lc, ld]
-    g_lines = []
+    # --- gradient (primitive level, contracted with gam), one routine per
+    # centre so that each keeps only its own recursion intermediates live
+    grad_flops = 0
     for ctr in range(3):
+        em = Emitter()
+        v = Vrr(em, L + 1)
+        h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
+        g_lines = []
         for x in range(3):
             up_terms, dn_terms = [], []
             k = 0
@@ -239,25 +240,25 @@ def gen_class(la, lb, lc, ld):
                                 dn_terms.append(f"{cc}gam[{k}] * {h.full(*qd)}")
                             k += 1
             su = em.tmp(" + ".join(up_terms), 2 * len(up_terms) - 1)
-            expr = f"tw[{ctr}] * {su}"
+            expr = f"tw * {su}"
             fl = 2
             if dn_terms:
                 sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
                 expr += f" - {sd}"
                 fl += 1
-            g_lines.append(f"    g[{3 * ctr + x}] += w * ({expr});")
-            em.flops += fl + 1
-    grad_flops = em.flops
-    src.append("  // tw[c] = 2 * exponent of centre c (A, B, C); w = primitive weight")
-    src.append("  __device__ static __forceinline__ void grad(const R* __restrict__ I, const R* __restrict__ PA,")
-    src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
-    src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
-    src.append("      const R* __restrict__ tw, R w, const R* __restrict__ gam, R* __restrict__ g) {")
-    src.extend(em.lines)
-    src.extend(g_lines)
-    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
-    src.append("    (void)AB; (void)CD;")
-    src.append("  }")
+            g_lines.append(f"    g[{x}] += {expr};")
+            em.flops += fl
+        grad_flops += em.flops
+        src.append(f"  // centre {'ABC'[ctr]}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
+        src.append(f"  __device__ static __forceinline__ void grad{'ABC'[ctr]}(const R* __restrict__ I, const R* __restrict__ PA,")
+        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
+        src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+        src.append("      R tw, const R* __restrict__ gam, R* __restrict__ g) {")
+        src.extend(em.lines)
+        src.extend(g_lines)
+        src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+        src.append("    (void)AB; (void)CD;")
+        src.append("  }")
     src.append(f"  static constexpr int VRR_FLOPS = {vrr_flops};")
     src.append(f"  static constexpr int HRR_FLOPS = {hrr_flops};")
     src.append(f"  static constexpr int GRAD_FLOPS = {grad_flops};")
@@ -265,20 +266,141 @@ def gen_class(la, lb, lc, ld):
     return "\n".join(src), dict(tag=tag, L=L, nacc=nacc, nout=nout, vrr=vrr_flops, hrr=hrr_flops, grad=grad_flops)
 
 
+class Vrr1e:
+    """OS recursion for the nuclear attraction of one primitive pair and one
+    nucleus C: [e|A_C|0]^(m) from I_m = pref * F_m(p |PC|^2)."""
+
+    def __init__(self, em: Emitter):
+        self.em = em
+        self.memo = {}
+
+    def V(self, e, m):
+        key = (e, m)
+        if key in self.memo:
+            return self.memo[key]
+        if lsum(e) == 0:
+            r = f"I[{m}]"
+        else:
+            i = first_axis(e)
+            e1 = down(e, i)
+            expr = f"PA[{i}] * {self.V(e1, m)} - PC[{i}] * {self.V(e1, m + 1)}"
+            fl = 3
+            if e1[i] > 0:
+                e2 = down(e1, i)
+                c = f"{e1[i]}.0 * " if e1[i] > 1 else ""
+                expr += f" + {c}o2p * ({self.V(e2, m)} - {self.V(e2, m + 1)})"
+                fl += 3 + (1 if e1[i] > 1 else 0)
+            r = self.em.tmp(expr, fl)
+        self.memo[key] = r
+        return r
+
+
+class Hrr1e:
+    def __init__(self, em: Emitter, base):
+        self.em = em
+        self.base = base
+        self.memo = {}
+
+    def ab(self, a, b):
+        key = (a, b)
+        if key in self.memo:
+            return self.memo[key]
+        if lsum(b) == 0:
+            r = self.base(a)
+        else:
+            i = first_axis(b)
+            r = self.em.tmp(f"{self.ab(up(a, i), down(b, i))} + AB[{i}] * {self.ab(a, down(b, i))}", 2)
+        self.memo[key] = r
+        return r
+
+
+def gen_one_electron(la, lb):
+    """Nuclear attraction (one nucleus) and its density-contracted
+    derivative with respect to the two centres, class (la|lb), la >= lb."""
+    L = la + lb
+    na, nb = len(comps(la)), len(comps(lb))
+    src = [f"template <typename R> struct NucClass<R, {la}, {lb}> {{",
+           f"  static constexpr int L = {L};",
+           f"  static constexpr int NOUT = {na * nb};"]
+    em = Emitter()
+    v = Vrr1e(em)
+    h = Hrr1e(em, lambda a: v.V(a, 0))
+    out = []
+    k = 0
+    for a in comps(la):
+        for b in comps(lb):
+            out.append(f"    out[{k}] += {h.ab(a, b)};")
+            em.flops += 1
+            k += 1
+    vflops = em.flops
+    src.append("  __device__ static __forceinline__ void vint(const R* __restrict__ I, const R* __restrict__ PA,")
+    src.append("      const R* __restrict__ PC, R o2p, const R* __restrict__ AB, R* __restrict__ out) {")
+    src.extend(em.lines)
+    src.extend(out)
+    src.append("    (void)PA; (void)PC; (void)o2p; (void)AB;")
+    src.append("  }")
+    em = Emitter()
+    v = Vrr1e(em)
+    h = Hrr1e(em, lambda a: v.V(a, 0))
+    lines = []
+    for ctr in range(2):
+        for x in range(3):
+            ups, dns = [], []
+            k = 0
+            for a in comps(la):
+                for b in comps(lb):
+                    q = [a, b]
+                    qu = list(q)
+                    qu[ctr] = up(q[ctr], x)
+                    ups.append(f"dens[{k}] * {h.ab(*qu)}")
+                    cnt = q[ctr][x]
+                    if cnt > 0:
+                        qd = list(q)
+                        qd[ctr] = down(q[ctr], x)
+                        cc = f"{cnt}.0 * " if cnt > 1 else ""
+                        dns.append(f"{cc}dens[{k}] * {h.ab(*qd)}")
+                    k += 1
+            su = em.tmp(" + ".join(ups), 2 * len(ups) - 1)
+            expr = f"tw[{ctr}] * {su}"
+            if dns:
+                sd = em.tmp(" + ".join(dns), 2 * len(dns) - 1)
+                expr += f" - {sd}"
+            lines.append(f"    g[{3 * ctr + x}] += {expr};")
+            em.flops += 3
+    gflops = em.flops
+    src.append("  // g[0..2] += d/dA, g[3..5] += d/dB of sum_ab dens_ab (a|A_C|b); tw = {2 alpha, 2 beta}")
+    src.append("  __device__ static __forceinline__ void vgrad(const R* __restrict__ I, const R* __restrict__ PA,")
+    src.append("      const R* __restrict__ PC, R o2p, const R* __restrict__ AB, const R* __restrict__ tw,")
+    src.append("      const R* __restrict__ dens, R* __restrict__ g) {")
+    src.extend(em.lines)
+    src.extend(lines)
+    src.append("    (void)PA; (void)PC; (void)o2p; (void)AB;")
+    src.append("  }")
+    src.append(f"  static constexpr int VINT_FLOPS = {vflops};")
+    src.append(f"  static constexpr int VGRAD_FLOPS = {gflops};")
+    src.append("};")
+    return "\n".join(src)
+
+
 CLASSES = [(0, 0, 0, 0), (1, 0, 0, 0), (1, 0, 1, 0), (1, 1, 0, 0), (1, 1, 1, 0), (1, 1, 1, 1)]
+ONE_E_CLASSES = [(0, 0), (1, 0), (1, 1)]
 
 
 def generate() -> str:
     parts = ["// Generated by gen_eri.py -- do not edit by hand.",
              "// Obara-Saika VRR / Head-Gordon-Pople HRR for s/p shell quartets.",
              "#pragma once", "",
-             "template <typename R, int LA, int LB, int LC, int LD> struct EriClass;", ""]
+             "template <typename R, int LA, int LB, int LC, int LD> struct EriClass;",
+             "template <typename R, int LA, int LB> struct NucClass;", ""]
     table = []
     for cl in CLASSES:
         s, info = gen_class(*cl)
         parts.append(s)
         parts.append("")
         table.append(info)
+    for cl in ONE_E_CLASSES:
+        parts.append(gen_one_electron(*cl))
+        parts.append("")
     parts.append("// class | L | accumulators | outputs | vrr flops/prim | hrr flops/contr | grad flops/prim")
     for t in table:
         parts.append(f"//  {t['tag']}  | {t['L']} | {t['nacc']:3d} | {t['nout']:3d} | {t['vrr']:5d} | {t['hrr']:4d} | {t['grad']:6d}")

@@ -611,8 +611,11 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
           const double PA[3] = {b2.x, b2.y, b2.z};
           PrimGeo<double> pg;
           prim_setup<double, C::L + 1>(b0, b1, k0, k1, pg);
-          const double tw[3] = {2.0 * b0.w, 2.0 * (b0.x - b0.w), 2.0 * k0.w};
-          C::grad(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, tw, 1.0, gam, g);
+          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * b0.w, gam, g);
+          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * (b0.x - b0.w),
+                   gam, g + 3);
+          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * k0.w, gam,
+                   g + 6);
         }
       }
       double fac = 4.0;
@@ -727,217 +730,159 @@ void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bc, int kc, i
 }
 
 // ===========================================================================
-// One-electron integrals: the reference's formulas per primitive pair
-// (overlap.f90:121-174 OS overlap, overlap.f90:24-60 + kinetic.f90:20-54
-// binomial kinetic, nuclear.f90:19-136 Cook/THO nuclear attraction).
+// One-electron integrals and their gradient.
+// Overlap by the 1-D Obara-Saika recursion of overlap.f90:121-145, kinetic
+// energy by the directional formula of kinetic.f90:20-54 on the same 1-D
+// overlaps, nuclear attraction by the OS recursion of the generated
+// NucClass (the Cook/THO sum of nuclear.f90:66-136 in recursive form).
+// One warp per shell pair of one class (l_a >= l_b); the lanes share the
+// (primitive pair, nucleus) work; primitive pairs whose prefactor is below
+// 1e-17 are skipped.
 // ===========================================================================
-__device__ __forceinline__ double ipowd(double x, int n) {
-  double r = 1.0;
-  for (int i = 0; i < n; ++i) r *= x;
-  return r;
-}
-__device__ __forceinline__ double factd(int n) {
-  double r = 1.0;
-  for (int i = 2; i <= n; ++i) r *= i;
-  return r;
-}
-__device__ __forceinline__ double fact2d(int n) {
-  double r = 1.0;
-  for (int i = n; i > 1; i -= 2) r *= i;
-  return r;
-}
-__device__ __forceinline__ double binomd(int n, int k) { return factd(n) / (factd(k) * factd(n - k)); }
-
-// 1-D overlap S(a,b) by the recursion of overlap.f90:121-145 (with the
-// Gaussian factor sqrt(pi/p) exp(-ab/p X^2) of S00 included).
-__device__ double sij_1d(int a, int b, double aa, double bb, double Ra, double Rb, double Rp) {
-  if (a < 0 || b < 0) return 0.0;
-  double S[6][6];
-  for (int i = 0; i < 6; ++i)
-    for (int j = 0; j < 6; ++j) S[i][j] = 0.0;
-  const double p = aa + bb;
-  S[1][1] = sqrt(3.14159265358979323846 / p) * exp(-(aa * bb) / p * (Ra - Rb) * (Ra - Rb));
-  const double o2p = 1.0 / (2.0 * p);
-  for (int i = 0; i <= a; ++i)
-    for (int j = 0; j <= b; ++j) {
-      if (i + 1 <= a) S[i + 2][j + 1] = (Rp - Ra) * S[i + 1][j + 1] + o2p * (i * S[i][j + 1] + j * S[i + 1][j]);
-      if (j + 1 <= b) S[i + 1][j + 2] = (Rp - Rb) * S[i + 1][j + 1] + o2p * (i * S[i][j + 1] + j * S[i + 1][j]);
+template <int NI, int NJ>
+__device__ __forceinline__ void ovl1d(double s00, double PA, double PB, double o2p, double (&S)[NI][NJ]) {
+#pragma unroll
+  for (int i = 0; i < NI; ++i)
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      double v;
+      if (i == 0 && j == 0) v = s00;
+      else if (i > 0) {
+        v = PA * S[i - 1][j];
+        if (i > 1) v += (i - 1) * o2p * S[i - 2][j];
+        if (j > 0) v += j * o2p * S[i - 1][j - 1];
+      } else {
+        v = PB * S[i][j - 1];
+        if (j > 1) v += (j - 1) * o2p * S[i][j - 2];
+      }
+      S[i][j] = v;
     }
-  return S[a + 1][b + 1];
-}
-
-// Binomial 1-D overlap Si of overlap.f90:24-60 (no Gaussian factor).
-__device__ double si_binom(int a, int b, double aa, double bb, double Ra, double Rb, double R) {
-  double s = 0.0;
-  for (int i = 0; i <= a; ++i)
-    for (int j = 0; j <= b; ++j)
-      if (((i + j) & 1) == 0) {
-        double t = binomd(a, i) * binomd(b, j) * fact2d(i + j - 1);
-        t *= ipowd(R - Ra, a - i);
-        t *= ipowd(R - Rb, b - j);
-        t /= pow(2.0 * (aa + bb), (i + j) / 2.0);
-        s += t;
-      }
-  return s;
-}
-
-__device__ double ki_term(int ac, int a1, int a2, int bc, int b1, int b2, double aa, double bb, double Ra, double Rb,
-                          double Ra1, double Rb1, double Ra2, double Rb2, double Rc, double R1, double R2, double cp) {
-  double k = 0.0;
-  k += ac * bc * si_binom(ac - 1, bc - 1, aa, bb, Ra, Rb, Rc);
-  k -= 2.0 * aa * bc * si_binom(ac + 1, bc - 1, aa, bb, Ra, Rb, Rc);
-  k -= 2.0 * ac * bb * si_binom(ac - 1, bc + 1, aa, bb, Ra, Rb, Rc);
-  k += 4.0 * aa * bb * si_binom(ac + 1, bc + 1, aa, bb, Ra, Rb, Rc);
-  k *= 0.5;
-  double v = cp * pow(3.14159265358979323846 / (aa + bb), 1.5) * k;
-  v *= si_binom(a1, b1, aa, bb, Ra1, Rb1, R1);
-  v *= si_binom(a2, b2, aa, bb, Ra2, Rb2, R2);
-  return v;
-}
-
-struct Prim1e {
-  double aa, bb, p, cp;
-  double A[3], B[3], P[3];
-};
-
-__device__ __forceinline__ bool valid3(const int* a) { return a[0] >= 0 && a[1] >= 0 && a[2] >= 0; }
-
-__device__ double overlap_u(const int* a, const int* b, const Prim1e& g) {
-  if (!valid3(a) || !valid3(b)) return 0.0;
-  double s = 1.0;
-  for (int x = 0; x < 3; ++x) s *= sij_1d(a[x], b[x], g.aa, g.bb, g.A[x], g.B[x], g.P[x]);
-  return s;
-}
-
-__device__ double kinetic_u(const int* a, const int* b, const Prim1e& g) {
-  if (!valid3(a) || !valid3(b)) return 0.0;
-  const double *A = g.A, *B = g.B, *P = g.P;
-  double k = ki_term(a[0], a[1], a[2], b[0], b[1], b[2], g.aa, g.bb, A[0], B[0], A[1], B[1], A[2], B[2], P[0], P[1], P[2], g.cp);
-  k += ki_term(a[1], a[2], a[0], b[1], b[2], b[0], g.aa, g.bb, A[1], B[1], A[2], B[2], A[0], B[0], P[1], P[2], P[0], g.cp);
-  k += ki_term(a[2], a[0], a[1], b[2], b[0], b[1], g.aa, g.bb, A[2], B[2], A[0], B[0], A[1], B[1], P[2], P[0], P[1], g.cp);
-  return k;
-}
-
-__device__ double fcoefd(int j, int l, int m, double a, double b) {
-  double r = 0.0;
-  for (int k = max(0, j - m); k <= min(j, l); ++k) r += binomd(l, k) * binomd(m, j - k) * ipowd(a, l - k) * ipowd(b, m + k - j);
-  return r;
-}
-__device__ double afac(int l, int r, int i, int l1, int l2, double Ra, double Rb, double Rc, double Rp, double eps) {
-  double a = (l & 1) ? -1.0 : 1.0;
-  a *= fcoefd(l, l1, l2, Rp - Ra, Rp - Rb);
-  a *= (i & 1) ? -1.0 : 1.0;
-  a *= factd(l);
-  a *= ipowd(Rp - Rc, l - 2 * r - 2 * i);
-  a *= ipowd(eps, r + i);
-  a /= factd(r) * factd(i) * factd(l - 2 * r - 2 * i);
-  return a;
-}
-
-// <a| 1/|r-C| |b> (unnormalised) * 2 pi / p * K_AB given F_0..F_{la+lb}.
-__device__ double nuclear_u(const int* a, const int* b, const Prim1e& g, const double* C, const double* F) {
-  if (!valid3(a) || !valid3(b)) return 0.0;
-  const double eps = 1.0 / (4.0 * g.p);
-  double v = 0.0;
-  for (int l = 0; l <= a[0] + b[0]; ++l)
-    for (int r = 0; r <= l / 2; ++r)
-      for (int i = 0; i <= (l - 2 * r) / 2; ++i) {
-        const double Ax = afac(l, r, i, a[0], b[0], g.A[0], g.B[0], C[0], g.P[0], eps);
-        for (int m = 0; m <= a[1] + b[1]; ++m)
-          for (int s = 0; s <= m / 2; ++s)
-            for (int j = 0; j <= (m - 2 * s) / 2; ++j) {
-              const double Ay = afac(m, s, j, a[1], b[1], g.A[1], g.B[1], C[1], g.P[1], eps);
-              for (int n = 0; n <= a[2] + b[2]; ++n)
-                for (int t = 0; t <= n / 2; ++t)
-                  for (int k = 0; k <= (n - 2 * t) / 2; ++k) {
-                    const double Az = afac(n, t, k, a[2], b[2], g.A[2], g.B[2], C[2], g.P[2], eps);
-                    v += Ax * Ay * Az * F[l + m + n - 2 * (r + s + t) - (i + j + k)];
-                  }
-            }
-      }
-  return v * g.cp * 2.0 * 3.14159265358979323846 / g.p;
 }
 
 __device__ __forceinline__ void cart_comp(int l, int k, int* c) {
-  // x descending, then y (cartesian.f90:7-23), l <= 2
+  // x descending, then y (cartesian.f90:7-23), l <= 1
   if (l == 0) { c[0] = c[1] = c[2] = 0; return; }
-  if (l == 1) { c[0] = (k == 0); c[1] = (k == 1); c[2] = (k == 2); return; }
-  const int t[6][3] = {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}};
-  c[0] = t[k][0]; c[1] = t[k][1]; c[2] = t[k][2];
+  c[0] = (k == 0); c[1] = (k == 1); c[2] = (k == 2);
 }
 
-__device__ __forceinline__ double norm_comp(const int* c, double a) {
-  const int l = c[0] + c[1] + c[2];
-  double n = pow(2.0 * a * 0.31830988618379067154, 0.75) * pow(4.0 * a, 0.5 * l);
-  return n / sqrt(fact2d(2 * c[0] - 1) * fact2d(2 * c[1] - 1) * fact2d(2 * c[2] - 1));
+// S_ab and T_ab of unnormalised Cartesian components a, b from 1-D tables
+// (the Gaussian prefactor is carried by the tables).
+template <int NI, int NJ>
+__device__ __forceinline__ double ovl3(const double (&S)[3][NI][NJ], const int* a, const int* b) {
+  if (a[0] < 0 || a[1] < 0 || a[2] < 0 || b[0] < 0 || b[1] < 0 || b[2] < 0) return 0.0;
+  return S[0][a[0]][b[0]] * S[1][a[1]][b[1]] * S[2][a[2]][b[2]];
 }
-
-__device__ __forceinline__ void prim1e_setup(double aa, double bb, const double4& A, const double4& B, Prim1e& g) {
-  g.aa = aa; g.bb = bb; g.p = aa + bb;
-  g.A[0] = A.x; g.A[1] = A.y; g.A[2] = A.z;
-  g.B[0] = B.x; g.B[1] = B.y; g.B[2] = B.z;
-  double ab2 = 0.0;
-  for (int x = 0; x < 3; ++x) {
-    g.P[x] = (aa * g.A[x] + bb * g.B[x]) / g.p;
-    ab2 += (g.A[x] - g.B[x]) * (g.A[x] - g.B[x]);
+template <int NI, int NJ>
+__device__ __forceinline__ double kin3(const double (&S)[3][NI][NJ], const int* a, const int* b, double al,
+                                       double be) {
+  if (a[0] < 0 || a[1] < 0 || a[2] < 0 || b[0] < 0 || b[1] < 0 || b[2] < 0) return 0.0;
+  double t = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int x = a[d], y = b[d];
+    double k = 4.0 * al * be * S[d][x + 1][y + 1];
+    if (y > 0) k -= 2.0 * al * y * S[d][x + 1][y - 1];
+    if (x > 0) k -= 2.0 * be * x * S[d][x - 1][y + 1];
+    if (x > 0 && y > 0) k += x * y * S[d][x - 1][y - 1];
+    t += 0.5 * k * S[(d + 1) % 3][a[(d + 1) % 3]][b[(d + 1) % 3]] * S[(d + 2) % 3][a[(d + 2) % 3]][b[(d + 2) % 3]];
   }
-  g.cp = exp(-aa * bb / g.p * ab2);
+  return t;
 }
 
-// One warp per shell pair (a <= b): lanes share the (primitive pair, atom)
-// combinations; S and T use the primitive pairs only.
-__global__ void one_electron_kernel(int npair, const int2* __restrict__ pairs, const double4* __restrict__ cen,
-                                    const int4* __restrict__ desc, const int* __restrict__ nprim,
-                                    const double* __restrict__ ex, const double* __restrict__ co, OneEArgs args) {
+struct Prim1e {
+  double al, be, p, o2p, w;  // w = c_a c_b N_a N_b exp(-al be/p |AB|^2)
+  double P[3], PA[3], PB[3];
+};
+
+__device__ __forceinline__ void prim1e_setup(double al, double ca, int la, double be, double cb, int lb,
+                                             const double4& A, const double4& B, Prim1e& g) {
+  g.al = al; g.be = be; g.p = al + be; g.o2p = 0.5 / g.p;
+  const double A3[3] = {A.x, A.y, A.z}, B3[3] = {B.x, B.y, B.z};
+  double ab2 = 0.0;
+#pragma unroll
+  for (int x = 0; x < 3; ++x) {
+    g.P[x] = (al * A3[x] + be * B3[x]) / g.p;
+    g.PA[x] = g.P[x] - A3[x];
+    g.PB[x] = g.P[x] - B3[x];
+    ab2 += (A3[x] - B3[x]) * (A3[x] - B3[x]);
+  }
+  g.w = ca * cb * prim_norm(la, al) * prim_norm(lb, be) * exp(-al * be / g.p * ab2);
+}
+
+// 1-D overlap tables of one primitive pair: (pi/p)^{3/2} w carried by z.
+template <int NI, int NJ>
+__device__ __forceinline__ void st_tables(const Prim1e& g, double (&S)[3][NI][NJ]) {
+  const double pre = g.w * pow(3.14159265358979323846 / g.p, 1.5);
+  ovl1d<NI, NJ>(1.0, g.PA[0], g.PB[0], g.o2p, S[0]);
+  ovl1d<NI, NJ>(1.0, g.PA[1], g.PB[1], g.o2p, S[1]);
+  ovl1d<NI, NJ>(pre, g.PA[2], g.PB[2], g.o2p, S[2]);
+}
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2* __restrict__ pairs,
+                                                           const double4* __restrict__ cen,
+                                                           const int4* __restrict__ desc, const int* __restrict__ nprim,
+                                                           const double* __restrict__ ex,
+                                                           const double* __restrict__ co, OneEArgs args) {
+  using NCl = NucClass<double, LA, LB>;
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= npair) return;
   const int2 pr = pairs[w];
   const int4 da = desc[pr.x], db = desc[pr.y];
-  const int la = da.x, lb = db.x, na = nprim[pr.x], nb = nprim[pr.y];
-  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
+  const int na = nprim[pr.x], nb = nprim[pr.y];
   const double4 A = cen[pr.x], B = cen[pr.y];
-  double s[9], t[9], v[9];
-  for (int i = 0; i < 9; ++i) s[i] = t[i] = v[i] = 0.0;
+  const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+  double s[NA * NB], t[NA * NB], v[NA * NB];
+#pragma unroll
+  for (int i = 0; i < NA * NB; ++i) s[i] = t[i] = v[i] = 0.0;
   const int npp = na * nb;
   const int work = npp * args.natoms;
   for (int idx = lane; idx < work; idx += 32) {
     const int pp = idx % npp, c = idx / npp;
     const int ka = pp / nb, kb = pp % nb;
-    const double aa = ex[da.w + ka], bb = ex[db.w + kb];
     Prim1e g;
-    prim1e_setup(aa, bb, A, B, g);
-    const double4 Cn = args.atoms[c];
-    const double C[3] = {Cn.x, Cn.y, Cn.z};
-    double pc2 = 0.0;
-    for (int x = 0; x < 3; ++x) pc2 += (g.P[x] - C[x]) * (g.P[x] - C[x]);
-    double F[PF_BOYS_MMAX + 1];
-    boys_runtime(args.boys_mode, la + lb, g.p * pc2, F);
-    const double cc = co[da.w + ka] * co[db.w + kb];
-    for (int ia = 0; ia < nca; ++ia)
-      for (int ib = 0; ib < ncb; ++ib) {
-        int ca[3], cb[3];
-        cart_comp(la, ia, ca);
-        cart_comp(lb, ib, cb);
-        const double w2 = cc * norm_comp(ca, aa) * norm_comp(cb, bb);
-        if (c == 0) {
-          s[ia * 3 + ib] += w2 * overlap_u(ca, cb, g);
-          t[ia * 3 + ib] += w2 * kinetic_u(ca, cb, g);
+    prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
+    if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
+    if (c == 0) {
+      double S[3][LA + 2][LB + 2];
+      st_tables<LA + 2, LB + 2>(g, S);
+#pragma unroll
+      for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+          int ca[3], cb[3];
+          cart_comp(LA, ia, ca);
+          cart_comp(LB, ib, cb);
+          s[ia * NB + ib] += ovl3(S, ca, cb);
+          t[ia * NB + ib] += kin3(S, ca, cb, g.al, g.be);
         }
-        v[ia * 3 + ib] += w2 * (-Cn.w) * nuclear_u(ca, cb, g, C, F);
-      }
+    }
+    const double4 Cn = args.atoms[c];
+    const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
+    double F[PF_BOYS_MMAX + 1];
+    boys_runtime(args.boys_mode, LA + LB, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
+    const double pref = -Cn.w * g.w * 6.2831853071795864769 / g.p;
+    double I[LA + LB + 1];
+#pragma unroll
+    for (int m = 0; m <= LA + LB; ++m) I[m] = pref * F[m];
+    NCl::vint(I, g.PA, PC, g.o2p, AB, v);
   }
-  for (int i = 0; i < 9; ++i) {
+#pragma unroll
+  for (int i = 0; i < NA * NB; ++i) {
     s[i] = warp_sum(s[i]);
     t[i] = warp_sum(t[i]);
     v[i] = warp_sum(v[i]);
   }
   if (lane == 0) {
     const int n = args.nbf;
-    for (int ia = 0; ia < nca; ++ia)
-      for (int ib = 0; ib < ncb; ++ib) {
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
         const size_t mu = da.z + ia, nu = db.z + ib;
-        const int k = ia * 3 + ib;
+        const int k = ia * NB + ib;
         if (args.S) { args.S[mu * n + nu] = s[k]; args.S[nu * n + mu] = s[k]; }
         if (args.T) { args.T[mu * n + nu] = t[k]; args.T[nu * n + mu] = t[k]; }
         if (args.V) { args.V[mu * n + nu] = v[k]; args.V[nu * n + mu] = v[k]; }
@@ -945,90 +890,149 @@ __global__ void one_electron_kernel(int npair, const int2* __restrict__ pairs, c
   }
 }
 
-void launch_one_electron(const ShellDev& sh, int npair, const int2* pairs, const OneEArgs& a, cudaStream_t s) {
-  if (npair <= 0) return;
-  one_electron_kernel<<<(npair + 3) / 4, 128, 0, s>>>(npair, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
-  PF_CUDA(cudaGetLastError());
-  count_launch();
+void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEArgs& a,
+                         cudaStream_t s) {
+  for (int c = 0; c < NCLASS; ++c) {
+    if (npair[c] <= 0) continue;
+    dim3 grid((npair[c] + 3) / 4), block(128);
+    if (c == 0) one_electron_kernel<0, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    if (c == 1) one_electron_kernel<1, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    if (c == 2) one_electron_kernel<1, 1><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    PF_CUDA(cudaGetLastError());
+    count_launch();
+  }
 }
 
-// Gradient of the one-electron energy over canonical shell pairs (a <= b):
-//   sum P (dT + dV) - sum W dS, d/dB = -d/dA for the two-centre S and T,
-//   d/dC V^C = -(d/dA + d/dB) V^C for every nucleus C.
-__global__ void grad1e_kernel(int npair, const int2* __restrict__ pairs, const double4* __restrict__ cen,
-                              const int4* __restrict__ desc, const int* __restrict__ nprim,
-                              const double* __restrict__ ex, const double* __restrict__ co, OneEGradArgs args) {
+// Gradient of the one-electron energy: sum P (dT + dV) - sum W dS over the
+// pairs of one class; d/dB = -d/dA for the two-centre S and T, and
+// d/dC V^C = -(d/dA + d/dB) V^C for every nucleus C.  Each lane owns a set
+// of nuclei; the nuclear (C) terms go to a shared-memory gradient that the
+// block adds to the global one at the end.
+template <int LA, int LB>
+__global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __restrict__ pairs,
+                                                     const double4* __restrict__ cen, const int4* __restrict__ desc,
+                                                     const int* __restrict__ nprim, const double* __restrict__ ex,
+                                                     const double* __restrict__ co, OneEGradArgs args) {
+  using NCl = NucClass<double, LA, LB>;
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
+  extern __shared__ double gsh[];  // 3 * natoms
+  for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gsh[i] = 0.0;
+  __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= npair) return;
-  const int2 pr = pairs[w];
-  const int4 da = desc[pr.x], db = desc[pr.y];
-  const int la = da.x, lb = db.x, na = nprim[pr.x], nb = nprim[pr.y];
-  const int nca = (la + 1) * (la + 2) / 2, ncb = (lb + 1) * (lb + 2) / 2;
-  const double4 A = cen[pr.x], B = cen[pr.y];
-  const double wgt = (pr.x == pr.y) ? 1.0 : 2.0;
+  const int nwarp_total = (gridDim.x * blockDim.x) >> 5;
   const int n = args.nbf;
-  double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
-  const int npp = na * nb;
-  const int work = npp * args.natoms;
-  for (int idx = lane; idx < work; idx += 32) {
-    const int pp = idx % npp, c = idx / npp;
-    const int ka = pp / nb, kb = pp % nb;
-    const double aa = ex[da.w + ka], bb = ex[db.w + kb];
-    Prim1e g;
-    prim1e_setup(aa, bb, A, B, g);
-    const double4 Cn = args.atoms[c];
-    const double C[3] = {Cn.x, Cn.y, Cn.z};
-    double pc2 = 0.0;
-    for (int x = 0; x < 3; ++x) pc2 += (g.P[x] - C[x]) * (g.P[x] - C[x]);
-    double F[PF_BOYS_MMAX + 1];
-    boys_runtime(args.boys_mode, la + lb + 1, g.p * pc2, F);
-    const double cc = co[da.w + ka] * co[db.w + kb];
-    double gC[3] = {0, 0, 0};
-    for (int ia = 0; ia < nca; ++ia)
-      for (int ib = 0; ib < ncb; ++ib) {
-        int ca[3], cb[3];
-        cart_comp(la, ia, ca);
-        cart_comp(lb, ib, cb);
-        const size_t mu = da.z + ia, nu = db.z + ib;
-        const double pw = wgt * cc * norm_comp(ca, aa) * norm_comp(cb, bb);
-        const double P = args.P[mu * n + nu] * pw, W = args.W[mu * n + nu] * pw;
-        for (int x = 0; x < 3; ++x) {
-          int up[3] = {ca[0], ca[1], ca[2]}, dn[3] = {ca[0], ca[1], ca[2]};
-          int bu[3] = {cb[0], cb[1], cb[2]}, bd[3] = {cb[0], cb[1], cb[2]};
-          up[x] += 1; dn[x] -= 1; bu[x] += 1; bd[x] -= 1;
-          double va = 2.0 * aa * nuclear_u(up, cb, g, C, F) - ca[x] * nuclear_u(dn, cb, g, C, F);
-          double vb = 2.0 * bb * nuclear_u(ca, bu, g, C, F) - cb[x] * nuclear_u(ca, bd, g, C, F);
-          va *= -Cn.w * P;
-          vb *= -Cn.w * P;
-          gA[x] += va;
-          gB[x] += vb;
-          gC[x] -= va + vb;
-          if (c == 0) {
-            const double ds = 2.0 * aa * overlap_u(up, cb, g) - ca[x] * overlap_u(dn, cb, g);
-            const double dt = 2.0 * aa * kinetic_u(up, cb, g) - ca[x] * kinetic_u(dn, cb, g);
-            const double d = P * dt - W * ds;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < npair; w += nwarp_total) {
+    const int2 pr = pairs[w];
+    const int4 da = desc[pr.x], db = desc[pr.y];
+    const int na = nprim[pr.x], nb = nprim[pr.y];
+    const double4 A = cen[pr.x], B = cen[pr.y];
+    const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+    const double wgt = (pr.x == pr.y) ? 1.0 : 2.0;
+    double Pd[NA * NB], Wd[NA * NB];
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib) {
+        const size_t k = (size_t)(da.z + ia) * n + db.z + ib;
+        Pd[ia * NB + ib] = wgt * args.P[k];
+        Wd[ia * NB + ib] = wgt * args.W[k];
+      }
+    double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
+    const int npp = na * nb;
+    // kinetic and overlap: lanes over primitive pairs
+    for (int pp = lane; pp < npp; pp += 32) {
+      const int ka = pp / nb, kb = pp % nb;
+      Prim1e g;
+      prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
+      if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
+      double S[3][LA + 3][LB + 2];
+      st_tables<LA + 3, LB + 2>(g, S);
+#pragma unroll
+      for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+          int ca[3], cb[3];
+          cart_comp(LA, ia, ca);
+          cart_comp(LB, ib, cb);
+#pragma unroll
+          for (int x = 0; x < 3; ++x) {
+            int up[3] = {ca[0], ca[1], ca[2]}, dn[3] = {ca[0], ca[1], ca[2]};
+            up[x] += 1;
+            dn[x] -= 1;
+            double ds = 2.0 * g.al * ovl3(S, up, cb);
+            double dt = 2.0 * g.al * kin3(S, up, cb, g.al, g.be);
+            if (ca[x] > 0) {
+              ds -= ca[x] * ovl3(S, dn, cb);
+              dt -= ca[x] * kin3(S, dn, cb, g.al, g.be);
+            }
+            const double d = Pd[ia * NB + ib] * dt - Wd[ia * NB + ib] * ds;
             gA[x] += d;
             gB[x] -= d;
           }
         }
+    }
+    // nuclear attraction: lanes over nuclei, all primitive pairs each
+    for (int c = lane; c < args.natoms; c += 32) {
+      const double4 Cn = args.atoms[c];
+      double gv[6] = {0, 0, 0, 0, 0, 0};
+      for (int pp = 0; pp < npp; ++pp) {
+        const int ka = pp / nb, kb = pp % nb;
+        Prim1e g;
+        prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
+        if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
+        const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
+        double F[PF_BOYS_MMAX + 1];
+        boys_runtime(args.boys_mode, LA + LB + 1, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
+        const double pref = -Cn.w * g.w * 6.2831853071795864769 / g.p;
+        double I[LA + LB + 2];
+#pragma unroll
+        for (int m = 0; m <= LA + LB + 1; ++m) I[m] = pref * F[m];
+        const double tw[2] = {2.0 * g.al, 2.0 * g.be};
+        NCl::vgrad(I, g.PA, PC, g.o2p, AB, tw, Pd, gv);
       }
-    for (int x = 0; x < 3; ++x) atomicAdd(args.grad + 3 * c + x, gC[x]);
-  }
-  for (int x = 0; x < 3; ++x) {
-    const double sa = warp_sum(gA[x]), sb = warp_sum(gB[x]);
-    if (lane == 0) {
-      atomicAdd(args.grad + 3 * da.y + x, sa);
-      atomicAdd(args.grad + 3 * db.y + x, sb);
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        gA[x] += gv[x];
+        gB[x] += gv[3 + x];
+        atomicAdd(gsh + 3 * c + x, -(gv[x] + gv[3 + x]));
+      }
+    }
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const double sa = warp_sum(gA[x]), sb = warp_sum(gB[x]);
+      if (lane == 0) {
+        atomicAdd(gsh + 3 * da.y + x, sa);
+        atomicAdd(gsh + 3 * db.y + x, sb);
+      }
     }
   }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x)
+    if (gsh[i] != 0.0) atomicAdd(args.grad + i, gsh[i]);
 }
 
-void launch_grad1e(const ShellDev& sh, int npair, const int2* pairs, const OneEGradArgs& a, cudaStream_t s) {
-  if (npair <= 0) return;
-  grad1e_kernel<<<(npair + 3) / 4, 128, 0, s>>>(npair, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
-  PF_CUDA(cudaGetLastError());
-  count_launch();
+void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEGradArgs& a,
+                   int num_sms, cudaStream_t s) {
+  const size_t smem = 3 * (size_t)a.natoms * sizeof(double);
+  for (int c = 0; c < NCLASS; ++c) {
+    if (npair[c] <= 0) continue;
+    const int blocks = std::max(1, std::min((npair[c] + 3) / 4, 2 * num_sms));
+    dim3 grid(blocks), block(128);
+    if (c == 0) {
+      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      grad1e_kernel<0, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    }
+    if (c == 1) {
+      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      grad1e_kernel<1, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    }
+    if (c == 2) {
+      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      grad1e_kernel<1, 1><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    }
+    PF_CUDA(cudaGetLastError());
+    count_launch();
+  }
 }
 
 // ===========================================================================
@@ -1182,6 +1186,118 @@ void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const doub
                  const double* C, float* dmax, cudaStream_t s) {
   dim3 b(16, 16), g((ns + 15) / 16, (ns + 15) / 16);
   dmax_kernel<<<g, b, 0, s>>>(ns, bf_off, nfun, nbf, A, B, C, dmax);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Trace-correcting density-matrix purification (TC2, Niklasson 2002) of the
+// orthogonalised Fock matrix: X_0 = (l_max I - F')/(l_max - l_min) with
+// Gershgorin bounds, then X <- X^2 or X <- 2X - X^2, whichever moves Tr X
+// towards the occupation N.  X converges to the projector onto the N lowest
+// eigenvectors of F'.  The choice and the convergence test run on the device
+// (one block), so a purification needs no host round trip per step.
+// state: [0] l_min, [1] l_max, [2] Tr X, [3] Tr X^2, [4] converged flag,
+//        [5] steps taken, [6] remaining final steps.
+// ---------------------------------------------------------------------------
+__global__ void gersh_kernel(int n, const double* __restrict__ F, double* __restrict__ state) {
+  __shared__ double smin[32], smax[32];
+  double lo = 1e300, hi = -1e300;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double r = 0.0;
+    for (int j = 0; j < n; ++j)
+      if (j != i) r += fabs(F[(size_t)j * n + i]);
+    const double d = F[(size_t)i * n + i];
+    lo = fmin(lo, d - r);
+    hi = fmax(hi, d + r);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { smin[w] = lo; smax[w] = hi; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) { lo = fmin(lo, smin[k]); hi = fmax(hi, smax[k]); }
+    lo = fmin(lo, smin[0]);
+    hi = fmax(hi, smax[0]);
+    state[0] = lo;
+    state[1] = hi;
+    state[4] = 0.0;
+    state[5] = 0.0;
+    state[6] = 0.0;
+  }
+}
+
+__global__ void tc2_init_kernel(long long n2, int n, const double* __restrict__ F, const double* __restrict__ state,
+                                double* __restrict__ X) {
+  const double lo = state[0], hi = state[1];
+  const double sc = 1.0 / (hi - lo);
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % n), j = (int)(k / n);
+    X[k] = ((i == j ? hi : 0.0) - F[k]) * sc;
+  }
+}
+
+// One TC2 step on X given X2 = X*X: traces, choice, update, convergence.
+// Once Tr X - Tr X^2 < 1e-9 two more steps run (quadratic convergence takes
+// the remainder to round-off), then X is left unchanged.
+__global__ void tc2_step_kernel(int n, double nocc, double* __restrict__ X, const double* __restrict__ X2,
+                                double* __restrict__ state) {
+  __shared__ double s1[32], s2[32];
+  __shared__ double coef[2];
+  __shared__ int skip;
+  if (threadIdx.x == 0) skip = state[4] != 0.0;
+  __syncthreads();
+  if (skip) return;
+  double t1 = 0.0, t2 = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    t1 += X[(size_t)i * n + i];
+    t2 += X2[(size_t)i * n + i];
+  }
+  t1 = warp_sum(t1);
+  t2 = warp_sum(t2);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { s1[w] = t1; s2[w] = t2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    t1 = 0.0; t2 = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { t1 += s1[k]; t2 += s2[k]; }
+    state[2] = t1;
+    state[3] = t2;
+    state[5] += 1.0;
+    // X <- X^2 takes the trace to t2, X <- 2X - X^2 to 2 t1 - t2
+    if (fabs(t2 - nocc) < fabs(2.0 * t1 - t2 - nocc)) { coef[0] = 0.0; coef[1] = 1.0; }
+    else { coef[0] = 2.0; coef[1] = -1.0; }
+    if (state[6] > 0.0) {
+      state[6] -= 1.0;
+      if (state[6] <= 0.0) state[4] = 1.0;
+    } else if (t1 - t2 < 1e-9 && fabs(t1 - nocc) < 1e-6) {
+      state[6] = 2.0;
+    }
+  }
+  __syncthreads();
+  const double a = coef[0], b = coef[1];
+  const long long n2 = (long long)n * n;
+  for (long long k = threadIdx.x; k < n2; k += blockDim.x) X[k] = a * X[k] + b * X2[k];
+}
+
+void launch_gersh(int n, const double* F, double* state, cudaStream_t s) {
+  gersh_kernel<<<1, 1024, 0, s>>>(n, F, state);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s) {
+  const long long n2 = (long long)n * n;
+  const int g = (int)std::min<long long>((n2 + 255) / 256, 2048);
+  tc2_init_kernel<<<std::max(g, 1), 256, 0, s>>>(n2, n, F, state, X);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+void launch_tc2_step(int n, double nocc, double* X, const double* X2, double* state, cudaStream_t s) {
+  tc2_step_kernel<<<1, 1024, 0, s>>>(n, nocc, X, X2, state);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }

@@ -127,6 +127,63 @@ void System::density_from(const double* C, int nocc, double scale, double* Pm) {
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nocc, &scale, C, nbf, C, nbf, &zero, Pm, nbf));
 }
 
+bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
+  const double one = 1.0, zero = 0.0;
+  if (nocc <= 0) {
+    launch_zero(Pm, (size_t)nbf * nbf * sizeof(double), stream);
+    return true;
+  }
+  if (nocc >= nbf) {  // every orbital occupied: P = scale * X X^T = scale * S^-1
+    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, X, nbf, X, nbf, &zero, Pm, nbf));
+    return true;
+  }
+  double* Fp = Pu[0];
+  double* Xp = Pu[1];
+  double* X2 = Pu[2];
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
+  launch_gersh(nbf, Fp, pstate, stream);
+  launch_tc2_init(nbf, Fp, pstate, Xp, stream);
+  const int chunk = 8, kmax = 200;
+  double st_h[8];
+  bool ok = false;
+  for (int k = 0; k < kmax; k += chunk) {
+    for (int j = 0; j < chunk; ++j) {
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Xp, nbf, Xp, nbf, &zero, X2, nbf));
+      launch_tc2_step(nbf, (double)nocc, Xp, X2, pstate, stream);
+    }
+    PF_CUDA(cudaMemcpyAsync(st_h, pstate, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    if (st_h[4] != 0.0) {
+      ok = true;
+      break;
+    }
+  }
+  purify_steps += (int)st_h[5];
+  if (!ok) return false;
+  // P = scale * X Xp X^T
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));
+  return true;
+}
+
+// New density from a Fock matrix: purification, or eigenvectors when the
+// purification does not converge (no gap at the occupation number).
+void System::density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps) {
+  if (purify(Fm, nocc, scale, Pm)) return;
+  purify_fallbacks++;
+  diagonalize(Fm, C, eps);
+  density_from(C, nocc, scale, Pm);
+}
+
+// Orbitals of the final Fock matrices, for the caller's outputs.
+void System::final_orbitals() {
+  if (orbitals_ready) return;
+  const int nsp = uhf ? 2 : 1;
+  for (int s = 0; s < nsp; ++s) diagonalize(F[s], Cm[s], eps_dev + s * nbf);
+  orbitals_ready = true;
+}
+
 static bool solve_small(int m, std::vector<double> A, std::vector<double> b, std::vector<double>& x) {
   // Gaussian elimination with partial pivoting on an m x m system.
   for (int c = 0; c < m; ++c) {
@@ -177,11 +234,9 @@ void System::run_scf() {
   st.ms_1e = elapsed(a0, a1);
   orthogonalizer();
   // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144)
-  diagonalize(H, Cm[0], eps_dev);
-  for (int s = 0; s < nsp; ++s) {
-    if (s == 1) PF_CUDA(cudaMemcpyAsync(Cm[1], Cm[0], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    density_from(Cm[s], nocc[s], pscale, P[s]);
-  }
+  orbitals_ready = false;
+  purify_steps = purify_fallbacks = 0;
+  for (int s = 0; s < nsp; ++s) density_step(H, nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
   for (int s = 0; s < nsp; ++s) launch_zero(Pbuilt[s], n2 * sizeof(double), stream);
   launch_zero(J, n2 * sizeof(double), stream);
   for (int s = 0; s < nsp; ++s) launch_zero(K[s], n2 * sizeof(double), stream);
@@ -337,16 +392,11 @@ void System::run_scf() {
     }
     // ---- diagonalise and rebuild the density
     PF_CUDA(cudaEventRecord(a0, stream));
-    for (int s = 0; s < nsp; ++s) {
-      diagonalize(Fuse[s], Cm[s], eps_dev + s * nbf);
-      density_from(Cm[s], nocc[s], pscale, P[s]);
-    }
+    for (int s = 0; s < nsp; ++s) density_step(Fuse[s], nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
     PF_CUDA(cudaEventRecord(a1, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
     ms_diag += elapsed(a0, a1);
   }
-  // orbitals of the final Fock matrix (for W and the outputs)
-  for (int s = 0; s < nsp; ++s) diagonalize(F[s], Cm[s], eps_dev + s * nbf);
   PF_CUDA(cudaEventRecord(t1, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   st.ms_total = elapsed(t0, t1);
@@ -381,28 +431,24 @@ void System::gradient(double* g_host) {
   PF_CUDA(cudaEventCreate(&a0));
   PF_CUDA(cudaEventCreate(&a1));
   PF_CUDA(cudaEventRecord(a0, stream));
-  // W = sum_s sum_occ eps_i c_i c_i^T (x2 for RHF)
+  // Energy-weighted density without orbitals: at convergence
+  // sum_occ eps_i c_i c_i^T = P_s F_s P_s (UHF), = P F P / 4 for the RHF
+  // total density P = 2 C_occ C_occ^T, and W = 2 x that for RHF.
   const int nsp = uhf ? 2 : 1;
-  const int nocc[2] = {uhf ? nalpha : (nalpha + nbeta + 1) / 2, uhf ? nbeta : 0};
   launch_zero(Wm, n2 * sizeof(double), stream);
   for (int s = 0; s < nsp; ++s) {
-    if (nocc[s] <= 0) continue;
-    PF_CUDA(cudaMemcpyAsync(W1, Cm[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    PF_CUBLAS(cublasDdgmm(cublas, CUBLAS_SIDE_RIGHT, nbf, nocc[s], Cm[s], nbf, eps_dev + s * nbf, 1, W1, nbf));
-    const double f = uhf ? 1.0 : 2.0;
-    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nocc[s], &f, W1, nbf, Cm[s], nbf, &one, Wm, nbf));
+    const double f = uhf ? 1.0 : 0.5;
+    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, F[s], nbf, P[s], nbf, &zero, W1, nbf));
+    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &f, P[s], nbf, W1, nbf, &one, Wm, nbf));
   }
-  (void)zero;
-  // total density and spin densities of the final orbitals
+  // total density and spin densities of the converged SCF
   double* Pt = W2;
-  double* Ps[2] = {Pbuilt[0], Pbuilt[1]};
+  double* Ps[2] = {P[0], uhf ? P[1] : P[0]};
   if (uhf) {
-    density_from(Cm[0], nocc[0], 1.0, Ps[0]);
-    density_from(Cm[1], nocc[1], 1.0, Ps[1]);
-    launch_axpby((long long)n2, 1.0, Ps[0], 0.0, Pt, stream);
-    launch_axpby((long long)n2, 1.0, Ps[1], 1.0, Pt, stream);
+    launch_axpby((long long)n2, 1.0, P[0], 0.0, Pt, stream);
+    launch_axpby((long long)n2, 1.0, P[1], 1.0, Pt, stream);
   } else {
-    density_from(Cm[0], nocc[0], 2.0, Pt);
+    Pt = P[0];
   }
   launch_zero(grad_dev, 3 * natoms * sizeof(double), stream);
   OneEGradArgs g1;
@@ -413,7 +459,7 @@ void System::gradient(double* g_host) {
   g1.W = Wm;
   g1.nbf = nbf;
   g1.grad = grad_dev;
-  launch_grad1e(shd, n1e, pairs1e, g1, stream);
+  launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
   launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Pt, nullptr, nullptr, dmax, stream);
   GradArgs g2;
   g2.Pt = Pt;
@@ -477,6 +523,7 @@ void System::fill_result(pyfacc_result* r) {
       copy_out(stream, r->P, P[0], n2);
     }
   }
+  if (r->C_alpha || r->C_beta || r->eps_alpha || r->eps_beta) final_orbitals();
   copy_out(stream, r->C_alpha, Cm[0], n2);
   copy_out(stream, r->C_beta, Cm[uhf ? 1 : 0], n2);
   copy_out(stream, r->eps_alpha, eps_dev, nbf);

@@ -48,8 +48,8 @@ struct System {
   // ---- device data
   ShellDev shd;
   double4* atoms_dev = nullptr;
-  int2* pairs1e = nullptr;
-  int n1e = 0;
+  int2* pairs1e[NCLASS] = {nullptr, nullptr, nullptr};  // per class, l_a >= l_b
+  int n1e[NCLASS] = {0, 0, 0};
   int* bf_off_dev = nullptr;
   int* nfun_dev = nullptr;
   PairData pd;
@@ -63,6 +63,10 @@ struct System {
   double *P[2] = {nullptr, nullptr}, *Pbuilt[2] = {nullptr, nullptr}, *Pold[2] = {nullptr, nullptr};
   double *W1 = nullptr, *W2 = nullptr, *W3 = nullptr, *Err[2] = {nullptr, nullptr};
   double *Cm[2] = {nullptr, nullptr}, *Wm = nullptr, *small = nullptr;
+  double *Pu[3] = {nullptr, nullptr, nullptr};  // purification work matrices
+  double* pstate = nullptr;                      // TC2 state (device)
+  bool orbitals_ready = false;
+  int purify_steps = 0, purify_fallbacks = 0;
   float* dmax = nullptr;
   std::vector<double*> diis_F, diis_E;
   double* eps_dev = nullptr;
@@ -97,6 +101,11 @@ struct System {
   void orthogonalizer();
   void diagonalize(const double* Fm, double* C, double* eps);
   void density_from(const double* C, int nocc, double scale, double* Pm);
+  // P = scale * projector onto the nocc lowest eigenvectors of F (TC2
+  // purification of X^T F X); false if it did not converge.
+  bool purify(const double* Fm, int nocc, double scale, double* Pm);
+  void density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps);
+  void final_orbitals();
   void run_scf();
   void gradient(double* g_host);
   void fill_result(pyfacc_result* r);
