@@ -1,12 +1,11 @@
 // Boys function F_m(T) = int_0^1 t^(2m) exp(-T t^2) dt on the device.
 //
-// Accurate mode (default): for T < 36, an 8-term Taylor expansion of F_mmax
-// about the nearest point of a 0.1-spaced grid (|dT| <= 0.05, remainder
-// < 1e-16 relative), then the stable downward recursion
-//   F_m = (2T F_{m+1} + exp(-T)) / (2m+1);
-// for T >= 36, F_0 = sqrt(pi/T)/2 (erfc(6) ~ 2e-17) and the upward recursion
-//   F_{m+1} = ((2m+1) F_m - exp(-T)) / (2T),
-// which is stable for T > m.  The grid values are computed once on the host
+// Accurate mode (default): F_mmax from an 8-term Taylor expansion about the
+// nearest point of a 0.1-spaced grid (|dT| <= 0.05, remainder < 1e-16
+// relative) for T < 36, or for T >= 36 from F_0 = sqrt(pi/T)/2
+// (erfc(6) ~ 2e-17) and the upward recursion
+//   F_{m+1} = ((2m+1) F_m - exp(-T)) / (2T)   (stable for T > m);
+// then the stable downward recursion F_m = (2T F_{m+1} + exp(-T)) / (2m+1).  The grid values are computed once on the host
 // in long double from the positive series (ensure_boys_tables, kernels.cu).
 // FP32 mode (mixed precision) uses the same grid in float with 5 Taylor terms.
 //
@@ -32,60 +31,57 @@ namespace pyfacc {
 __device__ double g_boys_tab[PF_BOYS_NGRID * PF_BOYS_NCOL];
 __device__ float g_boys_tabf[PF_BOYS_NGRID * PF_BOYS_NCOL];
 
+// Branch-free: every lane evaluates the Taylor value (from row 0 when T is
+// beyond the grid) and the asymptotic value and selects, so a warp whose
+// quartets straddle T = 36 does not execute both paths one after the other.
 template <int L>
 __device__ __forceinline__ void boys_fp64(double T, double* __restrict__ F) {
-  if (T < PF_BOYS_TMAX) {
-    const int k = __double2int_rn(T * PF_BOYS_INV_STEP);
-    const double x = k * PF_BOYS_STEP - T;  // F_m(T) = sum_j F_{m+j}(T_k) x^j / j!
-    const double* row = g_boys_tab + k * PF_BOYS_NCOL + L;
-    double f = __ldg(row + PF_BOYS_NT - 1);
+  const bool tab = T < PF_BOYS_TMAX;
+  const int k = tab ? __double2int_rn(T * PF_BOYS_INV_STEP) : 0;
+  const double x = k * PF_BOYS_STEP - T;  // F_m(T) = sum_j F_{m+j}(T_k) x^j / j!
+  const double* row = g_boys_tab + k * PF_BOYS_NCOL + L;
+  double f = __ldg(row + PF_BOYS_NT - 1);
 #pragma unroll
-    for (int j = PF_BOYS_NT - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0 / (j + 1));
-    F[L] = f;
-    if (L > 0) {
-      const double e = exp(-T);
-      const double t2 = 2.0 * T;
-#pragma unroll
-      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
-    }
-  } else {
-    const double rt = rsqrt(T);
-    F[0] = 0.88622692545275801365 * rt;  // sqrt(pi)/2
-    if (L > 0) {
-      const double e = exp(-T);
-      const double o2t = 0.5 * rt * rt;
-#pragma unroll
-      for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * o2t;
-    }
+  for (int j = PF_BOYS_NT - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0 / (j + 1));
+  const double rt = rsqrt(fmax(T, PF_BOYS_TMAX));
+  double fa = 0.88622692545275801365 * rt;  // sqrt(pi/T)/2
+  if (L == 0) {
+    F[0] = tab ? f : fa;
+    return;
   }
+  const double e = exp(-T);
+  const double o2t = 0.5 * rt * rt;
+#pragma unroll
+  for (int m = 0; m < L; ++m) fa = ((2 * m + 1) * fa - e) * o2t;
+  F[L] = tab ? f : fa;
+  const double t2 = 2.0 * T;
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0 / (2 * m + 1));
 }
 
 template <int L>
 __device__ __forceinline__ void boys_fp32(float T, float* __restrict__ F) {
-  if (T < (float)PF_BOYS_TMAX) {
-    const int k = __float2int_rn(T * (float)PF_BOYS_INV_STEP);
-    const float x = k * (float)PF_BOYS_STEP - T;
-    const float* row = g_boys_tabf + k * PF_BOYS_NCOL + L;
-    float f = __ldg(row + PF_BOYS_NTF - 1);
+  const bool tab = T < (float)PF_BOYS_TMAX;
+  const int k = tab ? __float2int_rn(T * (float)PF_BOYS_INV_STEP) : 0;
+  const float x = k * (float)PF_BOYS_STEP - T;
+  const float* row = g_boys_tabf + k * PF_BOYS_NCOL + L;
+  float f = __ldg(row + PF_BOYS_NTF - 1);
 #pragma unroll
-    for (int j = PF_BOYS_NTF - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0f / (j + 1));
-    F[L] = f;
-    if (L > 0) {
-      const float e = expf(-T);
-      const float t2 = 2.0f * T;
-#pragma unroll
-      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
-    }
-  } else {
-    const float rt = rsqrtf(T);
-    F[0] = 0.88622692545275801365f * rt;
-    if (L > 0) {
-      const float e = expf(-T);
-      const float o2t = 0.5f * rt * rt;
-#pragma unroll
-      for (int m = 0; m < L; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) * o2t;
-    }
+  for (int j = PF_BOYS_NTF - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0f / (j + 1));
+  const float rt = rsqrtf(fmaxf(T, (float)PF_BOYS_TMAX));
+  float fa = 0.88622692545275801365f * rt;
+  if (L == 0) {
+    F[0] = tab ? f : fa;
+    return;
   }
+  const float e = expf(-T);
+  const float o2t = 0.5f * rt * rt;
+#pragma unroll
+  for (int m = 0; m < L; ++m) fa = ((2 * m + 1) * fa - e) * o2t;
+  F[L] = tab ? f : fa;
+  const float t2 = 2.0f * T;
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
 }
 
 template <int L, typename R> struct Boys;

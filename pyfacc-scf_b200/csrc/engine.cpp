@@ -228,6 +228,27 @@ void System::upload_shells() {
   PF_CUDA(cudaStreamSynchronize(stream));
 }
 
+// Largest |K| = |c_a N_a c_b N_b| sqrt(2) pi^(5/4) / p over primitive pairs of
+// shells on one atom (|AB| = 0 maximises the Gaussian factor).
+double max_prim_prefactor(const Basis& b) {
+  double mx = 0.0;
+  const double c0 = 5.9149671727956128778;
+  auto nrm = [](int l, double a) {
+    const double n = std::pow(2.0 * a / 3.14159265358979323846, 0.75);
+    return l ? n * 2.0 * std::sqrt(a) : n;
+  };
+  for (size_t i = 0; i < b.shells.size(); ++i)
+    for (size_t j = 0; j <= i; ++j) {
+      const Shell &A = b.shells[i], &B = b.shells[j];
+      if (A.atom != B.atom) continue;
+      for (size_t x = 0; x < A.ex.size(); ++x)
+        for (size_t y = 0; y < B.ex.size(); ++y)
+          mx = std::max(mx, std::fabs(A.co[x] * nrm(A.l, A.ex[x]) * B.co[y] * nrm(B.l, B.ex[y])) * c0 /
+                                (A.ex[x] + B.ex[y]));
+    }
+  return mx;
+}
+
 // Canonical shell pairs grouped by class, Schwarz factors on the GPU, then
 // sorted by Q (descending) inside each class; pairs that cannot reach the
 // threshold against the largest Q are dropped.  Task lists per class pair.
@@ -264,7 +285,8 @@ void System::build_pairs() {
                s_i0 = carve(np_all * sizeof(int4)), s_i1 = carve(np_all * sizeof(int4)),
                s_i2 = carve(np_all * sizeof(int4)), s_g = carve(np_all * sizeof(double4)),
                s_pr = carve((size_t)std::max(nprim_tot, 1) * 3 * sizeof(double4)), s_q = carve(np_all * sizeof(double)),
-               s_perm = carve(np_all * sizeof(int)), s_ps = carve(np_all * sizeof(int));
+               s_perm = carve(np_all * sizeof(int)), s_ps = carve(np_all * sizeof(int)),
+               s_kept = carve(np_all * sizeof(int));
   DeviceBuf scratch;
   scratch.ensure(o);
   char* sb = scratch.as<char>();
@@ -279,12 +301,17 @@ void System::build_pairs() {
   double* d_q = reinterpret_cast<double*>(sb + s_q);
   int* d_perm = reinterpret_cast<int*>(sb + s_perm);
   int* d_ps = reinterpret_cast<int*>(sb + s_ps);
+  int* d_kept = reinterpret_cast<int*>(sb + s_kept);
+  const double cut = PRIM_CUT_REL * max_prim_prefactor(basis);
   PF_CUDA(cudaMemcpyAsync(d_pl0, all0.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(d_pl1, all1.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
-  launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, stream);
+  launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, cut, d_kept,
+                     stream);
   launch_schwarz(tmp, off, d_q, stream);
   std::vector<double> q(np_all);
+  std::vector<int> kept(np_all);
   PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaMemcpyAsync(kept.data(), d_kept, np_all * sizeof(int), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   const double qmax = np_all ? *std::max_element(q.begin(), q.end()) : 0.0;
   const double thr = opt.schwarz_thresh;
@@ -301,7 +328,7 @@ void System::build_pairs() {
     for (int k : idx) {
       perm.push_back(k);
       new_ps.push_back(nprim_new);
-      nprim_new += (int)(basis.shells[all0[k].x].ex.size() * basis.shells[all0[k].y].ex.size());
+      nprim_new += kept[k];
       pd.q_host.push_back(q[k]);
       pd.cls_host.push_back(c);
     }
@@ -324,8 +351,8 @@ void System::build_pairs() {
   if (pd.npair > 0) {
     PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
     PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
-    launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, pd.info0,
-                        pd.info1, pd.info2, pd.geom, nullptr, pd.prim, nullptr, stream);
+    launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, cut,
+                        pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, stream);
   }
   PF_CUDA(cudaStreamSynchronize(stream));
   build_tasks();

@@ -12,7 +12,7 @@
 //                 {p, 1/(2p), K, alpha}, {P, 0}, {P-A, 0} with
 //                 K = c_a c_b N_a N_b exp(-alpha beta/p |AB|^2) sqrt(2) pi^(5/4) / p
 //                 so that a primitive quartet prefactor is K_ab K_cd / sqrt(p+q);
-//                 a float copy serves the FP32 quartets of mixed precision.
+//                 primitive pairs with |K| < 1e-16 max|K| are left out.
 //  * tasks        per (bra class, ket class, precision): for bra pair i the
 //                 ket range [ket_lo[i], ket_hi[i]) in chunks of 32 (one warp,
 //                 one ket per lane); task_off is the exclusive prefix sum.
@@ -92,9 +92,7 @@ struct PairData {
   int4* info1 = nullptr;     // {shell_a, shell_b, atom_a, atom_b}
   int4* info2 = nullptr;     // {mat_off lo, mat_off hi, ld, molecule}
   double4* geom = nullptr;   // {ABx, ABy, ABz, Q}
-  float4* geomf = nullptr;
   double4* prim = nullptr;   // 3 per primitive pair
-  float4* primf = nullptr;
   std::vector<double> q_host;   // Q of the sorted pairs
   std::vector<int> cls_host;    // class of the sorted pairs
   std::vector<int> mol_host;    // molecule of the sorted pairs
@@ -132,13 +130,19 @@ struct ShellDev {  // device copies of the shells (packed over a batch)
 };
 
 // Pair construction: canonical pair list -> records, then Schwarz factors.
+// Primitive pairs with |K| < cut are dropped from the sorted records; kept[i]
+// receives the number kept for pair i (may be null).
 void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const int4* pl1, int4* info0,
-                        int4* info1, int4* info2, double4* geom, double4* prim, cudaStream_t s);
+                        int4* info1, int4* info2, double4* geom, double4* prim, double cut, int* kept,
+                        cudaStream_t s);
 void launch_schwarz(const PairData& pd, int npair_class_begin[NCLASS + 1], double* q, cudaStream_t s);
 void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
-                         const int4* i2, const double4* g, const double4* pr, const double* q, int4* o0,
-                         int4* o1, int4* o2, double4* og, float4* ogf, double4* opr, float4* oprf,
-                         cudaStream_t s);
+                         const int4* i2, const double4* g, const double4* pr, const double* q, double cut,
+                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, cudaStream_t s);
+// Largest primitive-pair prefactor |K| of a basis (reached at |AB| = 0) and
+// the relative cut below which primitive pairs are dropped.
+double max_prim_prefactor(const Basis& b);
+constexpr double PRIM_CUT_REL = 1e-16;
 
 struct JkArgs {
   const double* Dj;      // density for J
@@ -164,6 +168,7 @@ struct GradArgs {
   double thresh;
   int uhf;
   double* grad;  // natoms*3 (packed over a batch via the pair's atom index)
+  unsigned long long* stats;  // [0..5] quartets, [6..11] primitive quartets per class, or null
 };
 void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, const GradArgs& a,
                    int num_sms, cudaStream_t s);

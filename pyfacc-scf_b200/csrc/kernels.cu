@@ -105,13 +105,16 @@ __device__ __forceinline__ double prim_norm(int l, double a) {
   return l == 0 ? n : n * 2.0 * sqrt(a);
 }
 
-// pl0 = {shell a, shell b, prim_start, 0}, pl1 = {mat_off, ld, molecule, 0}
+// pl0 = {shell a, shell b, prim_start, 0}, pl1 = {mat_off, ld, molecule, 0}.
+// Every primitive pair is written (the Schwarz factors use them all);
+// kept[i] counts those with |K| >= cut, the ones the gather keeps.
 __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, const int4* __restrict__ desc,
                                    const int* __restrict__ nprim, const double* __restrict__ ex,
                                    const double* __restrict__ co, const int4* __restrict__ pl0,
                                    const int4* __restrict__ pl1, int4* __restrict__ info0,
                                    int4* __restrict__ info1, int4* __restrict__ info2,
-                                   double4* __restrict__ geom, double4* __restrict__ prim) {
+                                   double4* __restrict__ geom, double4* __restrict__ prim, double cut,
+                                   int* __restrict__ kept) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npair) return;
   const int4 p0 = pl0[i];
@@ -126,6 +129,7 @@ __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, c
   info2[i] = pl1[i];
   geom[i] = make_double4(ABx, ABy, ABz, 0.0);
   const double c0 = 5.9149671727956128778;  // sqrt(2) * pi^(5/4)
+  int nk = 0;
   for (int ka = 0; ka < na; ++ka) {
     const double al = ex[da.w + ka], ca = co[da.w + ka] * prim_norm(da.x, ex[da.w + ka]);
     for (int kb = 0; kb < nb; ++kb) {
@@ -137,15 +141,18 @@ __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, c
       r[0] = make_double4(p, 0.5 * op, K, al);
       r[1] = make_double4(Px, Py, Pz, 0.0);
       r[2] = make_double4(Px - A.x, Py - A.y, Pz - A.z, 0.0);
+      nk += fabs(K) >= cut;
     }
   }
+  if (kept) kept[i] = nk;
 }
 
 void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const int4* pl1, int4* info0,
-                        int4* info1, int4* info2, double4* geom, double4* prim, cudaStream_t s) {
+                        int4* info1, int4* info2, double4* geom, double4* prim, double cut, int* kept,
+                        cudaStream_t s) {
   if (npair <= 0) return;
   build_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, pl0, pl1,
-                                                         info0, info1, info2, geom, prim);
+                                                         info0, info1, info2, geom, prim, cut, kept);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }
@@ -254,33 +261,46 @@ void launch_schwarz(const PairData& pd, int off[NCLASS + 1], double* q, cudaStre
   }
 }
 
+// Sorted copy of the pair records; primitive pairs with |K| < cut are left
+// out (their count was taken by build_pairs_kernel).
 __global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, const int* __restrict__ new_ps,
                                     const int4* __restrict__ i0, const int4* __restrict__ i1,
                                     const int4* __restrict__ i2, const double4* __restrict__ g,
-                                    const double4* __restrict__ pr, const double* __restrict__ q,
+                                    const double4* __restrict__ pr, const double* __restrict__ q, double cut,
                                     int4* __restrict__ o0, int4* __restrict__ o1, int4* __restrict__ o2,
                                     double4* __restrict__ og, double4* __restrict__ opr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npair) return;
   const int j = perm[i];
   int4 a = i0[j];
-  const int old_ps = a.z;
+  const int old_ps = a.z, old_np = a.w;
   a.z = new_ps[i];
+  int nk = 0;
+  for (int k = 0; k < old_np; ++k) {
+    const double4* src = pr + 3 * (size_t)(old_ps + k);
+    const double4 r0 = src[0];
+    if (fabs(r0.z) < cut) continue;
+    double4* dst = opr + 3 * (size_t)(a.z + nk);
+    dst[0] = r0;
+    dst[1] = src[1];
+    dst[2] = src[2];
+    ++nk;
+  }
+  a.w = nk;
   o0[i] = a;
   o1[i] = i1[j];
   o2[i] = i2[j];
   double4 gg = g[j];
   gg.w = q[j];
   og[i] = gg;
-  for (int k = 0; k < 3 * a.w; ++k) opr[3 * (size_t)a.z + k] = pr[3 * (size_t)old_ps + k];
 }
 
 void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
-                         const int4* i2, const double4* g, const double4* pr, const double* q, int4* o0,
-                         int4* o1, int4* o2, double4* og, float4*, double4* opr, float4*, cudaStream_t s) {
+                         const int4* i2, const double4* g, const double4* pr, const double* q, double cut,
+                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, cudaStream_t s) {
   if (npair <= 0) return;
-  gather_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, perm, new_pstart, i0, i1, i2, g, pr, q, o0, o1, o2,
-                                                          og, opr);
+  gather_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, perm, new_pstart, i0, i1, i2, g, pr, q, cut, o0,
+                                                          o1, o2, og, opr);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }
@@ -353,10 +373,14 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     }
     const unsigned amask = __ballot_sync(0xffffffffu, active);
     if (amask == 0u) continue;
-    if (A.stats && lane == 0) {
-      atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
-      atomicAdd(A.stats + (2 + args.prec) * NQCLASS + args.qclass,
-                (unsigned long long)__popc(amask) * (unsigned long long)(bi0.w * ki0.w));
+    if (A.stats) {
+      unsigned long long tot = active ? (unsigned long long)(bi0.w * ki0.w) : 0ull;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (lane == 0) {
+        atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
+        atomicAdd(A.stats + (2 + args.prec) * NQCLASS + args.qclass, tot);
+      }
     }
     R out[C::NOUT];
     if (active) {
@@ -539,7 +563,7 @@ struct GradKernelArgs {
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
-  int nbra, ntasks, bra_base, ket_base, same_class;
+  int nbra, ntasks, bra_base, ket_base, same_class, qclass;
 };
 
 template <int LA, int LB, int LC, int LD>
@@ -568,7 +592,18 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
         active = bound >= (float)A.thresh;
       }
     }
-    if (__ballot_sync(0xffffffffu, active) == 0u) continue;
+    const unsigned amask = __ballot_sync(0xffffffffu, active);
+    if (amask == 0u) continue;
+    if (A.stats) {
+      const unsigned long long np = active ? (unsigned long long)(bi0.w * ki0.w) : 0ull;
+      unsigned long long tot = np;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (lane == 0) {
+        atomicAdd(A.stats + args.qclass, (unsigned long long)__popc(amask));
+        atomicAdd(A.stats + NQCLASS + args.qclass, tot);
+      }
+    }
     double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (active) {
       const size_t mo = (size_t)bi2.x;
@@ -657,8 +692,9 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, const
   k.nbra = tl.nbra; k.ntasks = tl.ntasks;
   k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);
+  k.qclass = qclass_of(bc, kc);
   dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
-  switch (qclass_of(bc, kc)) {
+  switch (k.qclass) {
     case 0: grad2e_kernel<0, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
     case 1: grad2e_kernel<1, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
     case 2: grad2e_kernel<1, 0, 1, 0><<<grid, block, 0, s>>>(k); break;

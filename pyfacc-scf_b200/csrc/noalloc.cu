@@ -148,7 +148,7 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
         c.take<int4>(npair); c.take<int4>(npair); c.take<int4>(npair); c.take<double4>(npair);
         c.take<double4>((size_t)3 * nprim);
       }
-      c.take<double>(npair); c.take<int>(npair); c.take<int>(npair);
+      c.take<double>(npair); c.take<int>(npair); c.take<int>(npair); c.take<int>(npair);
       c.take<float>((size_t)ns * ns);
       c.take<int>(ntask_ints);
       return c.off;
@@ -188,6 +188,8 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
     double* d_q = cv.take<double>(npair);
     int* d_perm = cv.take<int>(npair);
     int* d_ps = cv.take<int>(npair);
+    int* d_kept = cv.take<int>(npair);
+    const double cut = PRIM_CUT_REL * max_prim_prefactor(B);
     float* d_dmax = cv.take<float>((size_t)ns * ns);
     int* d_tasks = cv.take<int>((size_t)3 * (npair + 6) * NCLASS);
 
@@ -202,10 +204,12 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
     PF_CUDA(cudaMemcpyAsync(d_pl1, pl1.data(), npair * sizeof(int4), cudaMemcpyHostToDevice, s));
 
     // ---- pair records and Schwarz factors, then sort by Q inside each class
-    launch_build_pairs(shd, npair, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, s);
+    launch_build_pairs(shd, npair, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, cut, d_kept, s);
     launch_schwarz(tmp, off, d_q, s);
     std::vector<double> q(npair);
+    std::vector<int> kept(npair);
     PF_CUDA(cudaMemcpyAsync(q.data(), d_q, npair * sizeof(double), cudaMemcpyDeviceToHost, s));
+    PF_CUDA(cudaMemcpyAsync(kept.data(), d_kept, npair * sizeof(int), cudaMemcpyDeviceToHost, s));
     PF_CUDA(cudaStreamSynchronize(s));
     const double qmax = npair ? *std::max_element(q.begin(), q.end()) : 0.0;
     std::vector<int> perm, new_ps;
@@ -220,7 +224,7 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
       for (int k : idx) {
         perm.push_back(k);
         new_ps.push_back(nprim_new);
-        nprim_new += np[pl0[k].x] * np[pl0[k].y];
+        nprim_new += kept[k];
         qs.push_back(q[k]);
       }
       pd.class_off[c + 1] = (int)perm.size();
@@ -229,8 +233,8 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
     if (pd.npair > 0) {
       PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, s));
       PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, s));
-      launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, pd.info0,
-                          pd.info1, pd.info2, pd.geom, nullptr, pd.prim, nullptr, s);
+      launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, cut,
+                          pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, s);
     }
 
     // ---- task lists (FP64, Schwarz only)

@@ -470,21 +470,21 @@ void System::gradient(double* g_host) {
   g2.thresh = opt.schwarz_thresh;
   g2.uhf = uhf ? 1 : 0;
   g2.grad = grad_dev;
-  st.flops_grad = 0.0;
+  unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
+  PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
+  g2.stats = gstats;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) {
-      launch_grad2e(pd, tasks[bc][kc][0], bc, kc, g2, num_sms, stream);
-      const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
-      // every pair of STO-nG shells has K^2 primitive pairs
-      const double k2 = basis.shells.empty() ? 1.0 : (double)basis.shells[0].ex.size() * basis.shells[0].ex.size();
-      st.flops_grad += (double)tasks[bc][kc][0].nquartets * k2 * k2 *
-                       (class_flops(qc).grad + prim_overhead_flops(qc, false));
-    }
+    for (int kc = bc; kc >= 0; --kc) launch_grad2e(pd, tasks[bc][kc][0], bc, kc, g2, num_sms, stream);
   PF_CUDA(cudaEventRecord(a1, stream));
   std::vector<double> g(3 * natoms, 0.0);
   PF_CUDA(cudaMemcpyAsync(g.data(), grad_dev, 3 * natoms * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   st.ms_grad = elapsed(a0, a1);
+  unsigned long long cnt[2 * NQCLASS];
+  PF_CUDA(cudaMemcpy(cnt, gstats, sizeof(cnt), cudaMemcpyDeviceToHost));
+  st.flops_grad = 0.0;
+  for (int q = 0; q < NQCLASS; ++q)
+    st.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false));
   nuclear_repulsion_gradient(g.data());
   grad_host = g;
   if (g_host) std::memcpy(g_host, g.data(), g.size() * sizeof(double));
