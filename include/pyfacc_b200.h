@@ -38,6 +38,8 @@ extern "C" {
 #define PYFACC_SCF_AUTO                  0 /* RHF if nalpha == nbeta          */
 #define PYFACC_SCF_RHF                   1
 #define PYFACC_SCF_UHF                   2
+#define PYFACC_GUESS_CORE                0 /* core Hamiltonian (rscf.f90:113) */
+#define PYFACC_GUESS_ATOMIC              1 /* atomic aufbau occupations      */
 
 typedef struct pyfacc_options {
   double eps_energy;        /* |E_n - E_{n-1}| < eps_energy          (1e-10) */
@@ -58,6 +60,7 @@ typedef struct pyfacc_options {
   int shard_rank;           /* J/K work shard of this process           (0)   */
   int shard_count;          /* number of shards (1 = whole Fock build)  (1)   */
   const char *data_dir;     /* directory holding basis_set/; NULL = search    */
+  int guess;                /* PYFACC_GUESS_*                        (ATOMIC) */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {

@@ -94,6 +94,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->shard_rank = 0;
   o->shard_count = 1;
   o->data_dir = nullptr;
+  o->guess = PYFACC_GUESS_ATOMIC;
 }
 
 // scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.

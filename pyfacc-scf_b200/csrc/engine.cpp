@@ -417,6 +417,30 @@ void System::build_tasks() {
     }
   task_buf.ensure(std::max<size_t>(hostbuf.size() * sizeof(int), 256));
   int* d = task_buf.as<int>();
+  // device-built lists: same shapes, filled per Fock build
+  size_t dyn_ints = 2 * NQCLASS;
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) dyn_ints += 2 * (3 * (size_t)(pd.class_off[bc + 1] - pd.class_off[bc]) + 1);
+  dyn_buf.ensure(dyn_ints * sizeof(int) + 256);
+  int* dd = dyn_buf.as<int>();
+  dyn.ntasks_dev = dd;
+  dd += 2 * NQCLASS;
+  dyn.dmax_global = reinterpret_cast<double*>(dyn_buf.as<char>() + dyn_ints * sizeof(int) + 128 - (dyn_ints * sizeof(int)) % 128);
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
+      const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
+      for (int part = 0; part < 2; ++part) {
+        TaskList& tl = dyn.lists[2 * qc + part];
+        tl.nbra = nb;
+        tl.ntasks = std::max(1, tasks[bc][kc][0].ntasks);
+        tl.task_off = dd;
+        tl.ket_lo = dd + nb + 1;
+        tl.ket_hi = dd + 2 * nb + 1;
+        tl.ntasks_dev = dyn.ntasks_dev + 2 * qc + part;
+        dd += 3 * nb + 1;
+      }
+    }
   PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
   for (auto& p : pend) {
     TaskList& tl = tasks[p.bc][p.kc][p.prec];

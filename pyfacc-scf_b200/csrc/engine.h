@@ -76,10 +76,11 @@ struct DeviceBuf {
 struct TaskList {
   int nbra = 0;
   long long nquartets = 0;
-  int ntasks = 0;
-  int* task_off = nullptr;  // device, nbra + 1
-  int* ket_lo = nullptr;    // device, nbra
-  int* ket_hi = nullptr;    // device, nbra
+  int ntasks = 0;              // launch bound (the exact count for static lists)
+  int* task_off = nullptr;     // device, nbra + 1
+  int* ket_lo = nullptr;       // device, nbra
+  int* ket_hi = nullptr;       // device, nbra
+  const int* ntasks_dev = nullptr;  // device count of a list built on the GPU
 };
 
 // Packed pair data of one molecule or of a batch (every pair stores the
@@ -158,6 +159,19 @@ struct JkArgs {
 };
 void launch_jk(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, int nk,
                const JkArgs& a, int num_sms, cudaStream_t s);
+
+// Task lists rebuilt on the GPU for one Fock build from the density bound
+// dmax (ns x ns): a bra pair i keeps the ket prefix with
+// Q_i Q_j max|D| >= thresh, the FP64 part being the prefix with
+// Q_i Q_j max|D| >= fp32_thresh (the rest runs in FP32).  lists[2*(combo)+p]
+// for the six class combos (bra >= ket) and p = 0 (FP64), 1 (FP32).
+struct DynTaskSet {
+  TaskList lists[2 * NQCLASS];
+  int* ntasks_dev = nullptr;   // 2 * NQCLASS counts
+  double* dmax_global = nullptr;
+};
+void launch_dyn_tasks(const PairData& pd, const float* dmax, int ns, double thresh, double fp32_thresh,
+                      DynTaskSet& dt, cudaStream_t s);
 
 struct GradArgs {
   const double* Pt;

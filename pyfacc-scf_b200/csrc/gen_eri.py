@@ -214,14 +214,14 @@ def gen_class(la, lb, lc, ld):
     src.append("    (void)AB; (void)CD;")
     src.append("  }")
     # --- gradient (primitive level, contracted with gam), one routine per
-    # centre so that each keeps only its own recursion intermediates live
+    # centre and direction so that each keeps only its own recursion
+    # intermediates live; grad{A,B,C} call the three directions in turn
     grad_flops = 0
     for ctr in range(3):
-        em = Emitter()
-        v = Vrr(em, L + 1)
-        h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
-        g_lines = []
         for x in range(3):
+            em = Emitter()
+            v = Vrr(em, L + 1)
+            h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
             up_terms, dn_terms = [], []
             k = 0
             for a in comps(la):
@@ -246,18 +246,29 @@ def gen_class(la, lb, lc, ld):
                 sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
                 expr += f" - {sd}"
                 fl += 1
-            g_lines.append(f"    g[{x}] += {expr};")
             em.flops += fl
-        grad_flops += em.flops
-        src.append(f"  // centre {'ABC'[ctr]}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
-        src.append(f"  __device__ static __forceinline__ void grad{'ABC'[ctr]}(const R* __restrict__ I, const R* __restrict__ PA,")
+            grad_flops += em.flops
+            name = f"grad{'ABC'[ctr]}{'xyz'[x]}"
+            # the (pp|pp) routines are large enough that one inlined body
+            # exhausts the register file; compiled separately they do not
+            inl = "__noinline__" if L >= 4 else "__forceinline__"
+            src.append(f"  __device__ static {inl} R {name}(const R* __restrict__ I, const R* __restrict__ PA,")
+            src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
+            src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+            src.append("      R tw, const R* __restrict__ gam) {")
+            src.extend(em.lines)
+            src.append(f"    return {expr};")
+            src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+            src.append("    (void)AB; (void)CD;")
+            src.append("  }")
+        c = 'ABC'[ctr]
+        src.append(f"  // centre {c}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
+        src.append(f"  __device__ static __forceinline__ void grad{c}(const R* __restrict__ I, const R* __restrict__ PA,")
         src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
         src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
         src.append("      R tw, const R* __restrict__ gam, R* __restrict__ g) {")
-        src.extend(em.lines)
-        src.extend(g_lines)
-        src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
-        src.append("    (void)AB; (void)CD;")
+        for x in range(3):
+            src.append(f"    g[{x}] += grad{c}{'xyz'[x]}(I, PA, WP, QC, WQ, o2p, rp, o2q, rq, o2pq, AB, CD, tw, gam);")
         src.append("  }")
     src.append(f"  static constexpr int VRR_FLOPS = {vrr_flops};")
     src.append(f"  static constexpr int HRR_FLOPS = {hrr_flops};")

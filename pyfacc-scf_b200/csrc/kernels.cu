@@ -334,6 +334,7 @@ __device__ __forceinline__ float dmax_bound(const float* __restrict__ dm, int ld
 
 struct JkKernelArgs {
   JkArgs a;
+  const int* ntasks_dev;
   const int4* info0;
   const int4* info1;
   const int4* info2;
@@ -352,7 +353,8 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const JkArgs& A = args.a;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+  const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
+  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nw) {
     const int ib = find_bra(args.task_off, args.nbra, t);
     const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
     const int bp = args.bra_base + ib;
@@ -535,6 +537,7 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   if (tl.ntasks <= 0) return;
   JkKernelArgs k;
   k.a = a;
+  k.ntasks_dev = tl.ntasks_dev;
   k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
   k.geom = pd.geom; k.prim = pd.prim;
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
@@ -546,6 +549,136 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
   if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, s, k);
   else jk_dispatch<double>(k.qclass, nk, grid, block, s, k);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// ---------------------------------------------------------------------------
+// Task lists of one Fock build, built on the device (no host round trip).
+// One block per list: per bra a ket prefix by binary search over the ket
+// class's Q (descending), then a block-wide exclusive scan of the task counts.
+// ---------------------------------------------------------------------------
+__global__ void dmax_global_kernel(long long n, const float* __restrict__ dm, double* __restrict__ out) {
+  __shared__ float sh[32];
+  float m = 0.0f;
+  for (long long i = threadIdx.x; i < n; i += blockDim.x) m = fmaxf(m, dm[i]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) m = fmaxf(m, sh[k]);
+    m = fmaxf(m, sh[0]);
+    out[0] = (double)m;
+  }
+}
+
+struct DynListArgs {
+  int nbra, bra_base, ket_base, nket, same, part;  // part 0: FP64, 1: FP32
+  int* task_off;
+  int* ket_lo;
+  int* ket_hi;
+  int* ntasks;
+};
+struct DynAllArgs {
+  DynListArgs l[2 * NQCLASS];
+  const double4* geom;
+  const double* dmax_global;
+  double thresh, fp32_thresh;
+};
+
+__device__ __forceinline__ int ket_prefix(const double4* __restrict__ geom, int ket_base, int nket, double qb, double t) {
+  int lo = 0, hi = nket;  // count of j with qb * Q_j >= t, Q descending
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (qb * geom[ket_base + mid].w >= t) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(1024) dyn_tasks_kernel(const DynAllArgs A) {
+  const DynListArgs& L = A.l[blockIdx.x];
+  __shared__ int wsum[32];
+  __shared__ int carry;
+  const double dm = fmax(A.dmax_global[0], 1e-300);
+  const double t = A.thresh / dm, t64 = A.fp32_thresh / dm;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < L.nbra; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    int cnt = 0;
+    if (i < L.nbra) {
+      const double qb = A.geom[L.bra_base + i].w;
+      int m = ket_prefix(A.geom, L.ket_base, L.nket, qb, t);
+      if (L.same) m = min(m, i + 1);
+      const int m64 = min(ket_prefix(A.geom, L.ket_base, L.nket, qb, t64), m);
+      const int lo = L.part == 0 ? 0 : m64, hi = L.part == 0 ? m64 : m;
+      L.ket_lo[i] = lo;
+      L.ket_hi[i] = hi;
+      cnt = (hi - lo + TASK_WIDTH - 1) / TASK_WIDTH;
+    }
+    // block exclusive scan of cnt
+    int v = cnt;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    if (w == 0) {
+      int x = (lane < (int)(blockDim.x >> 5)) ? wsum[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      wsum[lane] = x;  // inclusive over warps
+    }
+    __syncthreads();
+    const int excl = carry + (w > 0 ? wsum[w - 1] : 0) + v - cnt;
+    if (i < L.nbra) L.task_off[i] = excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + cnt;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    L.task_off[L.nbra] = carry;
+    L.ntasks[0] = carry;
+  }
+}
+
+void launch_dyn_tasks(const PairData& pd, const float* dmax, int ns, double thresh, double fp32_thresh,
+                      DynTaskSet& dt, cudaStream_t s) {
+  dmax_global_kernel<<<1, 1024, 0, s>>>((long long)ns * ns, dmax, dt.dmax_global);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+  DynAllArgs A;
+  A.geom = pd.geom;
+  A.dmax_global = dt.dmax_global;
+  A.thresh = thresh;
+  A.fp32_thresh = fp32_thresh;
+  int k = 0;
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      const int qc = qclass_of(bc, kc);
+      for (int part = 0; part < 2; ++part, ++k) {
+        TaskList& tl = dt.lists[2 * qc + part];
+        DynListArgs& L = A.l[2 * qc + part];
+        L.nbra = tl.nbra;
+        L.bra_base = pd.class_off[bc];
+        L.ket_base = pd.class_off[kc];
+        L.nket = pd.class_off[kc + 1] - pd.class_off[kc];
+        L.same = bc == kc;
+        L.part = part;
+        L.task_off = tl.task_off;
+        L.ket_lo = tl.ket_lo;
+        L.ket_hi = tl.ket_hi;
+        L.ntasks = dt.ntasks_dev + 2 * qc + part;
+      }
+    }
+  dyn_tasks_kernel<<<2 * NQCLASS, 1024, 0, s>>>(A);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }

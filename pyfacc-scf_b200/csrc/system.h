@@ -56,6 +56,8 @@ struct System {
   TaskList tasks[NCLASS][NCLASS][3];  // [bra class][ket class][full fp64 | mixed fp64 | mixed fp32]
   DeviceBuf task_buf;
   long long quartets_total = 0;
+  DynTaskSet dyn;          // per-build task lists (mixed precision)
+  DeviceBuf dyn_buf;
 
   DeviceBuf mats;
   double *S = nullptr, *T = nullptr, *Vm = nullptr, *H = nullptr, *X = nullptr;
@@ -96,7 +98,8 @@ struct System {
   void one_electron();
   // J = J[Dj], K[k] = K[Dk[k]] (precision 0 = fp64, 1 = mixed); screening by
   // Q_ab Q_cd max|D| with the density(ies) given.
-  void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision);
+  void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
+          bool dynamic = false);
   void eri_tensor(double* eri);
   void orthogonalizer();
   void diagonalize(const double* Fm, double* C, double* eps);
@@ -106,6 +109,9 @@ struct System {
   bool purify(const double* Fm, int nocc, double scale, double* Pm);
   void density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps);
   void final_orbitals();
+  // Diagonal starting density from atomic aufbau occupations of the
+  // minimal-basis shells (total electrons, spread over 2 s / 6 p per shell).
+  std::vector<double> atomic_occupations() const;
   void run_scf();
   void gradient(double* g_host);
   void fill_result(pyfacc_result* r);

@@ -129,6 +129,11 @@ def _options(**kw) -> N.Options:
         kw["boys_mode"] = {"accurate": N.BOYS_ACCURATE, "reference_trapezoid": N.BOYS_REFERENCE_TRAPEZOID}[bm]
     elif bm is not None:
         kw["boys_mode"] = bm
+    gs = kw.pop("guess", None)
+    if isinstance(gs, str):
+        kw["guess"] = {"core": N.GUESS_CORE, "atomic": N.GUESS_ATOMIC}[gs]
+    elif gs is not None:
+        kw["guess"] = gs
     st = kw.pop("scf_type", None)
     if isinstance(st, str):
         kw["scf_type"] = {"auto": N.SCF_AUTO, "rhf": N.SCF_RHF, "uhf": N.SCF_UHF}[st.lower()]

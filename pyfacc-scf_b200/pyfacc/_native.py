@@ -35,6 +35,7 @@ BOYS_REFERENCE_TRAPEZOID = 1
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 SCF_AUTO, SCF_RHF, SCF_UHF = 0, 1, 2
+GUESS_CORE, GUESS_ATOMIC = 0, 1
 
 
 class Options(ctypes.Structure):
@@ -44,7 +45,7 @@ class Options(ctypes.Structure):
         ("boys_mode", c_int), ("schwarz_thresh", c_double), ("fp32_thresh", c_double),
         ("incremental", c_int), ("rebuild_every", c_int), ("compute_gradient", c_int),
         ("device", c_int), ("verbose", c_int), ("shard_rank", c_int), ("shard_count", c_int),
-        ("data_dir", c_char_p),
+        ("data_dir", c_char_p), ("guess", c_int),
     ]
 
 
