@@ -61,6 +61,8 @@ typedef struct pyfacc_options {
   int shard_count;          /* number of shards (1 = whole Fock build)  (1)   */
   const char *data_dir;     /* directory holding basis_set/; NULL = search    */
   int guess;                /* PYFACC_GUESS_*                        (ATOMIC) */
+  double incremental_thresh;/* screening of the incremental dP builds of
+                               mixed mode; <= 0: schwarz_thresh      (1e-11) */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {

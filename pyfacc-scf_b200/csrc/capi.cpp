@@ -95,6 +95,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->shard_count = 1;
   o->data_dir = nullptr;
   o->guess = PYFACC_GUESS_ATOMIC;
+  o->incremental_thresh = 1e-11;
 }
 
 // scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.

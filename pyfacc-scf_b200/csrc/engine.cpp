@@ -340,7 +340,8 @@ void System::build_pairs() {
   o = 0;
   const size_t f_i0 = carve(pd.npair * sizeof(int4)), f_i1 = carve(pd.npair * sizeof(int4)),
                f_i2 = carve(pd.npair * sizeof(int4)), f_g = carve(pd.npair * sizeof(double4)),
-               f_pr = carve((size_t)std::max(nprim_new, 1) * 3 * sizeof(double4));
+               f_pr = carve((size_t)std::max(nprim_new, 1) * 3 * sizeof(double4)),
+               f_prf = carve((size_t)std::max(nprim_new, 1) * 3 * sizeof(float4));
   pd.buf.ensure(std::max<size_t>(o, 256));
   char* pb = pd.buf.as<char>();
   pd.info0 = reinterpret_cast<int4*>(pb + f_i0);
@@ -348,11 +349,12 @@ void System::build_pairs() {
   pd.info2 = reinterpret_cast<int4*>(pb + f_i2);
   pd.geom = reinterpret_cast<double4*>(pb + f_g);
   pd.prim = reinterpret_cast<double4*>(pb + f_pr);
+  pd.primf = reinterpret_cast<float4*>(pb + f_prf);
   if (pd.npair > 0) {
     PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
     PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
     launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, cut,
-                        pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, stream);
+                        pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, pd.primf, stream);
   }
   PF_CUDA(cudaStreamSynchronize(stream));
   build_tasks();

@@ -94,6 +94,7 @@ struct PairData {
   int4* info2 = nullptr;     // {mat_off lo, mat_off hi, ld, molecule}
   double4* geom = nullptr;   // {ABx, ABy, ABz, Q}
   double4* prim = nullptr;   // 3 per primitive pair
+  float4* primf = nullptr;   // the same records in float (FP32 quartets)
   std::vector<double> q_host;   // Q of the sorted pairs
   std::vector<int> cls_host;    // class of the sorted pairs
   std::vector<int> mol_host;    // molecule of the sorted pairs
@@ -139,7 +140,7 @@ void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const in
 void launch_schwarz(const PairData& pd, int npair_class_begin[NCLASS + 1], double* q, cudaStream_t s);
 void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
                          const int4* i2, const double4* g, const double4* pr, const double* q, double cut,
-                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, cudaStream_t s);
+                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, float4* oprf, cudaStream_t s);
 // Largest primitive-pair prefactor |K| of a basis (reached at |AB| = 0) and
 // the relative cut below which primitive pairs are dropped.
 double max_prim_prefactor(const Basis& b);
@@ -184,7 +185,7 @@ struct GradArgs {
   double* grad;  // natoms*3 (packed over a batch via the pair's atom index)
   unsigned long long* stats;  // [0..5] quartets, [6..11] primitive quartets per class, or null
 };
-void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, const GradArgs& a,
+void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, const GradArgs& a,
                    int num_sms, cudaStream_t s);
 
 void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, int nbf,

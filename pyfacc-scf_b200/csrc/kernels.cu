@@ -168,10 +168,13 @@ struct PrimGeo {
   R o2p, rp, o2q, rq, o2pq;
 };
 
-// bra record b0..b2 and ket record k0..k2 (double4 x 3 each)
-template <typename R, int LM>
-__device__ __forceinline__ void prim_setup(const double4& b0, const double4& b1, const double4& k0,
-                                           const double4& k1, PrimGeo<R>& g) {
+template <typename R> struct Rec;  // primitive-pair record vector of a precision
+template <> struct Rec<double> { using T = double4; };
+template <> struct Rec<float> { using T = float4; };
+
+// bra record b0..b2 and ket record k0..k2 (3 vectors each)
+template <typename R, int LM, typename V>
+__device__ __forceinline__ void prim_setup(const V& b0, const V& b1, const V& k0, const V& k1, PrimGeo<R>& g) {
   const R p = (R)b0.x, q = (R)k0.x;
   const R PQx = (R)(b1.x - k1.x), PQy = (R)(b1.y - k1.y), PQz = (R)(b1.z - k1.z);
   const R zeta = p + q;
@@ -201,22 +204,25 @@ __device__ __forceinline__ void prim_setup(const double4& b0, const double4& b1,
 
 template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
 
-// Contracted (ab|cd) for one bra pair and one ket pair.
+// Contracted (ab|cd) for one bra pair and one ket pair (records of the
+// kernel's precision: double4 for FP64 quartets, float4 for FP32 ones).
 template <typename R, int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void contracted_quartet(const double4* __restrict__ prim, int4 bi0, int4 ki0,
+__device__ __forceinline__ void contracted_quartet(const typename Rec<R>::T* __restrict__ prim, int4 bi0, int4 ki0,
                                                    const double4& bgeo, const double4& kgeo,
                                                    R out[EriClass<R, LA, LB, LC, LD>::NOUT]) {
   using C = EriClass<R, LA, LB, LC, LD>;
+  using V = typename Rec<R>::T;
   R acc[C::NACC];
 #pragma unroll
   for (int i = 0; i < C::NACC; ++i) acc[i] = (R)0;
   for (int kq = 0; kq < ki0.w; ++kq) {
-    const double4* kr = prim + 3 * (size_t)(ki0.z + kq);
-    const double4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const V* kr = prim + 3 * (size_t)(ki0.z + kq);
+    const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
     const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+#pragma unroll 1
     for (int kp = 0; kp < bi0.w; ++kp) {
-      const double4* br = prim + 3 * (size_t)(bi0.z + kp);
-      const double4 b0 = br[0], b1 = br[1], b2 = br[2];
+      const V* br = prim + 3 * (size_t)(bi0.z + kp);
+      const V b0 = br[0], b1 = br[1], b2 = br[2];
       const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
       PrimGeo<R> g;
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
@@ -268,7 +274,8 @@ __global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, con
                                     const int4* __restrict__ i2, const double4* __restrict__ g,
                                     const double4* __restrict__ pr, const double* __restrict__ q, double cut,
                                     int4* __restrict__ o0, int4* __restrict__ o1, int4* __restrict__ o2,
-                                    double4* __restrict__ og, double4* __restrict__ opr) {
+                                    double4* __restrict__ og, double4* __restrict__ opr,
+                                    float4* __restrict__ oprf) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npair) return;
   const int j = perm[i];
@@ -281,9 +288,16 @@ __global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, con
     const double4 r0 = src[0];
     if (fabs(r0.z) < cut) continue;
     double4* dst = opr + 3 * (size_t)(a.z + nk);
+    const double4 r1 = src[1], r2 = src[2];
     dst[0] = r0;
-    dst[1] = src[1];
-    dst[2] = src[2];
+    dst[1] = r1;
+    dst[2] = r2;
+    if (oprf) {
+      float4* df = oprf + 3 * (size_t)(a.z + nk);
+      df[0] = make_float4((float)r0.x, (float)r0.y, (float)r0.z, (float)r0.w);
+      df[1] = make_float4((float)r1.x, (float)r1.y, (float)r1.z, 0.0f);
+      df[2] = make_float4((float)r2.x, (float)r2.y, (float)r2.z, 0.0f);
+    }
     ++nk;
   }
   a.w = nk;
@@ -297,10 +311,10 @@ __global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, con
 
 void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
                          const int4* i2, const double4* g, const double4* pr, const double* q, double cut,
-                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, cudaStream_t s) {
+                         int4* o0, int4* o1, int4* o2, double4* og, double4* opr, float4* oprf, cudaStream_t s) {
   if (npair <= 0) return;
   gather_pairs_kernel<<<(npair + 127) / 128, 128, 0, s>>>(npair, perm, new_pstart, i0, i1, i2, g, pr, q, cut, o0,
-                                                          o1, o2, og, opr);
+                                                          o1, o2, og, opr, oprf);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }
@@ -340,11 +354,16 @@ struct JkKernelArgs {
   const int4* info2;
   const double4* geom;
   const double4* prim;
+  const float4* primf;
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec;
 };
+
+template <typename R> __device__ __forceinline__ const typename Rec<R>::T* records(const JkKernelArgs& a);
+template <> __device__ __forceinline__ const double4* records<double>(const JkKernelArgs& a) { return a.prim; }
+template <> __device__ __forceinline__ const float4* records<float>(const JkKernelArgs& a) { return a.primf; }
 
 template <typename R, int LA, int LB, int LC, int LD, int NK>
 __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
@@ -386,7 +405,7 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     }
     R out[C::NOUT];
     if (active) {
-      contracted_quartet<R, LA, LB, LC, LD>(args.prim, bi0, ki0, bg, kg, out);
+      contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out);
     } else {
 #pragma unroll
       for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
@@ -539,7 +558,8 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   k.a = a;
   k.ntasks_dev = tl.ntasks_dev;
   k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
-  k.geom = pd.geom; k.prim = pd.prim;
+  k.geom = pd.geom; k.prim = pd.prim; k.primf = pd.primf;
+  if (fp32 && !pd.primf) throw Error(PYFACC_ERR_INVALID, "FP32 quartets need float primitive records");
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
   k.nbra = tl.nbra; k.ntasks = tl.ntasks;
   k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
@@ -693,15 +713,21 @@ struct GradKernelArgs {
   const int4* info2;
   const double4* geom;
   const double4* prim;
+  const float4* primf;
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass;
 };
 
-template <int LA, int LB, int LC, int LD>
+template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
+template <> __device__ __forceinline__ const double4* grecords<double>(const GradKernelArgs& a) { return a.prim; }
+template <> __device__ __forceinline__ const float4* grecords<float>(const GradKernelArgs& a) { return a.primf; }
+
+template <typename R, int LA, int LB, int LC, int LD>
 __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) {
-  using C = EriClass<double, LA, LB, LC, LD>;
+  using C = EriClass<R, LA, LB, LC, LD>;
+  using V = typename Rec<R>::T;
   constexpr int NA = NC<LA>::v, NB = NC<LB>::v, NCc = NC<LC>::v, ND = NC<LD>::v;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -742,7 +768,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const size_t mo = (size_t)bi2.x;
       const int ld = bi2.y;
       const int ma = bi0.x, mb = bi0.y, mc = ki0.x, md = ki0.y;
-      double gam[C::NOUT];
+      R gam[C::NOUT];
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -765,25 +791,28 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
                 v -= 0.25 * (__ldg(Pt + mu * ld + la) * __ldg(Pt + nu * ld + si) +
                              __ldg(Pt + mu * ld + si) * __ldg(Pt + nu * ld + la));
               }
-              gam[((a * NB + b) * NCc + c) * ND + d] = v;
+              gam[((a * NB + b) * NCc + c) * ND + d] = (R)v;
             }
-      const double AB[3] = {bg.x, bg.y, bg.z};
-      const double CD[3] = {kg.x, kg.y, kg.z};
+      const R AB[3] = {(R)bg.x, (R)bg.y, (R)bg.z};
+      const R CD[3] = {(R)kg.x, (R)kg.y, (R)kg.z};
+      R gr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      const V* prim = grecords<R>(args);
       for (int kq = 0; kq < ki0.w; ++kq) {
-        const double4* kr = args.prim + 3 * (size_t)(ki0.z + kq);
-        const double4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
-        const double QC[3] = {k2.x, k2.y, k2.z};
+        const V* kr = prim + 3 * (size_t)(ki0.z + kq);
+        const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+        const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
         for (int kpp = 0; kpp < bi0.w; ++kpp) {
-          const double4* br = args.prim + 3 * (size_t)(bi0.z + kpp);
-          const double4 b0 = br[0], b1 = br[1], b2 = br[2];
-          const double PA[3] = {b2.x, b2.y, b2.z};
-          PrimGeo<double> pg;
-          prim_setup<double, C::L + 1>(b0, b1, k0, k1, pg);
-          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * b0.w, gam, g);
-          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * (b0.x - b0.w),
-                   gam, g + 3);
-          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, 2.0 * k0.w, gam,
-                   g + 6);
+          const V* br = prim + 3 * (size_t)(bi0.z + kpp);
+          const V b0 = br[0], b1 = br[1], b2 = br[2];
+          const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
+          PrimGeo<R> pg;
+          prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
+          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, (R)(2 * b0.w), gam,
+                   gr);
+          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD,
+                   (R)(2 * (b0.x - b0.w)), gam, gr + 3);
+          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, (R)(2 * k0.w), gam,
+                   gr + 6);
         }
       }
       double fac = 4.0;
@@ -791,7 +820,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       if (ki1.x == ki1.y) fac *= 0.5;
       if (args.same_class && bp == kp) fac *= 0.5;
 #pragma unroll
-      for (int i = 0; i < 9; ++i) g[i] *= fac;
+      for (int i = 0; i < 9; ++i) g[i] = fac * (double)gr[i];
     }
     // centre A and B are the bra's, uniform across the warp
     double* G = A.grad;
@@ -814,27 +843,34 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   }
 }
 
-void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, const GradArgs& a, int num_sms,
-                   cudaStream_t s) {
+template <typename R>
+static void grad2e_dispatch(int qc, dim3 grid, dim3 block, cudaStream_t s, const GradKernelArgs& k) {
+  switch (qc) {
+    case 0: grad2e_kernel<R, 0, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 1: grad2e_kernel<R, 1, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 2: grad2e_kernel<R, 1, 0, 1, 0><<<grid, block, 0, s>>>(k); break;
+    case 3: grad2e_kernel<R, 1, 1, 0, 0><<<grid, block, 0, s>>>(k); break;
+    case 4: grad2e_kernel<R, 1, 1, 1, 0><<<grid, block, 0, s>>>(k); break;
+    default: grad2e_kernel<R, 1, 1, 1, 1><<<grid, block, 0, s>>>(k); break;
+  }
+}
+
+void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32, const GradArgs& a,
+                   int num_sms, cudaStream_t s) {
   if (tl.ntasks <= 0) return;
   GradKernelArgs k;
   k.a = a;
   k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
-  k.geom = pd.geom; k.prim = pd.prim;
+  k.geom = pd.geom; k.prim = pd.prim; k.primf = pd.primf;
+  if (fp32 && !pd.primf) throw Error(PYFACC_ERR_INVALID, "FP32 quartets need float primitive records");
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
   k.nbra = tl.nbra; k.ntasks = tl.ntasks;
   k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
   dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
-  switch (k.qclass) {
-    case 0: grad2e_kernel<0, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 1: grad2e_kernel<1, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 2: grad2e_kernel<1, 0, 1, 0><<<grid, block, 0, s>>>(k); break;
-    case 3: grad2e_kernel<1, 1, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 4: grad2e_kernel<1, 1, 1, 0><<<grid, block, 0, s>>>(k); break;
-    default: grad2e_kernel<1, 1, 1, 1><<<grid, block, 0, s>>>(k); break;
-  }
+  if (fp32) grad2e_dispatch<float>(k.qclass, grid, block, s, k);
+  else grad2e_dispatch<double>(k.qclass, grid, block, s, k);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }

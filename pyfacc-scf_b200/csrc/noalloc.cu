@@ -234,7 +234,7 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
       PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, s));
       PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, s));
       launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, cut,
-                          pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, s);
+                          pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, nullptr, s);
     }
 
     // ---- task lists (FP64, Schwarz only)

@@ -51,7 +51,8 @@ void System::one_electron() {
 // density-weighted Schwarz test, the six class kernels (FP64 task lists, or
 // the FP64 and FP32 halves of the mixed lists), then J = Jh + Jh^T.
 void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-                bool dynamic) {
+                bool dynamic, double thresh) {
+  if (thresh <= 0) thresh = opt.schwarz_thresh;
   const size_t n2 = (size_t)nbf * nbf;
   launch_zero(Jo, n2 * sizeof(double), stream);
   for (int k = 0; k < nk; ++k) launch_zero(Ko[k], n2 * sizeof(double), stream);
@@ -63,12 +64,12 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   a.J = Jo;
   a.K0 = Ko[0];
   a.K1 = nk > 1 ? Ko[1] : Ko[0];
-  a.dmax = (opt.schwarz_thresh > 0) ? dmax : nullptr;
+  a.dmax = (thresh > 0) ? dmax : nullptr;
   a.ns_ld = ns;
-  a.thresh = opt.schwarz_thresh;
+  a.thresh = thresh;
   a.stats = stats_dev;
   const bool mixed = precision == PYFACC_PRECISION_MIXED;
-  if (dynamic) launch_dyn_tasks(pd, dmax, ns, opt.schwarz_thresh, mixed ? opt.fp32_thresh : 0.0, dyn, stream);
+  if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? opt.fp32_thresh : 0.0, dyn, stream);
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
@@ -254,6 +255,11 @@ void System::run_scf() {
   const double pscale = uhf ? 1.0 : 2.0;
   const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
   const bool incremental = opt.incremental < 0 ? mixed : (opt.incremental != 0);
+  // Incremental builds of mixed mode may screen harder: the reported energy
+  // comes from a full FP64 build at the converged density, and an error
+  // delta in F only moves that density by O(delta), the energy by O(delta^2).
+  const double inc_thresh =
+      (mixed && opt.incremental_thresh > 0) ? std::max(opt.incremental_thresh, opt.schwarz_thresh) : opt.schwarz_thresh;
   st = ScfState();
   PF_CUDA(cudaMemsetAsync(stats_dev, 0, sizeof(JkStats), stream));
   cudaEvent_t t0, t1, a0, a1;
@@ -329,9 +335,9 @@ void System::run_scf() {
       if (uhf) {
         launch_axpby((long long)n2, 1.0, dP[0], 0.0, Wm, stream);
         launch_axpby((long long)n2, 1.0, dP[1], 1.0, Wm, stream);
-        jk(Wm, 2, dPc, W1, dK, opt.precision, mixed);
+        jk(Wm, 2, dPc, W1, dK, opt.precision, mixed, inc_thresh);
       } else {
-        jk(dP[0], 1, dPc, W1, dK, opt.precision, mixed);
+        jk(dP[0], 1, dPc, W1, dK, opt.precision, mixed, inc_thresh);
       }
       launch_axpby((long long)n2, 1.0, W1, 1.0, J, stream);
       for (int s = 0; s < nsp; ++s) launch_axpby((long long)n2, 1.0, dK[s], 1.0, K[s], stream);
@@ -547,8 +553,19 @@ void System::gradient(double* g_host) {
   unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
   PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
   g2.stats = gstats;
+  // The derivative integrals run in FP64 in both precisions: on B200 the
+  // FP32 instantiation (grad_fp32 option) measured no faster, being bound
+  // by memory latency rather than by the FP64 pipe.
+  const bool split = opt.precision == PYFACC_PRECISION_MIXED && grad_fp32;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) launch_grad2e(pd, tasks[bc][kc][0], bc, kc, g2, num_sms, stream);
+    for (int kc = bc; kc >= 0; --kc) {
+      if (split) {
+        launch_grad2e(pd, tasks[bc][kc][1], bc, kc, false, g2, num_sms, stream);
+        launch_grad2e(pd, tasks[bc][kc][2], bc, kc, true, g2, num_sms, stream);
+      } else {
+        launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
+      }
+    }
   PF_CUDA(cudaEventRecord(a1, stream));
   std::vector<double> g(3 * natoms, 0.0);
   PF_CUDA(cudaMemcpyAsync(g.data(), grad_dev, 3 * natoms * sizeof(double), cudaMemcpyDeviceToHost, stream));

@@ -68,6 +68,7 @@ struct System {
   double *Pu[3] = {nullptr, nullptr, nullptr};  // purification work matrices
   double* pstate = nullptr;                      // TC2 state (device)
   bool orbitals_ready = false;
+  bool grad_fp32 = false;  // FP32 derivative integrals for small quartets (mixed)
   int purify_steps = 0, purify_fallbacks = 0;
   float* dmax = nullptr;
   std::vector<double*> diis_F, diis_E;
@@ -99,7 +100,7 @@ struct System {
   // J = J[Dj], K[k] = K[Dk[k]] (precision 0 = fp64, 1 = mixed); screening by
   // Q_ab Q_cd max|D| with the density(ies) given.
   void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-          bool dynamic = false);
+          bool dynamic = false, double thresh = -1.0);
   void eri_tensor(double* eri);
   void orthogonalizer();
   void diagonalize(const double* Fm, double* C, double* eps);

@@ -243,9 +243,9 @@ class System:
         self.nbf, self.nshell, self.natoms, self.npairs = nbf.value, ns.value, na.value, npair.value
 
     def close(self):
-        if getattr(self, "handle", None):
-            lib().pyfacc_system_destroy(self.handle)
-            self.handle = None
+        if getattr(self, "handle", None) and N is not None and N._lib is not None:
+            N._lib.pyfacc_system_destroy(self.handle)
+        self.handle = None
 
     __del__ = close
 

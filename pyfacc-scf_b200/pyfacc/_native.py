@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
         ("boys_mode", c_int), ("schwarz_thresh", c_double), ("fp32_thresh", c_double),
         ("incremental", c_int), ("rebuild_every", c_int), ("compute_gradient", c_int),
         ("device", c_int), ("verbose", c_int), ("shard_rank", c_int), ("shard_count", c_int),
-        ("data_dir", c_char_p), ("guess", c_int),
+        ("data_dir", c_char_p), ("guess", c_int), ("incremental_thresh", c_double),
     ]
 
 
