@@ -455,7 +455,7 @@ void System::build_tasks() {
 
 void System::alloc_matrices() {
   const size_t n2 = (size_t)nbf * nbf;
-  const int nmat = 27 + 4 * std::max(opt.diis_size, 1);
+  const int nmat = 28 + 4 * std::max(opt.diis_size, 1);
   mats.ensure(nmat * n2 * sizeof(double) + 64 * sizeof(double) + ns * ns * sizeof(float) + 1024);
   double* m = mats.as<double>();
   auto take = [&]() { double* r = m; m += n2; return r; };
@@ -464,7 +464,7 @@ void System::alloc_matrices() {
   P[0] = take(); P[1] = take(); Pbuilt[0] = take(); Pbuilt[1] = take(); Pold[0] = take(); Pold[1] = take();
   W1 = take(); W2 = take(); W3 = take(); Err[0] = take(); Err[1] = take(); Cm[0] = take(); Cm[1] = take();
   Wm = take();
-  Pu[0] = take(); Pu[1] = take(); Pu[2] = take();
+  Pu[0] = take(); Pu[1] = take(); Pu[2] = take(); Pu[3] = take();
   const int nd = std::max(opt.diis_size, 1);
   for (int i = 0; i < nd; ++i) {
     diis_F.push_back(m); m += 2 * n2;

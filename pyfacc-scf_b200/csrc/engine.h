@@ -233,7 +233,8 @@ void launch_zero(void* p, size_t bytes, cudaStream_t s);
 // TC2 purification helpers (state: l_min, l_max, Tr X, Tr X^2, converged, steps)
 void launch_gersh(int n, const double* F, double* state, cudaStream_t s);
 void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s);
-void launch_tc2_step(int n, double nocc, double* X, const double* X2, double* state, cudaStream_t s);
+void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, double* Xout, const double* sin,
+                     double* sout, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
 

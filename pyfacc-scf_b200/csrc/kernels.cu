@@ -1446,20 +1446,22 @@ __global__ void tc2_init_kernel(long long n2, int n, const double* __restrict__ 
   }
 }
 
-// One TC2 step on X given X2 = X*X: traces, choice, update, convergence.
-// Once Tr X - Tr X^2 < 1e-9 two more steps run (quadratic convergence takes
-// the remainder to round-off), then X is left unchanged.
-__global__ void tc2_step_kernel(int n, double nocc, double* __restrict__ X, const double* __restrict__ X2,
-                                double* __restrict__ state) {
+// One TC2 step, out of place: Xout = a Xin + b X2 with X2 = Xin Xin.
+// Every block reduces the two traces from the diagonals itself (the same
+// reduction order in every block, so all blocks take the same decision) and
+// updates its grid-stride share; block 0 writes the next state into the
+// other state buffer (sin and sout alternate), so no block reads a value
+// written during the same launch.  Once Tr X - Tr X^2 < 1e-9 two more steps
+// run (quadratic convergence takes the rest to round-off); afterwards X is
+// copied unchanged.
+__global__ void tc2_step_kernel(int n, double nocc, const double* __restrict__ Xin, const double* __restrict__ X2,
+                                double* __restrict__ Xout, const double* __restrict__ sin, double* __restrict__ sout) {
   __shared__ double s1[32], s2[32];
   __shared__ double coef[2];
-  __shared__ int skip;
-  if (threadIdx.x == 0) skip = state[4] != 0.0;
-  __syncthreads();
-  if (skip) return;
+  __shared__ int done;
   double t1 = 0.0, t2 = 0.0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    t1 += X[(size_t)i * n + i];
+    t1 += Xin[(size_t)i * n + i];
     t2 += X2[(size_t)i * n + i];
   }
   t1 = warp_sum(t1);
@@ -1470,23 +1472,41 @@ __global__ void tc2_step_kernel(int n, double nocc, double* __restrict__ X, cons
   if (threadIdx.x == 0) {
     t1 = 0.0; t2 = 0.0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { t1 += s1[k]; t2 += s2[k]; }
-    state[2] = t1;
-    state[3] = t2;
-    state[5] += 1.0;
+    const bool was_done = sin[4] != 0.0;
+    double countdown = sin[6];
+    bool now_done = was_done;
+    if (!was_done) {
+      if (countdown > 0.0) {
+        countdown -= 1.0;
+        if (countdown <= 0.0) now_done = true;
+      } else if (t1 - t2 < 1e-9 && fabs(t1 - nocc) < 1e-6) {
+        countdown = 2.0;
+      }
+    }
+    done = was_done;
     // X <- X^2 takes the trace to t2, X <- 2X - X^2 to 2 t1 - t2
     if (fabs(t2 - nocc) < fabs(2.0 * t1 - t2 - nocc)) { coef[0] = 0.0; coef[1] = 1.0; }
     else { coef[0] = 2.0; coef[1] = -1.0; }
-    if (state[6] > 0.0) {
-      state[6] -= 1.0;
-      if (state[6] <= 0.0) state[4] = 1.0;
-    } else if (t1 - t2 < 1e-9 && fabs(t1 - nocc) < 1e-6) {
-      state[6] = 2.0;
+    if (blockIdx.x == 0) {
+      sout[0] = sin[0];
+      sout[1] = sin[1];
+      sout[2] = t1;
+      sout[3] = t2;
+      sout[4] = now_done ? 1.0 : 0.0;
+      sout[5] = sin[5] + (was_done ? 0.0 : 1.0);
+      sout[6] = countdown;
     }
   }
   __syncthreads();
-  const double a = coef[0], b = coef[1];
   const long long n2 = (long long)n * n;
-  for (long long k = threadIdx.x; k < n2; k += blockDim.x) X[k] = a * X[k] + b * X2[k];
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  if (done) {
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += stride) Xout[k] = Xin[k];
+    return;
+  }
+  const double a = coef[0], b = coef[1];
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += stride)
+    Xout[k] = a * Xin[k] + b * X2[k];
 }
 
 void launch_gersh(int n, const double* F, double* state, cudaStream_t s) {
@@ -1501,8 +1521,11 @@ void launch_tc2_init(int n, const double* F, const double* state, double* X, cud
   PF_CUDA(cudaGetLastError());
   count_launch();
 }
-void launch_tc2_step(int n, double nocc, double* X, const double* X2, double* state, cudaStream_t s) {
-  tc2_step_kernel<<<1, 1024, 0, s>>>(n, nocc, X, X2, state);
+void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, double* Xout, const double* sin,
+                     double* sout, cudaStream_t s) {
+  const long long n2 = (long long)n * n;
+  const int blocks = (int)std::max<long long>(1, std::min<long long>((n2 + 511) / 512, 296));
+  tc2_step_kernel<<<blocks, 512, 0, s>>>(n, nocc, Xin, X2, Xout, sin, sout);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }

@@ -174,21 +174,31 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
     return true;
   }
   double* Fp = Pu[0];
-  double* Xp = Pu[1];
+  double* Xa = Pu[1];
+  double* Xb = Pu[3];
   double* X2 = Pu[2];
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
-  launch_gersh(nbf, Fp, pstate, stream);
-  launch_tc2_init(nbf, Fp, pstate, Xp, stream);
-  const int chunk = 8, kmax = 200;
-  double st_h[8];
+  double* S0 = pstate;
+  double* S1 = pstate + 8;
+  launch_gersh(nbf, Fp, S0, stream);
+  launch_tc2_init(nbf, Fp, S0, Xa, stream);
+  // check after 16 steps, then every 4 (TC2 converges quadratically once the
+  // eigenvalues approach 0 and 1; converged steps only copy X)
+  const int kmax = 200;
+  double st_h[8] = {0};
   bool ok = false;
-  for (int k = 0; k < kmax; k += chunk) {
-    for (int j = 0; j < chunk; ++j) {
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Xp, nbf, Xp, nbf, &zero, X2, nbf));
-      launch_tc2_step(nbf, (double)nocc, Xp, X2, pstate, stream);
+  int k = 0;
+  double* cur = Xa;
+  double* nxt = Xb;
+  while (k < kmax) {
+    const int chunk = (k == 0) ? 16 : 4;
+    for (int j = 0; j < chunk; ++j, ++k) {
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, X2, nbf));
+      launch_tc2_step(nbf, (double)nocc, cur, X2, nxt, (k % 2) ? S1 : S0, (k % 2) ? S0 : S1, stream);
+      std::swap(cur, nxt);
     }
-    PF_CUDA(cudaMemcpyAsync(st_h, pstate, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaMemcpyAsync(st_h, (k % 2) ? S1 : S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
     if (st_h[4] != 0.0) {
       ok = true;
@@ -197,6 +207,7 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   }
   purify_steps += (int)st_h[5];
   if (!ok) return false;
+  double* Xp = cur;
   // P = scale * X Xp X^T
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));
