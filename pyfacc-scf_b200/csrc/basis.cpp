@@ -18,6 +18,7 @@
 #include <sstream>
 
 #include "engine.h"
+#include "pool.h"
 
 namespace pyfacc {
 
@@ -77,12 +78,18 @@ static std::string trim(const std::string& s) {
   return s.substr(a, b - a);
 }
 
-Basis build_basis(const std::string& basis_file, const std::vector<std::string>& species,
-                  const std::vector<double>& xyz) {
-  std::ifstream in(basis_file);
-  if (!in) throw Error(PYFACC_ERR_BASIS_NOT_FOUND, "cannot open " + basis_file);
+static std::vector<std::string> read_lines(const std::string& path) {
+  std::ifstream in(path);
+  if (!in) throw Error(PYFACC_ERR_BASIS_NOT_FOUND, "cannot open " + path);
   std::vector<std::string> lines;
   for (std::string ln; std::getline(in, ln);) lines.push_back(ln);
+  return lines;
+}
+
+Basis build_basis(const std::string& basis_file, const std::vector<std::string>& species,
+                  const std::vector<double>& xyz) {
+  const auto text = basis_lines(basis_file, &read_lines);
+  const std::vector<std::string>& lines = *text;
   Basis B;
   const int natoms = (int)species.size();
   std::vector<int> seen(natoms, 0);

@@ -23,6 +23,7 @@
 #include <numeric>
 
 #include "engine.h"
+#include "pool.h"
 #include "system.h"
 
 namespace pyfacc {
@@ -30,11 +31,12 @@ namespace pyfacc {
 void DeviceBuf::ensure(size_t b) {
   if (b <= bytes) return;
   release();
-  PF_CUDA(cudaMalloc(&p, b));
-  bytes = b;
+  size_t got = 0;
+  p = pool_alloc(b, &got);
+  bytes = got;
 }
 void DeviceBuf::release() {
-  if (p) cudaFree(p);
+  if (p) pool_free(p, bytes);
   p = nullptr;
   bytes = 0;
 }
@@ -63,17 +65,14 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
   } else {
     PF_CUDA(cudaGetDevice(&device));
   }
-  cudaDeviceProp prop;
-  PF_CUDA(cudaGetDeviceProperties(&prop, device));
-  num_sms = prop.multiProcessorCount;
+  PF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
   ensure_boys_tables(device);
-  PF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-  PF_CUBLAS(cublasCreate(&cublas));
-  PF_CUBLAS(cublasSetStream(cublas, stream));
-  PF_CUSOLVER(cusolverDnCreate(&cusolver));
-  PF_CUSOLVER(cusolverDnSetStream(cusolver, stream));
-  PF_CUDA(cudaEventCreate(&ev0));
-  PF_CUDA(cudaEventCreate(&ev1));
+  ctx = context_acquire(device);
+  stream = ctx.stream;
+  cublas = ctx.cublas;
+  cusolver = ctx.cusolver;
+  ev0 = ctx.ev0;
+  ev1 = ctx.ev1;
 
   natoms = m.natoms;
   Z.assign(m.z, m.z + natoms);
@@ -111,12 +110,9 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
 
 System::~System() {
   cudaSetDevice(device);
-  if (cublas) cublasDestroy(cublas);
-  if (cusolver) cusolverDnDestroy(cusolver);
-  if (ev0) cudaEventDestroy(ev0);
-  if (ev1) cudaEventDestroy(ev1);
+  if (stream) cudaStreamSynchronize(stream);
   release_extra();
-  if (stream) cudaStreamDestroy(stream);
+  context_release(ctx);  // stream and handles go back to the per-device pool
 }
 
 // helper_functions.py:58-87: multiplicity 1 or 2, O2 -> 3, N2 -> 4.
@@ -473,11 +469,18 @@ void System::alloc_matrices() {
   small = m; m += 48;
   pstate = m; m += 16;
   dmax = reinterpret_cast<float*>(m);
-  PF_CUDA(cudaMalloc(&eps_dev, 2 * nbf * sizeof(double)));
-  PF_CUDA(cudaMalloc(&info_dev, sizeof(int)));
-  PF_CUDA(cudaMalloc(&stats_dev, sizeof(JkStats)));
-  PF_CUDA(cudaMalloc(&ptrs_dev, 64 * sizeof(double*)));
-  PF_CUDA(cudaMalloc(&grad_dev, 3 * natoms * sizeof(double)));
+  small_buf.ensure(2 * nbf * sizeof(double) + 256 + sizeof(JkStats) + 256 + 64 * sizeof(double*) + 256 +
+                   3 * natoms * sizeof(double) + 256 + 256);
+  {
+    char* b = small_buf.as<char>();
+    size_t o = 0;
+    auto take = [&](size_t n) { char* r = b + o; o += (n + 255) / 256 * 256; return r; };
+    eps_dev = reinterpret_cast<double*>(take(2 * nbf * sizeof(double)));
+    info_dev = reinterpret_cast<int*>(take(sizeof(int)));
+    stats_dev = reinterpret_cast<unsigned long long*>(take(sizeof(JkStats)));
+    ptrs_dev = reinterpret_cast<const double**>(take(64 * sizeof(double*)));
+    grad_dev = reinterpret_cast<double*>(take(3 * natoms * sizeof(double)));
+  }
   int lwork = 0;
   PF_CUSOLVER(cusolverDnDsyevd_bufferSize(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W1, nbf,
                                           eps_dev, &lwork));
@@ -486,11 +489,7 @@ void System::alloc_matrices() {
 }
 
 void System::release_extra() {
-  if (eps_dev) cudaFree(eps_dev);
-  if (info_dev) cudaFree(info_dev);
-  if (stats_dev) cudaFree(stats_dev);
-  if (ptrs_dev) cudaFree(ptrs_dev);
-  if (grad_dev) cudaFree(grad_dev);
+  small_buf.release();
   eps_dev = nullptr;
   info_dev = nullptr;
   stats_dev = nullptr;

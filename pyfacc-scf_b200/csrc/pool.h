@@ -1,0 +1,34 @@
+// Process-wide pools of device memory, GPU contexts and basis files (pool.cpp).
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace pyfacc {
+
+// Device memory: blocks come back from pool_free to a per-device free list
+// (at most 8 GiB cached per device) and are reused by later requests.
+void* pool_alloc(size_t bytes, size_t* got);
+void pool_free(void* p, size_t bytes);
+void pool_trim(int device);
+
+// One stream with its cuBLAS and cuSOLVER handles and two timing events.
+struct GpuContext {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+GpuContext context_acquire(int device);   // the current device must be `device`
+void context_release(const GpuContext& c);
+
+// Lines of a basis-set file, read once per process.
+std::shared_ptr<const std::vector<std::string>> basis_lines(const std::string& path,
+                                                            std::vector<std::string> (*reader)(const std::string&));
+
+}  // namespace pyfacc

@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "pool.h"
 
 namespace pyfacc {
 
@@ -35,6 +36,7 @@ struct System {
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  GpuContext ctx;
   int natoms = 0, charge = 0, nalpha = 0, nbeta = 0;
   bool uhf = false;
   std::vector<int> Z;
@@ -78,6 +80,7 @@ struct System {
   const double** ptrs_dev = nullptr;
   double* grad_dev = nullptr;
   DeviceBuf syev_work;
+  DeviceBuf small_buf;
   int syev_lwork = 0;
 
   ScfState st;
