@@ -173,6 +173,15 @@ int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double *x_dev, do
  * ranges: bounds[0..parts] (host only, no GPU needed). */
 int pyfacc_partition(int n, const double *cost, int parts, int *bounds);
 
+/* Sharded Fock builds across processes (one GPU each): a system created
+ * with options.shard_rank / shard_count evaluates its share of every
+ * quartet list; after each J/K build and after the two-electron gradient
+ * the engine synchronises its stream and calls fn(ctx, data_dev, count),
+ * which must sum the `count` doubles at data_dev over all shards in place
+ * (e.g. an NCCL all-reduce) before returning 0. */
+typedef int (*pyfacc_reduce_fn)(void *ctx, double *data_dev, long long count);
+int pyfacc_system_set_reducer(pyfacc_system *sys, pyfacc_reduce_fn fn, void *ctx);
+
 /* Sustained FP64 FMA rate of the current device, GFLOP/s (microbenchmark). */
 double pyfacc_probe_fp64_gflops(int device, double *fp32_gflops);
 

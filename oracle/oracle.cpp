@@ -655,8 +655,20 @@ void orc_schwarz(int ns, const int* l, const int* atom, const double* cen, const
 // symmetry over canonical shell quartets with Schwarz screening
 // Q_ab*Q_cd < thresh (thresh <= 0 disables screening).  J[d] = sum (mn|ls) D_ls,
 // K[d] = sum (ml|ns) D_ls.  Returns the number of quartets evaluated.
+long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                  const double* co, int boys_mode, int nd, const double* D, double thresh, int ij_begin, int ij_end,
+                  double* J, double* K);
+
 long orc_jk(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
             const double* co, int boys_mode, int nd, const double* D, double thresh, double* J, double* K) {
+  return orc_jk_range(ns, l, atom, cen, poff, ex, co, boys_mode, nd, D, thresh, 0, ns * (ns + 1) / 2, J, K);
+}
+
+// J/K from the canonical quartets whose bra pair index (a(a+1)/2 + b) lies
+// in [ij_begin, ij_end): the share of one rank of a sharded Fock build.
+long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                  const double* co, int boys_mode, int nd, const double* D, double thresh, int ij_begin, int ij_end,
+                  double* J, double* K) {
   Shells S(ns, l, atom, cen, poff, ex, co);
   const int n = S.nbf;
   const size_t nn = (size_t)n * n;
@@ -673,7 +685,7 @@ long orc_jk(int ns, const int* l, const int* atom, const double* cen, const int*
   {
     std::vector<double> Jl(nd * nn, 0.0), Kl(nd * nn, 0.0), o;
 #pragma omp for schedule(dynamic, 1)
-    for (int ij = npair - 1; ij >= 0; --ij) {
+    for (int ij = std::min(ij_end, npair) - 1; ij >= std::max(ij_begin, 0); --ij) {
       const int a = pa[ij], b = pb[ij];
       for (int kl = 0; kl <= ij; ++kl) {
         const int c = pa[kl], d = pb[kl];

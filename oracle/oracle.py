@@ -80,6 +80,8 @@ def lib():
         _LIB.orc_schwarz.argtypes = sh + [i, p]
         _LIB.orc_jk.restype = ctypes.c_long
         _LIB.orc_jk.argtypes = sh + [i, i, p, d, p, p]
+        _LIB.orc_jk_range.restype = ctypes.c_long
+        _LIB.orc_jk_range.argtypes = sh + [i, i, p, d, i, i, p, p]
         _LIB.orc_gradient.argtypes = sh + [i, p, p, i, p, p, p, p, d, p, p, p, p]
     return _LIB
 
@@ -270,6 +272,15 @@ def eri_tensor(mol: Molecule, boys_mode=0):
     out = np.zeros((n, n, n, n))
     lib().orc_eri_tensor(*mol.shells.args(), boys_mode, _ptr(out))
     return out
+
+
+def jk_range(mol: Molecule, dens, ij_begin, ij_end, thresh=1e-12):
+    """Partial J/K over bra shell pairs ij_begin <= a(a+1)/2 + b < ij_end."""
+    D = np.ascontiguousarray(np.asarray(dens, dtype=np.float64))[None]
+    J = np.zeros_like(D)
+    K = np.zeros_like(D)
+    lib().orc_jk_range(*mol.shells.args(), 0, 1, _ptr(D), thresh, ij_begin, ij_end, _ptr(J), _ptr(K))
+    return J[0], K[0]
 
 
 def schwarz(mol: Molecule, boys_mode=0):

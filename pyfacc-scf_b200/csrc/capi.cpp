@@ -291,17 +291,14 @@ int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double* x_dev, do
 
 int pyfacc_partition(int n, const double* cost, int parts, int* bounds) {
   if (n < 0 || parts < 1 || !bounds || (n > 0 && !cost)) return PYFACC_ERR_INVALID;
-  double total = 0.0;
-  for (int i = 0; i < n; ++i) total += cost[i] > 0 ? cost[i] : 0.0;
-  bounds[0] = 0;
-  double acc = 0.0;
-  int k = 1;
-  for (int i = 0; i < n && k < parts; ++i) {
-    acc += cost[i] > 0 ? cost[i] : 0.0;
-    // close part k-1 once its cumulative share is reached
-    while (k < parts && acc >= total * k / parts) bounds[k++] = i + 1;
-  }
-  while (k <= parts) bounds[k++] = n;
+  pyfacc::partition_costs(n, cost, parts, bounds);
+  return PYFACC_OK;
+}
+
+int pyfacc_system_set_reducer(pyfacc_system* sys, pyfacc_reduce_fn fn, void* ctx) {
+  if (!sys) return PYFACC_ERR_INVALID;
+  sys->impl->reducer = fn;
+  sys->impl->reducer_ctx = ctx;
   return PYFACC_OK;
 }
 

@@ -356,6 +356,22 @@ void System::build_pairs() {
   build_tasks();
 }
 
+// Contiguous ranges of n items with (as far as the granularity allows)
+// equal total cost: range k ends at the first item whose cumulative cost
+// reaches k/parts of the total.
+void partition_costs(int n, const double* cost, int parts, int* bounds) {
+  double total = 0.0;
+  for (int i = 0; i < n; ++i) total += cost[i] > 0 ? cost[i] : 0.0;
+  bounds[0] = 0;
+  double acc = 0.0;
+  int k = 1;
+  for (int i = 0; i < n && k < parts; ++i) {
+    acc += cost[i] > 0 ? cost[i] : 0.0;
+    while (k < parts && acc >= total * k / parts) bounds[k++] = i + 1;
+  }
+  while (k <= parts) bounds[k++] = n;
+}
+
 // Ket ranges per bra: kets are the pairs of the ket class, sorted by Q; a
 // bra reaches the prefix with Q_bra Q_ket >= thresh (and, in mixed mode, the
 // FP64 part is the prefix with Q_bra Q_ket >= fp32_thresh).  For equal
@@ -440,11 +456,33 @@ void System::build_tasks() {
       }
     }
   PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  const int nsh = std::max(opt.shard_count, 1), rank = std::min(std::max(opt.shard_rank, 0), nsh - 1);
   for (auto& p : pend) {
     TaskList& tl = tasks[p.bc][p.kc][p.prec];
     tl.task_off = d + p.off;
     tl.ket_lo = d + p.off + p.nbra + 1;
     tl.ket_hi = d + p.off + 2 * p.nbra + 1;
+    if (nsh > 1) {
+      // this shard's bra range of the list, balanced by task counts
+      const int* toff = hostbuf.data() + p.off;
+      std::vector<double> cost(p.nbra);
+      for (int i = 0; i < p.nbra; ++i) cost[i] = toff[i + 1] - toff[i];
+      std::vector<int> bounds(nsh + 1);
+      partition_costs(p.nbra, cost.data(), nsh, bounds.data());
+      const int b0 = bounds[rank], b1 = bounds[rank + 1];
+      const int* lo = hostbuf.data() + p.off + p.nbra + 1;
+      const int* hi = hostbuf.data() + p.off + 2 * p.nbra + 1;
+      long long q = 0;
+      for (int i = b0; i < b1; ++i) q += hi[i] - lo[i];
+      tl.bra_offset = b0;
+      tl.nbra = b1 - b0;
+      tl.task_off += b0;
+      tl.ket_lo += b0;
+      tl.ket_hi += b0;
+      tl.task_begin = toff[b0];
+      tl.ntasks = toff[b1] - toff[b0];
+      tl.nquartets = q;
+    }
   }
   PF_CUDA(cudaStreamSynchronize(stream));
 }

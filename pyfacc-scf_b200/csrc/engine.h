@@ -81,6 +81,8 @@ struct TaskList {
   int* ket_lo = nullptr;       // device, nbra
   int* ket_hi = nullptr;       // device, nbra
   const int* ntasks_dev = nullptr;  // device count of a list built on the GPU
+  int bra_offset = 0;   // first bra of this (shard of the) list within its class
+  int task_begin = 0;   // global index of the first task (task_off values are global)
 };
 
 // Packed pair data of one molecule or of a batch (every pair stores the
@@ -237,6 +239,10 @@ void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, do
                      double* sout, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
+
+// Cost-balanced contiguous split of n weighted items into parts ranges
+// (bounds[0..parts]); the host side of pyfacc_partition.
+void partition_costs(int n, const double* cost, int parts, int* bounds);
 
 // Detail text returned by pyfacc_last_message() (capi.cpp).
 void set_last_message(const std::string& m);

@@ -358,7 +358,7 @@ struct JkKernelArgs {
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
-  int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec;
+  int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec, task_begin;
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* records(const JkKernelArgs& a);
@@ -373,7 +373,8 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const JkArgs& A = args.a;
   const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < ntasks; t += nw) {
+  for (int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tl < ntasks; tl += nw) {
+    const int t = args.task_begin + tl;
     const int ib = find_bra(args.task_off, args.nbra, t);
     const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
     const int bp = args.bra_base + ib;
@@ -561,8 +562,8 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   k.geom = pd.geom; k.prim = pd.prim; k.primf = pd.primf;
   if (fp32 && !pd.primf) throw Error(PYFACC_ERR_INVALID, "FP32 quartets need float primitive records");
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
-  k.nbra = tl.nbra; k.ntasks = tl.ntasks;
-  k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  k.nbra = tl.nbra; k.ntasks = tl.ntasks; k.task_begin = tl.task_begin;
+  k.bra_base = pd.class_off[bc] + tl.bra_offset; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
   k.prec = fp32 ? 1 : 0;
@@ -717,7 +718,7 @@ struct GradKernelArgs {
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
-  int nbra, ntasks, bra_base, ket_base, same_class, qclass;
+  int nbra, ntasks, bra_base, ket_base, same_class, qclass, task_begin;
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
@@ -732,7 +733,8 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const GradArgs& A = args.a;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+  for (int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tl < args.ntasks; tl += nw) {
+    const int t = args.task_begin + tl;
     const int ib = find_bra(args.task_off, args.nbra, t);
     const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
     const int bp = args.bra_base + ib;
@@ -864,8 +866,8 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   k.geom = pd.geom; k.prim = pd.prim; k.primf = pd.primf;
   if (fp32 && !pd.primf) throw Error(PYFACC_ERR_INVALID, "FP32 quartets need float primitive records");
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
-  k.nbra = tl.nbra; k.ntasks = tl.ntasks;
-  k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  k.nbra = tl.nbra; k.ntasks = tl.ntasks; k.task_begin = tl.task_begin;
+  k.bra_base = pd.class_off[bc] + tl.bra_offset; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
   dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);

@@ -69,6 +69,7 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   a.thresh = thresh;
   a.stats = stats_dev;
   const bool mixed = precision == PYFACC_PRECISION_MIXED;
+  if (opt.shard_count > 1) dynamic = false;  // shards use their static sub-lists
   if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? opt.fp32_thresh : 0.0, dyn, stream);
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
@@ -83,9 +84,19 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
         launch_jk(pd, tasks[bc][kc][0], bc, kc, false, nk, a, num_sms, stream);
       }
     }
+  if (reducer) {  // partial J/K of this shard -> sums over all shards
+    reduce(Jo, (long long)n2);
+    for (int k = 0; k < nk; ++k) reduce(Ko[k], (long long)n2);
+  }
   launch_symmetrize_add(nbf, Jo, stream);
   for (int k = 0; k < nk; ++k) launch_symmetrize_add(nbf, Ko[k], stream);
   st.n_fock++;
+}
+
+void System::reduce(double* data, long long count) {
+  PF_CUDA(cudaStreamSynchronize(stream));
+  const int rc = reducer(reducer_ctx, data, count);
+  if (rc != 0) throw Error(PYFACC_ERR_CUDA, "shard reduction failed (" + std::to_string(rc) + ")");
 }
 
 void System::eri_tensor(double* eri) {
@@ -550,7 +561,8 @@ void System::gradient(double* g_host) {
   g1.W = Wm;
   g1.nbf = nbf;
   g1.grad = grad_dev;
-  launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
+  // one-electron terms once (shard 0); the two-electron term is sharded
+  if (opt.shard_count <= 1 || opt.shard_rank == 0) launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
   launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Pt, nullptr, nullptr, dmax, stream);
   GradArgs g2;
   g2.Pt = Pt;
@@ -577,6 +589,7 @@ void System::gradient(double* g_host) {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }
     }
+  if (reducer) reduce(grad_dev, 3LL * natoms);
   PF_CUDA(cudaEventRecord(a1, stream));
   std::vector<double> g(3 * natoms, 0.0);
   PF_CUDA(cudaMemcpyAsync(g.data(), grad_dev, 3 * natoms * sizeof(double), cudaMemcpyDeviceToHost, stream));

@@ -84,6 +84,9 @@ struct System {
   int syev_lwork = 0;
 
   ScfState st;
+  pyfacc_reduce_fn reducer = nullptr;   // sums shard results across processes
+  void* reducer_ctx = nullptr;
+  void reduce(double* data, long long count);
   bool one_e_done = false;
   std::vector<double> grad_host;
 

@@ -71,6 +71,8 @@ class Result(ctypes.Structure):
     ]
 
 
+REDUCE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, ctypes.c_longlong)
+
 # Every symbol include/pyfacc_b200.h declares, with its ctypes signature.
 SIGNATURES = {
     "run_scf_c": (None, [c_int, c_int, c_int, c_int, c_int, c_void_p, P_double, c_double, c_int, P_double,
@@ -98,6 +100,7 @@ SIGNATURES = {
     "pyfacc_launch_count": (ctypes.c_longlong, []),
     "pyfacc_boys_dev": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "pyfacc_partition": (c_int, [c_int, P_double, c_int, ctypes.POINTER(c_int)]),
+    "pyfacc_system_set_reducer": (c_int, [c_void_p, REDUCE_FN, c_void_p]),
     "pyfacc_probe_fp64_gflops": (c_double, [c_int, P_double]),
     "pyfacc_version": (c_char_p, []),
     "pyfacc_jk_noalloc": (c_int, [ctypes.POINTER(MoleculeC), c_char_p, c_double, c_void_p, c_void_p, c_void_p]),

@@ -19,6 +19,9 @@ def declared_symbols():
         text = open(h).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b(\w+)\s*\(", text, flags=re.M):
+            line = text[m.start():text.find("\n", m.start())]
+            if line.startswith("typedef"):
+                continue
             name = m.group(1)
             if name not in ("if", "defined"):
                 names.add(name)
