@@ -63,6 +63,9 @@ typedef struct pyfacc_options {
   int guess;                /* PYFACC_GUESS_*                        (ATOMIC) */
   double incremental_thresh;/* screening of the incremental dP builds of
                                mixed mode; <= 0: schwarz_thresh      (1e-11) */
+  int task_width;           /* kets per J/K task (8, 16 or 32; a warp runs
+                               32/task_width tasks); 0 = 32 for one molecule,
+                               chosen by timing for a batch            (0)   */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {
@@ -92,6 +95,7 @@ typedef struct pyfacc_result {
   long long quartets_fp64, quartets_fp32;   /* contracted quartets evaluated */
   double flops_fock;        /* algorithmic flops of all Fock builds           */
   double flops_gradient;    /* algorithmic flops of the two-electron gradient */
+  int task_width;           /* J/K task width used                           */
 } pyfacc_result;
 
 typedef struct pyfacc_system pyfacc_system;   /* opaque, one molecule on one GPU */
@@ -129,10 +133,24 @@ void pyfacc_default_options(pyfacc_options *opt);
  * nuclear gradient (rscf.f90:26-168 / uscf.f90:25-219 plus gradient). */
 int pyfacc_run(const pyfacc_molecule *mol, const pyfacc_options *opt, pyfacc_result *res);
 
-/* Many molecules of uneven size converged together on one GPU: batched J/K
- * launches over all molecules' shell quartets and a batched eigensolver. */
+/* Many molecules of uneven size converged together on one GPU: the shell
+ * quartets of all closed-shell molecules (up to 160 basis functions each)
+ * run in the same J/K launches, every SCF iteration of the batch is one CUDA
+ * graph (J/K class kernels + one dense-step kernel with a thread block per
+ * molecule: Fock matrix, energy, DIIS, TC2 purification), and J/K task widths
+ * are picked per quartet class by timing (options.task_width = 0).  Open-shell
+ * or larger molecules, results that ask for matrices, and molecules whose
+ * batched purification fails run through pyfacc_run.  res[i] as in
+ * pyfacc_run (timings and counters are those of the whole batch); returns the
+ * worst per-molecule status. */
 int pyfacc_run_batch(int nmol, const pyfacc_molecule *mols, const pyfacc_options *opt,
                      pyfacc_result *res);
+/* Statistics of the last batched run on this thread: out[0..n) =
+ * {ms_total, ms_setup, ms_one_electron, ms_tune, ms_scf, ms_polish,
+ *  ms_gradient, iterations, flops_fock, flops_gradient, quartets_fp64,
+ *  quartets_fp32, task width of the six quartet classes (ss|ss) (ps|ss)
+ *  (ps|ps) (pp|ss) (pp|ps) (pp|pp)}. */
+int pyfacc_batch_last_stats(double *out, int n);
 
 /* Handle API: basis, shell pairs and Schwarz factors stay resident on the
  * GPU between calls. */

@@ -1,0 +1,762 @@
+// Host side of the batched engine: packing of many molecules into one set
+// of shells, pairs, task lists and matrices; the per-class task-width
+// autotuner; the CUDA-graph SCF loop; the batched gradient.
+#include "batch.h"
+
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+#include "system.h"
+
+namespace pyfacc {
+
+static double wall_ms() {
+  using namespace std::chrono;
+  return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+static int qclass_index(int bc, int kc) { return (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc); }
+static const int kWidths[3] = {32, 16, 8};
+
+BatchMolHost batch_parse(const pyfacc_molecule& m, const pyfacc_options& o, bool* uhf) {
+  if (m.natoms <= 0 || !m.z || !m.coords || !m.basis) throw Error(PYFACC_ERR_INVALID, "empty molecule");
+  BatchMolHost h;
+  h.natoms = m.natoms;
+  h.Z.assign(m.z, m.z + m.natoms);
+  h.xyz.assign(m.coords, m.coords + 3 * m.natoms);
+  h.species.resize(m.natoms);
+  for (int a = 0; a < m.natoms; ++a) {
+    if (m.species) {
+      std::string s(m.species + 2 * a, 2);
+      while (!s.empty() && (s.back() == ' ' || s.back() == '\0')) s.pop_back();
+      h.species[a] = s;
+    } else {
+      h.species[a] = element_symbol(h.Z[a]);
+    }
+    if (h.species[a].empty() || element_z(h.species[a]) == 0)
+      throw Error(PYFACC_ERR_ELEMENT, "unknown element at atom " + std::to_string(a));
+  }
+  if (m.nalpha >= 0 && m.nbeta >= 0) {
+    h.nalpha = m.nalpha;
+    h.nbeta = m.nbeta;
+  } else {
+    System::spin_electrons(h.species, m.charge, &h.nalpha, &h.nbeta);
+  }
+  *uhf = (o.scf_type == PYFACC_SCF_UHF) || (o.scf_type == PYFACC_SCF_AUTO && h.nalpha != h.nbeta);
+  h.nocc = (h.nalpha + h.nbeta + 1) / 2;  // rscf.f90:54-55
+  h.basis = build_basis(resolve_basis_file(m.basis, o.data_dir), h.species, h.xyz);
+  h.nbf = h.basis.nbf;
+  h.ns = (int)h.basis.shells.size();
+  // molecule.f90:31-52
+  for (int i = 0; i < h.natoms; ++i)
+    for (int j = i + 1; j < h.natoms; ++j) {
+      double d2 = 0.0;
+      for (int x = 0; x < 3; ++x) d2 += (h.xyz[3 * i + x] - h.xyz[3 * j + x]) * (h.xyz[3 * i + x] - h.xyz[3 * j + x]);
+      const double r = std::sqrt(d2);
+      if (r > 1.0e-10) h.e_nuc += (double)h.Z[i] * h.Z[j] / r;
+    }
+  return h;
+}
+
+Batch::Batch(const std::vector<BatchMolHost>& ms, const pyfacc_options& o) : opt(o), mols(ms) {
+  const double t0 = wall_ms();
+  nmol = (int)mols.size();
+  if (nmol > 65535) throw Error(PYFACC_ERR_INVALID, "at most 65535 molecules per batch");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(PYFACC_ERR_NO_DEVICE, "no CUDA device");
+  if (opt.device >= 0) {
+    device = opt.device;
+    PF_CUDA(cudaSetDevice(device));
+  } else {
+    PF_CUDA(cudaGetDevice(&device));
+  }
+  PF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  if (opt.task_width != 0 && opt.task_width != 8 && opt.task_width != 16 && opt.task_width != 32)
+    throw Error(PYFACC_ERR_INVALID, "task_width must be 0, 8, 16 or 32");
+  ensure_boys_tables(device);
+  ctx = context_acquire(device);
+  stream = ctx.stream;
+  const int nd = std::min(std::max(opt.diis_size, 0), BATCH_DIIS_MAX);
+  long long mo = 0, dofs = 0;
+  int aoff = 0, soff = 0;
+  for (auto& m : mols) {
+    if (m.nbf > BATCH_NBF_MAX) throw Error(PYFACC_ERR_INVALID, "molecule too large for the batched engine");
+    m.atom_off = aoff;
+    m.shell_off = soff;
+    m.mat_off = mo;
+    m.diis_off = dofs;
+    aoff += m.natoms;
+    soff += m.ns;
+    mo += (long long)m.nbf * m.nbf;
+    dofs += 2LL * nd * m.nbf * m.nbf;
+    ns_max = std::max(ns_max, m.ns);
+    nbf_max = std::max(nbf_max, m.nbf);
+  }
+  natoms_tot = aoff;
+  ns_tot = soff;
+  mtot = mo;
+  if (mtot >= (1LL << 31) || (long long)nmol * ns_max * ns_max >= (1LL << 31))
+    throw Error(PYFACC_ERR_INVALID, "batch too large: split it into several calls");
+  upload();
+  build_pairs();
+  build_tasks();
+  alloc();
+  timing.ms_setup = wall_ms() - t0;
+}
+
+Batch::~Batch() {
+  cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  if (graph_full) cudaGraphExecDestroy(graph_full);
+  if (graph_inc) cudaGraphExecDestroy(graph_inc);
+  if (active_host) cudaFreeHost(active_host);
+  context_release(ctx);
+}
+
+double Batch::energy(int m) const { return st_host[m].E_final + mols[m].e_nuc; }
+
+// Shells of all molecules (atoms and matrix offsets per shell), 1e pair
+// lists inside each molecule, per-molecule shell tables.
+void Batch::upload() {
+  std::vector<double4> cen(ns_tot);
+  std::vector<int4> desc(ns_tot), molt(ns_tot), mt(nmol);
+  std::vector<int> np(ns_tot), nf(ns_tot), bfo(ns_tot);
+  std::vector<double> ex, co;
+  std::vector<double4> atoms(natoms_tot);
+  std::vector<int2> p1[NCLASS];
+  for (int m = 0; m < nmol; ++m) {
+    const BatchMolHost& M = mols[m];
+    for (int s = 0; s < M.ns; ++s) {
+      const Shell& sh = M.basis.shells[s];
+      const int g = M.shell_off + s;
+      cen[g] = make_double4(sh.c[0], sh.c[1], sh.c[2], 0.0);
+      desc[g] = make_int4(sh.l, M.atom_off + sh.atom, M.basis.bf_off[s], (int)ex.size());
+      molt[g] = make_int4(M.atom_off, M.natoms, (int)M.mat_off, M.nbf);
+      np[g] = (int)sh.ex.size();
+      nf[g] = (sh.l + 1) * (sh.l + 2) / 2;
+      bfo[g] = M.basis.bf_off[s];
+      ex.insert(ex.end(), sh.ex.begin(), sh.ex.end());
+      co.insert(co.end(), sh.co.begin(), sh.co.end());
+    }
+    for (int a = 0; a < M.natoms; ++a)
+      atoms[M.atom_off + a] = make_double4(M.xyz[3 * a], M.xyz[3 * a + 1], M.xyz[3 * a + 2], (double)M.Z[a]);
+    for (int a = 0; a < M.ns; ++a)
+      for (int b = a; b < M.ns; ++b) {
+        int x = a, y = b;
+        if (M.basis.shells[x].l < M.basis.shells[y].l) std::swap(x, y);
+        p1[M.basis.shells[x].l + M.basis.shells[y].l].push_back(make_int2(M.shell_off + x, M.shell_off + y));
+      }
+    mt[m] = make_int4(M.shell_off, M.ns, (int)M.mat_off, M.nbf);
+  }
+  for (int c = 0; c < NCLASS; ++c) n1e[c] = (int)p1[c].size();
+  const size_t nex = std::max<size_t>(ex.size(), 1);
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    size_t o = off;
+    off += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  const size_t o_cen = carve(ns_tot * sizeof(double4)), o_desc = carve(ns_tot * sizeof(int4)),
+               o_np = carve(ns_tot * sizeof(int)), o_ex = carve(nex * sizeof(double)), o_co = carve(nex * sizeof(double)),
+               o_atoms = carve(natoms_tot * sizeof(double4)),
+               o_p1 = carve((n1e[0] + n1e[1] + n1e[2] + 3) * sizeof(int2)), o_bfo = carve(ns_tot * sizeof(int)),
+               o_nf = carve(ns_tot * sizeof(int)), o_molt = carve(ns_tot * sizeof(int4)),
+               o_mt = carve(nmol * sizeof(int4));
+  shd.buf.ensure(off);
+  char* base = shd.buf.as<char>();
+  shd.ns = ns_tot;
+  shd.cen = reinterpret_cast<double4*>(base + o_cen);
+  shd.desc = reinterpret_cast<int4*>(base + o_desc);
+  shd.nprim = reinterpret_cast<int*>(base + o_np);
+  shd.ex = reinterpret_cast<double*>(base + o_ex);
+  shd.co = reinterpret_cast<double*>(base + o_co);
+  shd.mol = reinterpret_cast<int4*>(base + o_molt);
+  atoms_dev = reinterpret_cast<double4*>(base + o_atoms);
+  pairs1e[0] = reinterpret_cast<int2*>(base + o_p1);
+  pairs1e[1] = pairs1e[0] + n1e[0];
+  pairs1e[2] = pairs1e[1] + n1e[1];
+  bf_off_dev = reinterpret_cast<int*>(base + o_bfo);
+  nfun_dev = reinterpret_cast<int*>(base + o_nf);
+  mt_dev = reinterpret_cast<int4*>(base + o_mt);
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    if (bytes) PF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+  };
+  up(shd.cen, cen.data(), ns_tot * sizeof(double4));
+  up(shd.desc, desc.data(), ns_tot * sizeof(int4));
+  up(shd.nprim, np.data(), ns_tot * sizeof(int));
+  up(shd.ex, ex.data(), ex.size() * sizeof(double));
+  up(shd.co, co.data(), co.size() * sizeof(double));
+  up(shd.mol, molt.data(), ns_tot * sizeof(int4));
+  up(atoms_dev, atoms.data(), natoms_tot * sizeof(double4));
+  for (int c = 0; c < NCLASS; ++c) up(pairs1e[c], p1[c].data(), n1e[c] * sizeof(int2));
+  up(bf_off_dev, bfo.data(), ns_tot * sizeof(int));
+  up(nfun_dev, nf.data(), ns_tot * sizeof(int));
+  up(mt_dev, mt.data(), nmol * sizeof(int4));
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Canonical pairs of every molecule, Schwarz factors on the GPU, then per
+// class sorted by (molecule, Q descending); pairs that cannot reach the
+// threshold against the largest Q of their molecule are dropped.
+void Batch::build_pairs() {
+  std::vector<int4> pl0[NCLASS], pl1[NCLASS];
+  std::vector<int> pm[NCLASS];
+  std::vector<int> nprim_of(ns_tot);
+  for (int m = 0; m < nmol; ++m)
+    for (int s = 0; s < mols[m].ns; ++s) nprim_of[mols[m].shell_off + s] = (int)mols[m].basis.shells[s].ex.size();
+  for (int m = 0; m < nmol; ++m) {
+    const BatchMolHost& M = mols[m];
+    for (int i = 0; i < M.ns; ++i)
+      for (int j = 0; j <= i; ++j) {
+        int a = i, b = j;
+        if (M.basis.shells[a].l < M.basis.shells[b].l) std::swap(a, b);
+        const int c = M.basis.shells[a].l + M.basis.shells[b].l;
+        pl0[c].push_back(make_int4(M.shell_off + a, M.shell_off + b, 0, M.shell_off));
+        pl1[c].push_back(make_int4((int)M.mat_off, M.nbf, m, m * ns_max * ns_max));
+        pm[c].push_back(m);
+      }
+  }
+  std::vector<int4> all0, all1;
+  std::vector<int> allm;
+  int off[NCLASS + 1] = {0, 0, 0, 0};
+  long long nprim_tot = 0;
+  for (int c = 0; c < NCLASS; ++c) {
+    off[c + 1] = off[c] + (int)pl0[c].size();
+    for (size_t k = 0; k < pl0[c].size(); ++k) {
+      int4 p = pl0[c][k];
+      p.z = (int)nprim_tot;
+      nprim_tot += (long long)nprim_of[p.x] * nprim_of[p.y];
+      all0.push_back(p);
+      all1.push_back(pl1[c][k]);
+      allm.push_back(pm[c][k]);
+    }
+  }
+  if (nprim_tot >= (1LL << 31)) throw Error(PYFACC_ERR_INVALID, "batch too large: split it into several calls");
+  const int np_all = off[NCLASS];
+  size_t o = 0;
+  auto carve = [&](size_t bytes) {
+    size_t r = o;
+    o += (bytes + 255) / 256 * 256;
+    return r;
+  };
+  const size_t s_pl0 = carve(np_all * sizeof(int4)), s_pl1 = carve(np_all * sizeof(int4)),
+               s_i0 = carve(np_all * sizeof(int4)), s_i1 = carve(np_all * sizeof(int4)),
+               s_i2 = carve(np_all * sizeof(int4)), s_g = carve(np_all * sizeof(double4)),
+               s_pr = carve((size_t)std::max<long long>(nprim_tot, 1) * 3 * sizeof(double4)),
+               s_q = carve(np_all * sizeof(double)), s_perm = carve(np_all * sizeof(int)),
+               s_ps = carve(np_all * sizeof(int)), s_kept = carve(np_all * sizeof(int));
+  DeviceBuf scratch;
+  scratch.ensure(o);
+  char* sb = scratch.as<char>();
+  int4* d_pl0 = reinterpret_cast<int4*>(sb + s_pl0);
+  int4* d_pl1 = reinterpret_cast<int4*>(sb + s_pl1);
+  PairData tmp;
+  tmp.info0 = reinterpret_cast<int4*>(sb + s_i0);
+  tmp.info1 = reinterpret_cast<int4*>(sb + s_i1);
+  tmp.info2 = reinterpret_cast<int4*>(sb + s_i2);
+  tmp.geom = reinterpret_cast<double4*>(sb + s_g);
+  tmp.prim = reinterpret_cast<double4*>(sb + s_pr);
+  double* d_q = reinterpret_cast<double*>(sb + s_q);
+  int* d_perm = reinterpret_cast<int*>(sb + s_perm);
+  int* d_ps = reinterpret_cast<int*>(sb + s_ps);
+  int* d_kept = reinterpret_cast<int*>(sb + s_kept);
+  double maxpref = 0.0;
+  for (const auto& m : mols) maxpref = std::max(maxpref, max_prim_prefactor(m.basis));
+  const double cut = PRIM_CUT_REL * maxpref;
+  PF_CUDA(cudaMemcpyAsync(d_pl0, all0.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
+  PF_CUDA(cudaMemcpyAsync(d_pl1, all1.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
+  launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, cut, d_kept,
+                     stream);
+  launch_schwarz(tmp, off, d_q, stream);
+  std::vector<double> q(np_all);
+  std::vector<int> kept(np_all);
+  PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaMemcpyAsync(kept.data(), d_kept, np_all * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  std::vector<double> qmax(nmol, 0.0);
+  for (int k = 0; k < np_all; ++k) qmax[allm[k]] = std::max(qmax[allm[k]], q[k]);
+  const double thr = opt.schwarz_thresh;
+  std::vector<int> perm, new_ps;
+  pd.class_off[0] = 0;
+  long long nprim_new = 0;
+  pd.q_host.clear();
+  pd.cls_host.clear();
+  pd.mol_host.clear();
+  for (int c = 0; c < NCLASS; ++c) {
+    std::vector<int> idx;
+    for (int k = off[c]; k < off[c + 1]; ++k)
+      if (thr <= 0 || q[k] * qmax[allm[k]] >= thr) idx.push_back(k);
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+      if (allm[x] != allm[y]) return allm[x] < allm[y];
+      return q[x] > q[y];
+    });
+    seg[c].assign(nmol + 1, 0);
+    for (int k : idx) {
+      perm.push_back(k);
+      new_ps.push_back((int)nprim_new);
+      nprim_new += kept[k];
+      pd.q_host.push_back(q[k]);
+      pd.cls_host.push_back(c);
+      pd.mol_host.push_back(allm[k]);
+      seg[c][allm[k] + 1]++;
+    }
+    for (int m = 0; m < nmol; ++m) seg[c][m + 1] += seg[c][m];
+    pd.class_off[c + 1] = (int)perm.size();
+  }
+  pd.npair = (int)perm.size();
+  pd.nprim = (int)nprim_new;
+  o = 0;
+  const size_t f_i0 = carve(pd.npair * sizeof(int4)), f_i1 = carve(pd.npair * sizeof(int4)),
+               f_i2 = carve(pd.npair * sizeof(int4)), f_g = carve(pd.npair * sizeof(double4)),
+               f_pr = carve((size_t)std::max<long long>(nprim_new, 1) * 3 * sizeof(double4)),
+               f_prf = carve((size_t)std::max<long long>(nprim_new, 1) * 3 * sizeof(float4));
+  pd.buf.ensure(std::max<size_t>(o, 256));
+  char* pb = pd.buf.as<char>();
+  pd.info0 = reinterpret_cast<int4*>(pb + f_i0);
+  pd.info1 = reinterpret_cast<int4*>(pb + f_i1);
+  pd.info2 = reinterpret_cast<int4*>(pb + f_i2);
+  pd.geom = reinterpret_cast<double4*>(pb + f_g);
+  pd.prim = reinterpret_cast<double4*>(pb + f_pr);
+  pd.primf = reinterpret_cast<float4*>(pb + f_prf);
+  if (pd.npair > 0) {
+    PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
+    PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
+    launch_gather_pairs(pd.npair, d_perm, d_ps, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, d_q, cut,
+                        pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, pd.primf, stream);
+  }
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+// Ket ranges per bra inside the bra's molecule (the segment of the ket
+// class): prefix with Q_bra Q_ket >= thresh, the FP64 part the prefix with
+// Q_bra Q_ket >= fp32_thresh; for equal classes only kets up to the bra.
+// The ranges are shared by the three task widths, whose task offsets differ.
+void Batch::build_tasks() {
+  const double thr = std::max(opt.schwarz_thresh, 0.0);
+  const double t32 = opt.fp32_thresh;
+  struct Pending { int bc, kc, prec; size_t lo_off, toff_off[3]; int nbra; };
+  std::vector<Pending> pend;
+  std::vector<int> hostbuf;
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
+      const double* qb = pd.q_host.data() + pd.class_off[bc];
+      const double* qk = pd.q_host.data() + pd.class_off[kc];
+      const int* mb = pd.mol_host.data() + pd.class_off[bc];
+      auto prefix = [&](double qbra, const double* q0, int nk, double t) {
+        if (t <= 0) return nk;
+        int lo = 0, hi = nk;
+        while (lo < hi) {
+          int mid = (lo + hi) / 2;
+          if (qbra * q0[mid] >= t) lo = mid + 1; else hi = mid;
+        }
+        return lo;
+      };
+      std::vector<int> full_hi(nb), split(nb), kstart(nb);
+      for (int i = 0; i < nb; ++i) {
+        const int m = mb[i];
+        const int ks = seg[kc][m], nk = seg[kc][m + 1] - ks;
+        int mm = prefix(qb[i], qk + ks, nk, thr);
+        if (bc == kc) mm = std::min(mm, i - seg[bc][m] + 1);
+        const int m64 = std::min(prefix(qb[i], qk + ks, nk, t32), mm);
+        kstart[i] = ks;
+        full_hi[i] = ks + mm;
+        split[i] = ks + m64;
+      }
+      for (int prec = 0; prec < 3; ++prec) {
+        Pending p{bc, kc, prec, hostbuf.size(), {0, 0, 0}, nb};
+        std::vector<int> lo(nb), hi(nb);
+        long long quart = 0;
+        for (int i = 0; i < nb; ++i) {
+          lo[i] = (prec == 2) ? split[i] : kstart[i];
+          hi[i] = (prec == 1) ? split[i] : full_hi[i];
+          quart += hi[i] - lo[i];
+        }
+        hostbuf.insert(hostbuf.end(), lo.begin(), lo.end());
+        hostbuf.insert(hostbuf.end(), hi.begin(), hi.end());
+        for (int wi = 0; wi < 3; ++wi) {
+          const int w = kWidths[wi];
+          p.toff_off[wi] = hostbuf.size();
+          int ntask = 0;
+          for (int i = 0; i < nb; ++i) {
+            hostbuf.push_back(ntask);
+            ntask += (hi[i] - lo[i] + w - 1) / w;
+          }
+          hostbuf.push_back(ntask);
+          TaskList& tl = tasks_w[wi][bc][kc][prec];
+          tl.width = w;
+          tl.nbra = nb;
+          tl.ntasks = ntask;
+          tl.nquartets = quart;
+        }
+        pend.push_back(p);
+      }
+    }
+  task_buf.ensure(std::max<size_t>(hostbuf.size() * sizeof(int), 256));
+  int* d = task_buf.as<int>();
+  PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  for (auto& p : pend)
+    for (int wi = 0; wi < 3; ++wi) {
+      TaskList& tl = tasks_w[wi][p.bc][p.kc][p.prec];
+      tl.ket_lo = d + p.lo_off;
+      tl.ket_hi = d + p.lo_off + p.nbra;
+      tl.task_off = d + p.toff_off[wi];
+    }
+  int wi0 = 0;
+  if (opt.task_width == 16) wi0 = 1;
+  if (opt.task_width == 8) wi0 = 2;
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      for (int p = 0; p < 3; ++p) tasks[bc][kc][p] = tasks_w[wi0][bc][kc][p];
+      timing.width[qclass_index(bc, kc)] = kWidths[wi0];
+    }
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Batch::alloc() {
+  const int nd = std::min(std::max(opt.diis_size, 0), BATCH_DIIS_MAX);
+  const size_t m8 = (size_t)mtot * sizeof(double);
+  constexpr size_t nmat = 16;
+  size_t o = 0;
+  auto carve = [&](size_t bytes) {
+    size_t r = o;
+    o += (bytes + 255) / 256 * 256;
+    return r;
+  };
+  size_t om[nmat];
+  for (size_t k = 0; k < nmat; ++k) om[k] = carve(m8);
+  const size_t o_diis = carve(std::max<size_t>(2 * nd * m8, 8));
+  const size_t o_dmax = carve((size_t)nmol * ns_max * ns_max * sizeof(float));
+  const size_t o_stats = carve(sizeof(JkStats) + 2 * NQCLASS * sizeof(unsigned long long));
+  const size_t o_grad = carve(3 * (size_t)natoms_tot * sizeof(double));
+  const size_t o_act = carve(sizeof(int));
+  mats.ensure(o);
+  char* b = mats.as<char>();
+  double* mp[nmat];
+  for (size_t k = 0; k < nmat; ++k) mp[k] = reinterpret_cast<double*>(b + om[k]);
+  S = mp[0];
+  T = mp[1];
+  V = mp[2];
+  W = mp[15];
+  dmax = reinterpret_cast<float*>(b + o_dmax);
+  stats_dev = reinterpret_cast<unsigned long long*>(b + o_stats);
+  grad_dev = reinterpret_cast<double*>(b + o_grad);
+  active_dev = reinterpret_cast<int*>(b + o_act);
+  const size_t st_bytes = (nmol * sizeof(BatchMolState) + 255) / 256 * 256;
+  state_buf.ensure(st_bytes + nmol * sizeof(BatchMolDev) + 256);
+  BatchMolState* st = state_buf.as<BatchMolState>();
+  BatchMolDev* md = reinterpret_cast<BatchMolDev*>(state_buf.as<char>() + st_bytes);
+  std::vector<BatchMolDev> mdh(nmol);
+  int occ_off = 0;
+  occ_host.clear();
+  for (int m = 0; m < nmol; ++m) {
+    const BatchMolHost& M = mols[m];
+    mdh[m] = BatchMolDev{M.nbf, M.nocc, M.ns, M.natoms, occ_off, 0, M.mat_off, M.diis_off};
+    const std::vector<double> occ = atomic_occupations(M.basis, M.Z, M.nalpha + M.nbeta);
+    occ_host.insert(occ_host.end(), occ.begin(), occ.end());
+    occ_off += M.nbf;
+  }
+  PF_CUDA(cudaMemcpyAsync(md, mdh.data(), nmol * sizeof(BatchMolDev), cudaMemcpyHostToDevice, stream));
+  occ_buf.ensure(std::max<size_t>(occ_host.size() * sizeof(double), 256));
+  PF_CUDA(cudaMemcpyAsync(occ_buf.as<double>(), occ_host.data(), occ_host.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, stream));
+  BatchDenseArgs& a = dargs;
+  a.mol = md;
+  a.st = st;
+  a.S = mp[0];
+  a.H = mp[3];
+  a.X = mp[4];
+  a.F = mp[5];
+  a.J = mp[6];
+  a.K = mp[7];
+  a.Jd = mp[8];
+  a.Kd = mp[9];
+  a.P = mp[10];
+  a.Db = mp[11];
+  a.T1 = mp[12];
+  a.T2 = mp[13];
+  a.T3 = mp[14];
+  a.diis = reinterpret_cast<double*>(b + o_diis);
+  a.ndiis = nd;
+  a.max_iter = std::max(opt.max_iter, 1);
+  a.rebuild_every = std::max(opt.rebuild_every, 1);
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+  a.incremental = (opt.incremental < 0 ? mixed : (opt.incremental != 0)) ? 1 : 0;
+  a.e_tol = mixed ? std::max(opt.eps_energy, 1e-8) : opt.eps_energy;
+  a.eps_diis = opt.eps_diis;
+  a.eps_density = opt.eps_density;
+  a.active = active_dev;
+  a.smem_nmax = nbf_max;  // nbf <= 160: at most 200 KB of shared memory
+  batch_set_smem(a);
+  PF_CUDA(cudaMallocHost(&active_host, sizeof(int)));
+  PF_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stats) {
+  launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.Db, dmax, stream);
+  JkArgs a;
+  a.Dj = dargs.Db;
+  a.Dk0 = dargs.Db;
+  a.Dk1 = dargs.Db;
+  a.J = dargs.Jd;
+  a.K0 = dargs.Kd;
+  a.K1 = dargs.Kd;
+  a.dmax = thresh > 0 ? dmax : nullptr;
+  a.ns_ld = ns_max;
+  a.thresh = thresh;
+  a.stats = stats;
+  for (int bc = NCLASS - 1; bc >= 0; --bc)
+    for (int kc = bc; kc >= 0; --kc) {
+      if (mixed_lists) {
+        launch_jk(pd, tasks[bc][kc][1], bc, kc, false, 1, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, stream);
+      } else {
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, 1, a, num_sms, stream);
+      }
+    }
+}
+
+// Task-width autotuner: every quartet class is timed with tasks of 32, 16
+// and 8 kets on the first (full) build of this batch, and the fastest width
+// is kept per class.  Results are cached per batch shape (precision and the
+// molecules' sizes), so repeated batches of the same shape skip the timing.
+void Batch::tune() {
+  static std::mutex mu;
+  static std::map<std::string, std::array<int, NQCLASS>> cache;
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+  std::ostringstream key;
+  key << device << ':' << (mixed ? 'm' : 'd') << ':' << opt.schwarz_thresh << ':' << opt.fp32_thresh;
+  for (const auto& m : mols) key << ',' << m.nbf << '/' << m.natoms;
+  std::array<int, NQCLASS> best{};
+  bool have = false;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key.str());
+    if (it != cache.end()) {
+      best = it->second;
+      have = true;
+    }
+  }
+  if (!have) {
+    const double t0 = wall_ms();
+    launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.Db, dmax, stream);
+    JkArgs a;
+    a.Dj = a.Dk0 = a.Dk1 = dargs.Db;
+    a.J = dargs.Jd;
+    a.K0 = a.K1 = dargs.Kd;
+    a.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
+    a.ns_ld = ns_max;
+    a.thresh = opt.schwarz_thresh;
+    a.stats = nullptr;
+    cudaEvent_t e0 = ctx.ev0, e1 = ctx.ev1;
+    auto run_class = [&](int wi, int bc, int kc) {
+      if (mixed) {
+        launch_jk(pd, tasks_w[wi][bc][kc][1], bc, kc, false, 1, a, num_sms, stream);
+        launch_jk(pd, tasks_w[wi][bc][kc][2], bc, kc, true, 1, a, num_sms, stream);
+      } else {
+        launch_jk(pd, tasks_w[wi][bc][kc][0], bc, kc, false, 1, a, num_sms, stream);
+      }
+    };
+    for (int bc = 0; bc < NCLASS; ++bc)
+      for (int kc = 0; kc <= bc; ++kc) {
+        const int q = qclass_index(bc, kc);
+        run_class(0, bc, kc);  // warm-up
+        float tbest = 0.0f;
+        best[q] = kWidths[0];
+        for (int wi = 0; wi < 3; ++wi) {
+          PF_CUDA(cudaEventRecord(e0, stream));
+          run_class(wi, bc, kc);
+          PF_CUDA(cudaEventRecord(e1, stream));
+          PF_CUDA(cudaEventSynchronize(e1));
+          float ms = 0.0f;
+          PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          // a narrower tile has to win by 3% to replace a wider one
+          if (wi == 0 || ms < 0.97f * tbest) {
+            tbest = ms;
+            best[q] = kWidths[wi];
+          }
+        }
+      }
+    launch_zero(dargs.Jd, (size_t)mtot * sizeof(double), stream);
+    launch_zero(dargs.Kd, (size_t)mtot * sizeof(double), stream);
+    PF_CUDA(cudaStreamSynchronize(stream));
+    timing.ms_tune = wall_ms() - t0;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key.str()] = best;
+  }
+  for (int bc = 0; bc < NCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) {
+      const int q = qclass_index(bc, kc);
+      const int wi = best[q] == 32 ? 0 : (best[q] == 16 ? 1 : 2);
+      for (int p = 0; p < 3; ++p) tasks[bc][kc][p] = tasks_w[wi][bc][kc][p];
+      timing.width[q] = best[q];
+    }
+}
+
+// One SCF iteration of the batch as a CUDA graph: density maxima of Db, the
+// J/K class kernels (full builds screen at schwarz_thresh, incremental ones
+// at incremental_thresh), the count reset and the dense step.
+cudaGraphExec_t Batch::capture(bool full, long long* launches) {
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+  const double inc_thresh = (mixed && opt.incremental_thresh > 0)
+                                ? std::max(opt.incremental_thresh, opt.schwarz_thresh)
+                                : opt.schwarz_thresh;
+  const long long c0 = launch_count();
+  cudaGraph_t g = nullptr;
+  PF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    fock_build(mixed, full ? opt.schwarz_thresh : inc_thresh, stats_dev);
+    PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(int), stream));
+    launch_batch_step(nmol, dargs, stream);
+  } catch (...) {
+    cudaStreamEndCapture(stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  PF_CUDA(cudaStreamEndCapture(stream, &g));
+  cudaGraphExec_t e = nullptr;
+  const cudaError_t rc = cudaGraphInstantiate(&e, g, 0);
+  cudaGraphDestroy(g);
+  if (rc != cudaSuccess) throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
+  *launches = launch_count() - c0;
+  return e;
+}
+
+void Batch::run(bool gradient) {
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+  const double t0 = wall_ms();
+  cudaEvent_t e0 = ctx.ev0, e1 = ctx.ev1;
+  PF_CUDA(cudaMemsetAsync(dargs.st, 0, nmol * sizeof(BatchMolState), stream));
+  PF_CUDA(cudaMemsetAsync(stats_dev, 0, sizeof(JkStats), stream));
+  // ---- one-electron integrals, orthogonaliser, starting density
+  PF_CUDA(cudaEventRecord(e0, stream));
+  OneEArgs oa;
+  oa.natoms = 0;
+  oa.atoms = atoms_dev;
+  oa.boys_mode = opt.boys_mode;
+  oa.S = S;
+  oa.T = T;
+  oa.V = V;
+  oa.nbf = 0;
+  launch_one_electron(shd, n1e, pairs1e, oa, stream);
+  double* H = const_cast<double*>(dargs.H);
+  launch_axpby(mtot, 1.0, T, 0.0, H, stream);
+  launch_axpby(mtot, 1.0, V, 1.0, H, stream);
+  launch_batch_lowdin(nmol, dargs, const_cast<double*>(dargs.X), stream);
+  const bool core = opt.guess == PYFACC_GUESS_CORE;
+  if (!core) launch_batch_guess(nmol, dargs, occ_buf.as<double>(), stream);
+  launch_batch_init(nmol, dargs, core ? 1 : 0, stream);
+  PF_CUDA(cudaEventRecord(e1, stream));
+  PF_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  timing.ms_1e = ms;
+  // ---- task widths, graphs
+  if (opt.task_width == 0) tune();
+  const double ts = wall_ms();
+  if (!graph_full) graph_full = capture(true, &graph_launches[0]);
+  if (dargs.incremental && !graph_inc) graph_inc = capture(false, &graph_launches[1]);
+  int it = 0;
+  for (it = 1; it <= dargs.max_iter; ++it) {
+    const bool full = !dargs.incremental || it == 1 || ((it - 1) % dargs.rebuild_every) == 0;
+    PF_CUDA(cudaGraphLaunch(full ? graph_full : graph_inc, stream));
+    count_launches(full ? graph_launches[0] : graph_launches[1]);
+    PF_CUDA(cudaMemcpyAsync(active_host, active_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    if (*active_host == 0) break;
+  }
+  timing.iterations = std::min(it, dargs.max_iter);
+  timing.ms_scf = wall_ms() - ts;
+  // ---- FP64 polish of mixed precision: F and E of the final densities
+  if (mixed) {
+    const double tp = wall_ms();
+    launch_batch_polish_density(nmol, dargs, stream);
+    fock_build(false, opt.schwarz_thresh, stats_dev);
+    launch_batch_polish(nmol, dargs, stream);
+    PF_CUDA(cudaStreamSynchronize(stream));
+    timing.ms_polish = wall_ms() - tp;
+  }
+  st_host.resize(nmol);
+  PF_CUDA(cudaMemcpyAsync(st_host.data(), dargs.st, nmol * sizeof(BatchMolState), cudaMemcpyDeviceToHost, stream));
+  JkStats js;
+  PF_CUDA(cudaMemcpyAsync(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  timing.quartets[0] = timing.quartets[1] = 0;
+  timing.flops_fock = 0.0;
+  for (int p = 0; p < 2; ++p)
+    for (int q = 0; q < NQCLASS; ++q) {
+      timing.quartets[p] += js.quartets[p][q];
+      const ClassFlops& cf = class_flops(q);
+      timing.flops_fock += (double)js.prims[p][q] * (cf.vrr + prim_overhead_flops(q, p == 1)) +
+                           (double)js.quartets[p][q] * (cf.hrr + digest_flops(q, 1));
+    }
+  if (gradient) gradient_run();
+  timing.ms_total = wall_ms() - t0;
+}
+
+// dE/dR = sum P dH - sum W dS + 1/2 sum Gamma d(mn|ls) + dV_nn for every
+// molecule: one batched W = 1/2 P F P, the batched one-electron gradient
+// kernel and the two-electron gradient over the FP64 task lists.
+void Batch::gradient_run() {
+  const double t0 = wall_ms();
+  launch_batch_wdens(nmol, dargs, W, stream);
+  launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.P, dmax, stream);
+  launch_zero(grad_dev, 3 * (size_t)natoms_tot * sizeof(double), stream);
+  OneEGradArgs g1;
+  g1.natoms = 0;
+  g1.atoms = atoms_dev;
+  g1.boys_mode = opt.boys_mode;
+  g1.P = dargs.P;
+  g1.W = W;
+  g1.nbf = 0;
+  g1.grad = grad_dev;
+  g1.natoms_total = natoms_tot;
+  launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
+  unsigned long long* gstats = stats_dev + sizeof(JkStats) / sizeof(unsigned long long);
+  PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
+  GradArgs g2;
+  g2.Pt = dargs.P;
+  g2.Pa = dargs.P;
+  g2.Pb = dargs.P;
+  g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
+  g2.ns_ld = ns_max;
+  g2.thresh = opt.schwarz_thresh;
+  g2.uhf = 0;
+  g2.grad = grad_dev;
+  g2.stats = gstats;
+  for (int bc = NCLASS - 1; bc >= 0; --bc)
+    for (int kc = bc; kc >= 0; --kc) launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
+  grad_host.assign(3 * (size_t)natoms_tot, 0.0);
+  PF_CUDA(cudaMemcpyAsync(grad_host.data(), grad_dev, grad_host.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                          stream));
+  unsigned long long cnt[2 * NQCLASS];
+  PF_CUDA(cudaMemcpyAsync(cnt, gstats, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  timing.flops_grad = 0.0;
+  for (int q = 0; q < NQCLASS; ++q)
+    timing.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false));
+  // nuclear repulsion (molecule.f90:31-52 differentiated)
+  for (const auto& M : mols)
+    for (int i = 0; i < M.natoms; ++i)
+      for (int j = 0; j < M.natoms; ++j) {
+        if (i == j) continue;
+        double d[3], r2 = 0.0;
+        for (int x = 0; x < 3; ++x) {
+          d[x] = M.xyz[3 * i + x] - M.xyz[3 * j + x];
+          r2 += d[x] * d[x];
+        }
+        const double r = std::sqrt(r2);
+        if (r <= 1.0e-10) continue;
+        for (int x = 0; x < 3; ++x)
+          grad_host[3 * (size_t)(M.atom_off + i) + x] -= (double)M.Z[i] * M.Z[j] * d[x] / (r2 * r);
+      }
+  timing.ms_grad = wall_ms() - t0;
+}
+
+}  // namespace pyfacc

@@ -1,0 +1,170 @@
+// Batched engine: many closed-shell molecules of uneven size converged
+// together on one GPU.
+//
+// Layout in HBM: the shells, shell pairs and primitive-pair records of all
+// molecules are packed into one ShellDev / PairData (pairs sorted by class,
+// then molecule, then Schwarz factor, so the kets of a bra are a contiguous
+// segment of its own molecule); every n x n matrix of molecule m lives at
+// offset mat_off[m] = sum_{k<m} n_k^2 of a packed array with leading
+// dimension n_m, and its shell-block density maxima at m * ns_max^2.
+//
+// One SCF iteration of the whole batch is one CUDA graph: the shell-block
+// density maxima of the build density, the J/K class kernels over the
+// quartets of all molecules, and one dense-step kernel with a thread block
+// per molecule (Fock matrix, energy, DIIS, Loewdin-orthogonalised TC2
+// purification and the next build density, all on chip).  Converged
+// molecules get a zero build density, so later builds skip their quartets.
+#pragma once
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "pool.h"
+
+namespace pyfacc {
+
+constexpr int BATCH_DIIS_MAX = 8;
+constexpr int BATCH_THREADS = 256;   // threads of a dense-step block
+constexpr int BATCH_NBF_MAX = 160;   // larger molecules run on their own
+
+struct BatchMolDev {
+  int nbf, nocc, ns, natoms;
+  int occ_off, pad;    // first diagonal entry of the molecule in the guess occupations
+  long long mat_off;   // first element of the molecule's n x n blocks
+  long long diis_off;  // first element of its DIIS history (ndiis F then ndiis errors)
+};
+
+struct BatchMolState {
+  double E, E_prev, err, dD, E_final;
+  double B[BATCH_DIIS_MAX * BATCH_DIIS_MAX];  // DIIS error overlaps
+  int age[BATCH_DIIS_MAX];                    // iteration that filled a slot, -1 empty
+  int iter, head, converged, done, failed, tc2_steps, pad[2];
+};
+
+struct BatchDenseArgs {
+  const BatchMolDev* mol;
+  BatchMolState* st;
+  const double *S, *H, *X;
+  double *F, *J, *K, *Jd, *Kd, *P, *Db, *T1, *T2, *T3;
+  double *diis;
+  int ndiis, max_iter, rebuild_every, incremental;
+  double e_tol, eps_diis, eps_density;
+  int* active;     // molecules still iterating after this step (atomic count)
+  int smem_nmax;   // molecules with nbf <= smem_nmax keep the TC2 iterate in shared memory
+};
+
+// X = S^{-1/2} of every molecule (coupled Newton-Schulz), into Xout; F, T1..T3
+// are work space.  A molecule whose iteration does not converge is marked failed.
+void launch_batch_lowdin(int nmol, const BatchDenseArgs& a, double* Xout, cudaStream_t s);
+// Dynamic shared memory of the dense-step kernels (the TC2 iterate of the
+// molecules with nbf <= a.smem_nmax); called once before any launch/capture.
+void batch_set_smem(const BatchDenseArgs& a);
+// P = diag(occ[occ_off + i]) of every molecule (atomic-occupation guess).
+void launch_batch_guess(int nmol, const BatchDenseArgs& a, const double* occ, cudaStream_t s);
+// Density of F = H (core guess) or of the guess already in P: sets P,
+// Db = P (the first build is full), resets the per-molecule state.
+void launch_batch_init(int nmol, const BatchDenseArgs& a, int core_guess, cudaStream_t s);
+// One SCF step after a J/K build of Db into Jd/Kd.
+void launch_batch_step(int nmol, const BatchDenseArgs& a, cudaStream_t s);
+// Db = P of the finished molecules (0 for the others) before the FP64 polish build.
+void launch_batch_polish_density(int nmol, const BatchDenseArgs& a, cudaStream_t s);
+// F and E of the final density after a full FP64 build (mixed precision);
+// E -> st.E_final.
+void launch_batch_polish(int nmol, const BatchDenseArgs& a, cudaStream_t s);
+// Energy-weighted density W = 1/2 P F P into out.
+void launch_batch_wdens(int nmol, const BatchDenseArgs& a, double* out, cudaStream_t s);
+// Shell-block maxima |D| of every molecule: dm[m * ns_max^2 + a * ns_max + b].
+// mt[m] = {first shell, ns, mat_off, nbf} (mat_off below 2^31).
+void launch_batch_dmax(int nmol, int ns_max, const int4* mt, const int* bf_off, const int* nfun, const double* D,
+                       float* dm, cudaStream_t s);
+
+struct BatchMolHost {
+  int natoms = 0, nbf = 0, ns = 0, nalpha = 0, nbeta = 0, nocc = 0;
+  int atom_off = 0, shell_off = 0;
+  long long mat_off = 0, diis_off = 0;
+  double e_nuc = 0.0;
+  std::vector<int> Z;
+  std::vector<double> xyz;
+  std::vector<std::string> species;
+  Basis basis;
+};
+
+struct BatchTiming {
+  double ms_total = 0, ms_setup = 0, ms_1e = 0, ms_tune = 0, ms_scf = 0, ms_polish = 0, ms_grad = 0;
+  int iterations = 0;
+  double flops_fock = 0.0, flops_grad = 0.0;
+  unsigned long long quartets[2] = {0, 0};
+  int width[NQCLASS] = {32, 32, 32, 32, 32, 32};
+};
+
+class Batch {
+ public:
+  // Closed-shell molecules with nbf <= BATCH_NBF_MAX.
+  Batch(const std::vector<BatchMolHost>& mols, const pyfacc_options& o);
+  ~Batch();
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+  void run(bool gradient);
+  // per molecule: energy, iterations, convergence, failure, gradient (3 natoms)
+  double energy(int m) const;
+  int iterations(int m) const { return st_host[m].iter; }
+  bool converged(int m) const { return st_host[m].converged != 0; }
+  bool failed(int m) const { return st_host[m].failed != 0; }
+  double last_delta_e(int m) const { return std::fabs(st_host[m].E - st_host[m].E_prev); }
+  double last_error(int m) const { return st_host[m].err; }
+  const double* gradient(int m) const { return grad_host.data() + 3 * (size_t)mols[m].atom_off; }
+  BatchTiming timing;
+
+ private:
+  pyfacc_options opt;
+  int device = 0, num_sms = 148;
+  GpuContext ctx;
+  cudaStream_t stream = nullptr;
+  std::vector<BatchMolHost> mols;
+  int nmol = 0, ns_tot = 0, natoms_tot = 0, ns_max = 0, nbf_max = 0;
+  long long mtot = 0;
+  ShellDev shd;
+  double4* atoms_dev = nullptr;
+  int2* pairs1e[NCLASS] = {nullptr, nullptr, nullptr};
+  int n1e[NCLASS] = {0, 0, 0};
+  int* bf_off_dev = nullptr;
+  int* nfun_dev = nullptr;
+  int4* mt_dev = nullptr;
+  PairData pd;
+  std::vector<int> seg[NCLASS];   // per class: nmol + 1 pair offsets (relative to the class start)
+  TaskList tasks_w[3][NCLASS][NCLASS][3];  // per width (32, 16, 8)
+  TaskList tasks[NCLASS][NCLASS][3];       // the widths in use
+  DeviceBuf task_buf;
+  DeviceBuf mats, state_buf;
+  BatchDenseArgs dargs{};
+  double *S = nullptr, *T = nullptr, *V = nullptr, *W = nullptr;
+  float* dmax = nullptr;
+  unsigned long long* stats_dev = nullptr;
+  double* grad_dev = nullptr;
+  int* active_dev = nullptr;
+  int* active_host = nullptr;   // pinned
+  cudaGraphExec_t graph_full = nullptr, graph_inc = nullptr;
+  long long graph_launches[2] = {0, 0};   // kernels per replay of graph_full / graph_inc
+  std::vector<BatchMolState> st_host;
+  std::vector<double> grad_host;
+  std::vector<double> occ_host;          // atomic-occupation guess, all molecules' diagonals
+  DeviceBuf occ_buf;
+
+  void upload();
+  void build_pairs();
+  void build_tasks();
+  void alloc();
+  // J/K of Db into Jd/Kd: FP64 lists, or the FP64 + FP32 halves of mixed mode
+  void fock_build(bool mixed_lists, double thresh, unsigned long long* stats);
+  void tune();
+  cudaGraphExec_t capture(bool full, long long* launches);
+  void gradient_run();
+};
+
+// Molecule description -> host record (species, electrons, basis, E_nn);
+// throws Error on bad input.  uhf is set when the molecule needs UHF under
+// the options' scf_type.
+BatchMolHost batch_parse(const pyfacc_molecule& m, const pyfacc_options& o, bool* uhf);
+
+}  // namespace pyfacc

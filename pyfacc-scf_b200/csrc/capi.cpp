@@ -6,6 +6,9 @@
 #include <memory>
 #include <string>
 
+#include <vector>
+
+#include "batch.h"
 #include "engine.h"
 #include "system.h"
 
@@ -16,6 +19,7 @@ namespace {
 
 thread_local int g_last_status = PYFACC_OK;
 thread_local std::string g_last_message;
+thread_local pyfacc::BatchTiming g_batch_stats;
 
 template <typename Fn>
 int guarded(Fn&& fn) {
@@ -96,6 +100,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->data_dir = nullptr;
   o->guess = PYFACC_GUESS_ATOMIC;
   o->incremental_thresh = 1e-11;
+  o->task_width = 0;
 }
 
 // scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.
@@ -152,16 +157,102 @@ int pyfacc_run(const pyfacc_molecule* mol, const pyfacc_options* opt, pyfacc_res
   return st != PYFACC_OK ? st : status;
 }
 
-// Molecules one after another on the current GPU (the batched engine
-// replaces this loop; statuses are per molecule, the return value the worst).
+// Closed-shell molecules of up to 160 basis functions run together in the
+// batched engine (batch.h); open-shell or larger molecules, molecules whose
+// results ask for matrices or orbitals, and any molecule whose batched
+// purification or orthogonalisation did not converge run one by one through
+// pyfacc_run.  The return value is the worst per-molecule status.
 int pyfacc_run_batch(int nmol, const pyfacc_molecule* mols, const pyfacc_options* opt, pyfacc_result* res) {
   if (nmol < 0 || (nmol > 0 && !mols)) return PYFACC_ERR_INVALID;
-  int worst = PYFACC_OK;
+  pyfacc_options o;
+  if (opt) o = *opt; else pyfacc_default_options(&o);
+  std::vector<int> status(nmol, PYFACC_OK), single, in_batch;
+  std::vector<pyfacc::BatchMolHost> hosts;
   for (int i = 0; i < nmol; ++i) {
-    const int s = pyfacc_run(&mols[i], opt, res ? &res[i] : nullptr);
-    if (s != PYFACC_OK && (worst == PYFACC_OK || worst == PYFACC_ERR_NOT_CONVERGED)) worst = s;
+    pyfacc_result* r = res ? &res[i] : nullptr;
+    const bool wants_matrices = r && (r->S || r->T || r->V || r->P || r->C_alpha || r->C_beta || r->eps_alpha ||
+                                      r->eps_beta);
+    bool uhf = false;
+    pyfacc::BatchMolHost h;
+    const int st = guarded([&] { h = pyfacc::batch_parse(mols[i], o, &uhf); });
+    if (st != PYFACC_OK) {
+      status[i] = st;
+      if (r) r->energy = std::numeric_limits<double>::quiet_NaN();
+      continue;
+    }
+    if (uhf || wants_matrices || h.nbf > pyfacc::BATCH_NBF_MAX) {
+      single.push_back(i);
+    } else {
+      in_batch.push_back(i);
+      hosts.push_back(std::move(h));
+    }
   }
+  if (!hosts.empty()) {
+    const int st = guarded([&] {
+      pyfacc::Batch b(hosts, o);
+      b.run(o.compute_gradient != 0);
+      const pyfacc::BatchTiming& t = b.timing;
+      g_batch_stats = t;
+      for (size_t k = 0; k < in_batch.size(); ++k) {
+        const int i = in_batch[k];
+        if (b.failed((int)k)) {
+          single.push_back(i);
+          continue;
+        }
+        status[i] = b.converged((int)k) ? PYFACC_OK : PYFACC_ERR_NOT_CONVERGED;
+        if (!res) continue;
+        pyfacc_result* r = &res[i];
+        const pyfacc::BatchMolHost& h = hosts[k];
+        r->energy = b.energy((int)k);
+        r->e_elec = r->energy - h.e_nuc;
+        r->e_nuc = h.e_nuc;
+        r->converged = b.converged((int)k) ? 1 : 0;
+        r->n_iter = b.iterations((int)k);
+        r->scf_type = PYFACC_SCF_RHF;
+        r->nbf = h.nbf;
+        r->nshell = h.ns;
+        r->n_fock_builds = b.iterations((int)k) + (o.precision == PYFACC_PRECISION_MIXED ? 1 : 0);
+        r->last_delta_e = b.last_delta_e((int)k);
+        r->last_diis_error = b.last_error((int)k);
+        if (r->gradient && o.compute_gradient)
+          std::memcpy(r->gradient, b.gradient((int)k), 3 * (size_t)h.natoms * sizeof(double));
+        // whole-batch statistics
+        r->ms_total = t.ms_total;
+        r->ms_one_electron = t.ms_1e;
+        r->ms_fock = t.ms_scf + t.ms_polish;
+        r->ms_diag = 0.0;
+        r->ms_gradient = t.ms_grad;
+        r->quartets_fp64 = (long long)t.quartets[0];
+        r->quartets_fp32 = (long long)t.quartets[1];
+        r->flops_fock = t.flops_fock;
+        r->flops_gradient = t.flops_grad;
+        r->task_width = t.width[pyfacc::NQCLASS - 1];
+      }
+    });
+    if (st != PYFACC_OK)
+      for (int i : in_batch) {
+        status[i] = st;
+        if (res) res[i].energy = std::numeric_limits<double>::quiet_NaN();
+      }
+  }
+  for (int i : single) status[i] = pyfacc_run(&mols[i], &o, res ? &res[i] : nullptr);
+  int worst = PYFACC_OK;
+  for (int s : status)
+    if (s != PYFACC_OK && (worst == PYFACC_OK || worst == PYFACC_ERR_NOT_CONVERGED)) worst = s;
   return worst;
+}
+
+// Statistics of the last batched run on this thread (extension).
+int pyfacc_batch_last_stats(double* out, int n) {
+  if (!out || n <= 0) return PYFACC_ERR_INVALID;
+  const pyfacc::BatchTiming& b = g_batch_stats;
+  const double v[] = {b.ms_total, b.ms_setup, b.ms_1e, b.ms_tune, b.ms_scf, b.ms_polish, b.ms_grad,
+                      (double)b.iterations, b.flops_fock, b.flops_grad, (double)b.quartets[0],
+                      (double)b.quartets[1], (double)b.width[0], (double)b.width[1], (double)b.width[2],
+                      (double)b.width[3], (double)b.width[4], (double)b.width[5]};
+  const int nv = (int)(sizeof(v) / sizeof(v[0]));
+  for (int k = 0; k < n; ++k) out[k] = k < nv ? v[k] : 0.0;
+  return PYFACC_OK;
 }
 
 int pyfacc_system_create(const pyfacc_molecule* mol, const pyfacc_options* opt, pyfacc_system** out) {

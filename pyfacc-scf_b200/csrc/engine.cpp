@@ -66,6 +66,9 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
     PF_CUDA(cudaGetDevice(&device));
   }
   PF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  if (opt.task_width != 0 && opt.task_width != 8 && opt.task_width != 16 && opt.task_width != 32)
+    throw Error(PYFACC_ERR_INVALID, "task_width must be 0, 8, 16 or 32");
+  if (opt.task_width) task_width = opt.task_width;
   ensure_boys_tables(device);
   ctx = context_acquire(device);
   stream = ctx.stream;
@@ -414,12 +417,13 @@ void System::build_tasks() {
           lo[i] = l;
           hi[i] = h;
           toff[i] = ntask;
-          ntask += (h - l + TASK_WIDTH - 1) / TASK_WIDTH;
+          ntask += (h - l + task_width - 1) / task_width;
           quart += h - l;
         }
         toff[nb] = ntask;
         if (prec == 0) quartets_total += quart;
         TaskList& tl = tasks[bc][kc][prec];
+        tl.width = task_width;
         tl.nbra = nb;
         tl.ntasks = ntask;
         tl.nquartets = quart;
@@ -446,6 +450,7 @@ void System::build_tasks() {
       const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
       for (int part = 0; part < 2; ++part) {
         TaskList& tl = dyn.lists[2 * qc + part];
+        tl.width = task_width;
         tl.nbra = nb;
         tl.ntasks = std::max(1, tasks[bc][kc][0].ntasks);
         tl.task_off = dd;

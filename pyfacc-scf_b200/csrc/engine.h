@@ -40,7 +40,7 @@ struct Error : std::runtime_error {
 
 constexpr int NCLASS = 3;        // ss, ps, pp
 constexpr int NQCLASS = 6;       // (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|pp)
-constexpr int TASK_WIDTH = 32;   // kets per task = lanes per warp
+constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis
 struct Shell {
@@ -54,6 +54,9 @@ struct Basis {
   std::vector<int> bf_off;  // nshell + 1
   int nbf = 0;
 };
+
+// Diagonal atomic-occupation guess of a minimal basis (scf.cpp).
+std::vector<double> atomic_occupations(const Basis& basis, const std::vector<int>& Z, int nelec);
 
 // basis.cpp
 const char* element_symbol(int z);
@@ -83,6 +86,7 @@ struct TaskList {
   const int* ntasks_dev = nullptr;  // device count of a list built on the GPU
   int bra_offset = 0;   // first bra of this (shard of the) list within its class
   int task_begin = 0;   // global index of the first task (task_off values are global)
+  int width = TASK_WIDTH;  // kets per task: 32, 16 or 8 (a warp runs 32 / width tasks)
 };
 
 // Packed pair data of one molecule or of a batch (every pair stores the
@@ -119,6 +123,7 @@ double digest_flops(int qclass, int nk);
 // ------------------------------------------------------------- launchers
 // Every kernel launch of this library is counted (pyfacc_launch_count).
 void count_launch();
+void count_launches(long long n);  // kernels of a replayed CUDA graph
 long long launch_count();
 void ensure_boys_tables(int device);
 void launch_boys_test(int mode, int fp32, int mmax, int n, const double* x, double* out, cudaStream_t s);
@@ -130,6 +135,7 @@ struct ShellDev {  // device copies of the shells (packed over a batch)
   int* nprim = nullptr;
   double* ex = nullptr;
   double* co = nullptr;
+  int4* mol = nullptr;      // batches: per shell {first atom, natoms, mat_off, ld} of its molecule
   DeviceBuf buf;
 };
 
@@ -215,6 +221,7 @@ struct OneEGradArgs {
   const double* W;
   int nbf;
   double* grad;
+  int natoms_total;  // length of grad / 3 (all molecules of a batch)
 };
 void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEGradArgs& a,
                    int num_sms, cudaStream_t s);

@@ -25,6 +25,7 @@ namespace pyfacc {
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 // ===========================================================================
@@ -105,7 +106,9 @@ __device__ __forceinline__ double prim_norm(int l, double a) {
   return l == 0 ? n : n * 2.0 * sqrt(a);
 }
 
-// pl0 = {shell a, shell b, prim_start, 0}, pl1 = {mat_off, ld, molecule, 0}.
+// pl0 = {shell a, shell b, prim_start, first shell of the molecule},
+// pl1 = {mat_off, ld, molecule, dmax_off}; info1 holds molecule-local shell
+// indices (the density-maximum blocks of a molecule start at dmax_off).
 // Every primitive pair is written (the Schwarz factors use them all);
 // kept[i] counts those with |K| >= cut, the ones the gather keeps.
 __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, const int4* __restrict__ desc,
@@ -125,7 +128,7 @@ __global__ void build_pairs_kernel(int npair, const double4* __restrict__ cen, c
   const double ABx = A.x - B.x, ABy = A.y - B.y, ABz = A.z - B.z;
   const double ab2 = ABx * ABx + ABy * ABy + ABz * ABz;
   info0[i] = make_int4(da.z, db.z, ps, na * nb);
-  info1[i] = make_int4(a, b, da.y, db.y);
+  info1[i] = make_int4(a - p0.w, b - p0.w, da.y, db.y);
   info2[i] = pl1[i];
   geom[i] = make_double4(ABx, ABy, ABz, 0.0);
   const double c0 = 5.9149671727956128778;  // sqrt(2) * pi^(5/4)
@@ -359,7 +362,20 @@ struct JkKernelArgs {
   const int* ket_lo;
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec, task_begin;
+  int lwidth;  // log2 of the task width: one warp runs 32 >> lwidth tasks of (1 bra) x (1 << lwidth kets)
 };
+
+// Whether any lane of this lane's aligned group of w lanes is active.
+__device__ __forceinline__ bool active_any(unsigned mask, int lane, int w) {
+  const unsigned gm = (w == 32) ? 0xffffffffu : (((1u << w) - 1u) << (lane & ~(w - 1)));
+  return (mask & gm) != 0u;
+}
+
+// Sum over the aligned group of w lanes (w a power of two <= 32).
+__device__ __forceinline__ double group_sum(double v, int w) {
+  for (int o = w >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* records(const JkKernelArgs& a);
 template <> __device__ __forceinline__ const double4* records<double>(const JkKernelArgs& a) { return a.prim; }
@@ -373,13 +389,16 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const JkArgs& A = args.a;
   const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
-  for (int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tl < ntasks; tl += nw) {
-    const int t = args.task_begin + tl;
+  const int lw = args.lwidth, W = 1 << lw, sub = lane & (W - 1), tpw = 32 >> lw;
+  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < ntasks; tb += nw * tpw) {
+    const int tl = tb + (lane >> lw);
+    const bool valid = tl < ntasks;
+    const int t = args.task_begin + (valid ? tl : ntasks - 1);
     const int ib = find_bra(args.task_off, args.nbra, t);
-    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
+    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * W + sub;
     const int bp = args.bra_base + ib;
     const int kp = args.ket_base + ket;
-    bool active = ket < __ldg(args.ket_hi + ib);
+    bool active = valid && ket < __ldg(args.ket_hi + ib);
     const int4 bi0 = args.info0[bp], bi1 = args.info1[bp], bi2 = args.info2[bp];
     const double4 bg = args.geom[bp];
     int4 ki0 = bi0, ki1 = bi1;
@@ -389,7 +408,7 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
       ki1 = args.info1[kp];
       kg = args.geom[kp];
       if (A.dmax) {
-        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
         active = bound >= (float)A.thresh;
       }
     }
@@ -449,8 +468,8 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
           }
 #pragma unroll
     for (int i = 0; i < NA * NB; ++i) {
-      const double s = warp_sum(jab[i]);
-      if (lane == 0 && s != 0.0) atomicAdd(A.J + mo + (size_t)(ma + i / NB) * ld + mb + i % NB, 2.0 * s);
+      const double s = group_sum(jab[i], W);
+      if (sub == 0 && s != 0.0) atomicAdd(A.J + mo + (size_t)(ma + i / NB) * ld + mb + i % NB, 2.0 * s);
     }
     if (active) {
 #pragma unroll
@@ -545,6 +564,11 @@ static void jk_dispatch(int qc, int nk, dim3 grid, dim3 block, cudaStream_t s, c
   }
 }
 
+static int width_log2(int w) {
+  if (w != 8 && w != 16 && w != 32) throw Error(PYFACC_ERR_INVALID, "task width must be 8, 16 or 32");
+  return w == 8 ? 3 : (w == 16 ? 4 : 5);
+}
+
 static int grid_for(int ntasks, int num_sms) {
   long long warps_needed = ntasks;
   long long blocks = (warps_needed + 3) / 4;
@@ -567,7 +591,8 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
   k.prec = fp32 ? 1 : 0;
-  dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
+  k.lwidth = width_log2(tl.width);
+  dim3 grid(grid_for((tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width), num_sms)), block(128);
   if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, s, k);
   else jk_dispatch<double>(k.qclass, nk, grid, block, s, k);
   PF_CUDA(cudaGetLastError());
@@ -606,6 +631,7 @@ struct DynAllArgs {
   const double4* geom;
   const double* dmax_global;
   double thresh, fp32_thresh;
+  int width;
 };
 
 __device__ __forceinline__ int ket_prefix(const double4* __restrict__ geom, int ket_base, int nket, double qb, double t) {
@@ -636,7 +662,7 @@ __global__ void __launch_bounds__(1024) dyn_tasks_kernel(const DynAllArgs A) {
       const int lo = L.part == 0 ? 0 : m64, hi = L.part == 0 ? m64 : m;
       L.ket_lo[i] = lo;
       L.ket_hi[i] = hi;
-      cnt = (hi - lo + TASK_WIDTH - 1) / TASK_WIDTH;
+      cnt = (hi - lo + A.width - 1) / A.width;
     }
     // block exclusive scan of cnt
     int v = cnt;
@@ -680,6 +706,7 @@ void launch_dyn_tasks(const PairData& pd, const float* dmax, int ns, double thre
   A.dmax_global = dt.dmax_global;
   A.thresh = thresh;
   A.fp32_thresh = fp32_thresh;
+  A.width = dt.lists[0].width;
   int k = 0;
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
@@ -719,6 +746,7 @@ struct GradKernelArgs {
   const int* ket_lo;
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, task_begin;
+  int lwidth;
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
@@ -733,13 +761,16 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const GradArgs& A = args.a;
-  for (int tl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; tl < args.ntasks; tl += nw) {
-    const int t = args.task_begin + tl;
+  const int lw = args.lwidth, W = 1 << lw, sub = lane & (W - 1), tpw = 32 >> lw;
+  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < args.ntasks; tb += nw * tpw) {
+    const int tl = tb + (lane >> lw);
+    const bool valid = tl < args.ntasks;
+    const int t = args.task_begin + (valid ? tl : args.ntasks - 1);
     const int ib = find_bra(args.task_off, args.nbra, t);
-    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * TASK_WIDTH + lane;
+    const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * W + sub;
     const int bp = args.bra_base + ib;
     const int kp = args.ket_base + ket;
-    bool active = ket < __ldg(args.ket_hi + ib);
+    bool active = valid && ket < __ldg(args.ket_hi + ib);
     const int4 bi0 = args.info0[bp], bi1 = args.info1[bp], bi2 = args.info2[bp];
     const double4 bg = args.geom[bp];
     int4 ki0 = bi0, ki1 = bi1;
@@ -749,7 +780,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       ki1 = args.info1[kp];
       kg = args.geom[kp];
       if (A.dmax) {
-        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
         active = bound >= (float)A.thresh;
       }
     }
@@ -824,13 +855,13 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
 #pragma unroll
       for (int i = 0; i < 9; ++i) g[i] = fac * (double)gr[i];
     }
-    // centre A and B are the bra's, uniform across the warp
+    // centre A and B are the bra's, uniform across a task's lanes
     double* G = A.grad;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-      const double sa = warp_sum(g[x]);
-      const double sb = warp_sum(g[3 + x]);
-      if (lane == 0) {
+      const double sa = group_sum(g[x], W);
+      const double sb = group_sum(g[3 + x], W);
+      if (sub == 0 && active_any(amask, lane, W)) {
         atomicAdd(G + 3 * bi1.z + x, sa);
         atomicAdd(G + 3 * bi1.w + x, sb);
       }
@@ -870,7 +901,8 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   k.bra_base = pd.class_off[bc] + tl.bra_offset; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
-  dim3 grid(grid_for(tl.ntasks, num_sms)), block(128);
+  k.lwidth = width_log2(tl.width);
+  dim3 grid(grid_for((tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width), num_sms)), block(128);
   if (fp32) grad2e_dispatch<float>(k.qclass, grid, block, s, k);
   else grad2e_dispatch<double>(k.qclass, grid, block, s, k);
   PF_CUDA(cudaGetLastError());
@@ -887,9 +919,12 @@ __global__ void eri_tensor_kernel(const JkKernelArgs args, int n, double* __rest
   using C = EriClass<double, LA, LB, LC, LD>;
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < args.ntasks; t += nw) {
+  const int lw = args.lwidth, tpw = 32 >> lw;
+  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < args.ntasks; tb += nw * tpw) {
+    const int t = tb + (lane >> lw);
+    if (t >= args.ntasks) continue;
     const int ib = find_bra(args.task_off, args.nbra, t);
-    const int ket = args.ket_lo[ib] + (t - args.task_off[ib]) * TASK_WIDTH + lane;
+    const int ket = args.ket_lo[ib] + (t - args.task_off[ib]) * (1 << lw) + (lane & ((1 << lw) - 1));
     if (ket >= args.ket_hi[ib]) continue;
     const int bp = args.bra_base + ib, kp = args.ket_base + ket;
     const int4 bi0 = args.info0[bp], ki0 = args.info0[kp];
@@ -923,6 +958,7 @@ void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bc, int kc, i
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
   k.nbra = tl.nbra; k.ntasks = tl.ntasks;
   k.bra_base = pd.class_off[bc]; k.ket_base = pd.class_off[kc];
+  k.lwidth = width_log2(tl.width);
   dim3 grid((tl.ntasks + 3) / 4), block(128);
   switch (qclass_of(bc, kc)) {
     case 0: eri_tensor_kernel<0, 0, 0, 0><<<grid, block, 0, s>>>(k, nbf, eri); break;
@@ -1030,13 +1066,18 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
                                                            const double4* __restrict__ cen,
                                                            const int4* __restrict__ desc, const int* __restrict__ nprim,
                                                            const double* __restrict__ ex,
-                                                           const double* __restrict__ co, OneEArgs args) {
+                                                           const double* __restrict__ co,
+                                                           const int4* __restrict__ mol, OneEArgs args) {
   using NCl = NucClass<double, LA, LB>;
   constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
   const int lane = threadIdx.x & 31;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= npair) return;
   const int2 pr = pairs[w];
+  // the molecule of the pair: its nuclei and its matrix block
+  const int4 mi = mol ? mol[pr.x] : make_int4(0, args.natoms, 0, args.nbf);
+  const double4* atoms = args.atoms + mi.x;
+  const int natoms = mi.y;
   const int4 da = desc[pr.x], db = desc[pr.y];
   const int na = nprim[pr.x], nb = nprim[pr.y];
   const double4 A = cen[pr.x], B = cen[pr.y];
@@ -1045,7 +1086,7 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
 #pragma unroll
   for (int i = 0; i < NA * NB; ++i) s[i] = t[i] = v[i] = 0.0;
   const int npp = na * nb;
-  const int work = npp * args.natoms;
+  const int work = npp * natoms;
   for (int idx = lane; idx < work; idx += 32) {
     const int pp = idx % npp, c = idx / npp;
     const int ka = pp / nb, kb = pp % nb;
@@ -1066,7 +1107,7 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
           t[ia * NB + ib] += kin3(S, ca, cb, g.al, g.be);
         }
     }
-    const double4 Cn = args.atoms[c];
+    const double4 Cn = atoms[c];
     const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
     double F[PF_BOYS_MMAX + 1];
     boys_runtime(args.boys_mode, LA + LB, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
@@ -1083,16 +1124,16 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
     v[i] = warp_sum(v[i]);
   }
   if (lane == 0) {
-    const int n = args.nbf;
+    const size_t n = mi.w, mo = mi.z;
 #pragma unroll
     for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
       for (int ib = 0; ib < NB; ++ib) {
         const size_t mu = da.z + ia, nu = db.z + ib;
         const int k = ia * NB + ib;
-        if (args.S) { args.S[mu * n + nu] = s[k]; args.S[nu * n + mu] = s[k]; }
-        if (args.T) { args.T[mu * n + nu] = t[k]; args.T[nu * n + mu] = t[k]; }
-        if (args.V) { args.V[mu * n + nu] = v[k]; args.V[nu * n + mu] = v[k]; }
+        if (args.S) { args.S[mo + mu * n + nu] = s[k]; args.S[mo + nu * n + mu] = s[k]; }
+        if (args.T) { args.T[mo + mu * n + nu] = t[k]; args.T[mo + nu * n + mu] = t[k]; }
+        if (args.V) { args.V[mo + mu * n + nu] = v[k]; args.V[mo + nu * n + mu] = v[k]; }
       }
   }
 }
@@ -1102,9 +1143,9 @@ void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const
   for (int c = 0; c < NCLASS; ++c) {
     if (npair[c] <= 0) continue;
     dim3 grid((npair[c] + 3) / 4), block(128);
-    if (c == 0) one_electron_kernel<0, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
-    if (c == 1) one_electron_kernel<1, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
-    if (c == 2) one_electron_kernel<1, 1><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+    if (c == 0) one_electron_kernel<0, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
+    if (c == 1) one_electron_kernel<1, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
+    if (c == 2) one_electron_kernel<1, 1><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
     PF_CUDA(cudaGetLastError());
     count_launch();
   }
@@ -1119,17 +1160,23 @@ template <int LA, int LB>
 __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __restrict__ pairs,
                                                      const double4* __restrict__ cen, const int4* __restrict__ desc,
                                                      const int* __restrict__ nprim, const double* __restrict__ ex,
-                                                     const double* __restrict__ co, OneEGradArgs args) {
+                                                     const double* __restrict__ co,
+                                                     const int4* __restrict__ mol, int use_smem,
+                                                     OneEGradArgs args) {
   using NCl = NucClass<double, LA, LB>;
   constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
-  extern __shared__ double gsh[];  // 3 * natoms
-  for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x) gsh[i] = 0.0;
-  __syncthreads();
+  extern __shared__ double gsh[];  // 3 * natoms_total when use_smem
+  if (use_smem) {
+    for (int i = threadIdx.x; i < 3 * args.natoms_total; i += blockDim.x) gsh[i] = 0.0;
+    __syncthreads();
+  }
+  double* gacc = use_smem ? gsh : args.grad;  // per-atom accumulator (shared or global)
   const int lane = threadIdx.x & 31;
   const int nwarp_total = (gridDim.x * blockDim.x) >> 5;
-  const int n = args.nbf;
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < npair; w += nwarp_total) {
     const int2 pr = pairs[w];
+    const int4 mi = mol ? mol[pr.x] : make_int4(0, args.natoms, 0, args.nbf);
+    const size_t n = mi.w, mo = mi.z;
     const int4 da = desc[pr.x], db = desc[pr.y];
     const int na = nprim[pr.x], nb = nprim[pr.y];
     const double4 A = cen[pr.x], B = cen[pr.y];
@@ -1140,7 +1187,7 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
     for (int ia = 0; ia < NA; ++ia)
 #pragma unroll
       for (int ib = 0; ib < NB; ++ib) {
-        const size_t k = (size_t)(da.z + ia) * n + db.z + ib;
+        const size_t k = mo + (size_t)(da.z + ia) * n + db.z + ib;
         Pd[ia * NB + ib] = wgt * args.P[k];
         Wd[ia * NB + ib] = wgt * args.W[k];
       }
@@ -1179,8 +1226,8 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
         }
     }
     // nuclear attraction: lanes over nuclei, all primitive pairs each
-    for (int c = lane; c < args.natoms; c += 32) {
-      const double4 Cn = args.atoms[c];
+    for (int c = lane; c < mi.y; c += 32) {
+      const double4 Cn = args.atoms[mi.x + c];
       double gv[6] = {0, 0, 0, 0, 0, 0};
       for (int pp = 0; pp < npp; ++pp) {
         const int ka = pp / nb, kb = pp % nb;
@@ -1201,41 +1248,49 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
       for (int x = 0; x < 3; ++x) {
         gA[x] += gv[x];
         gB[x] += gv[3 + x];
-        atomicAdd(gsh + 3 * c + x, -(gv[x] + gv[3 + x]));
+        atomicAdd(gacc + 3 * (mi.x + c) + x, -(gv[x] + gv[3 + x]));
       }
     }
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
       const double sa = warp_sum(gA[x]), sb = warp_sum(gB[x]);
       if (lane == 0) {
-        atomicAdd(gsh + 3 * da.y + x, sa);
-        atomicAdd(gsh + 3 * db.y + x, sb);
+        atomicAdd(gacc + 3 * da.y + x, sa);
+        atomicAdd(gacc + 3 * db.y + x, sb);
       }
     }
   }
+  if (!use_smem) return;
   __syncthreads();
-  for (int i = threadIdx.x; i < 3 * args.natoms; i += blockDim.x)
+  for (int i = threadIdx.x; i < 3 * args.natoms_total; i += blockDim.x)
     if (gsh[i] != 0.0) atomicAdd(args.grad + i, gsh[i]);
 }
 
 void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEGradArgs& a,
                    int num_sms, cudaStream_t s) {
-  const size_t smem = 3 * (size_t)a.natoms * sizeof(double);
+  // per-atom partial sums in shared memory while they fit (one molecule),
+  // straight global atomics for the many atoms of a batch
+  const size_t need = 3 * (size_t)a.natoms_total * sizeof(double);
+  const int use_smem = need <= 96 * 1024;
+  const size_t smem = use_smem ? need : 0;
   for (int c = 0; c < NCLASS; ++c) {
     if (npair[c] <= 0) continue;
     const int blocks = std::max(1, std::min((npair[c] + 3) / 4, 2 * num_sms));
     dim3 grid(blocks), block(128);
     if (c == 0) {
       PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<0, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+      grad1e_kernel<0, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
+                                                    sh.mol, use_smem, a);
     }
     if (c == 1) {
       PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<1, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+      grad1e_kernel<1, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
+                                                    sh.mol, use_smem, a);
     }
     if (c == 2) {
       PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<1, 1><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, a);
+      grad1e_kernel<1, 1><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
+                                                    sh.mol, use_smem, a);
     }
     PF_CUDA(cudaGetLastError());
     count_launch();

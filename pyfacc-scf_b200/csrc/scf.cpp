@@ -146,14 +146,17 @@ void System::density_from(const double* C, int nocc, double scale, double* Pm) {
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nocc, &scale, C, nbf, C, nbf, &zero, Pm, nbf));
 }
 
-std::vector<double> System::atomic_occupations() const {
-  std::vector<double> occ(nbf, 0.0);
+// Diagonal starting density from atomic aufbau occupations of the
+// minimal-basis shells: Z electrons per atom over 1s, 2s, 2p, ... (2 per s,
+// 6 per p shell, in the order the basis lists them), scaled to nelec.
+std::vector<double> atomic_occupations(const Basis& basis, const std::vector<int>& Z, int nelec) {
+  const int natoms = (int)Z.size(), ns = (int)basis.shells.size();
+  std::vector<double> occ(basis.nbf, 0.0);
   double total = 0.0;
   for (int a = 0; a < natoms; ++a) {
     std::vector<int> ss, ps;
     for (int s = 0; s < ns; ++s)
       if (basis.shells[s].atom == a) (basis.shells[s].l == 0 ? ss : ps).push_back(s);
-    // 1s, 2s, 2p, 3s, 3p, ... in the order the basis lists them
     std::vector<int> order;
     for (size_t k = 0; k < std::max(ss.size(), ps.size() + 1); ++k) {
       if (k < ss.size()) order.push_back(ss[k]);
@@ -168,10 +171,13 @@ std::vector<double> System::atomic_occupations() const {
       total += take;
     }
   }
-  const double ne = (double)(nalpha + nbeta);
   if (total > 0)
-    for (double& v : occ) v *= ne / total;  // charge
+    for (double& v : occ) v *= (double)nelec / total;  // charge
   return occ;
+}
+
+std::vector<double> System::atomic_occupations() const {
+  return pyfacc::atomic_occupations(basis, Z, nalpha + nbeta);
 }
 
 bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
@@ -561,6 +567,7 @@ void System::gradient(double* g_host) {
   g1.W = Wm;
   g1.nbf = nbf;
   g1.grad = grad_dev;
+  g1.natoms_total = natoms;
   // one-electron terms once (shard 0); the two-electron term is sharded
   if (opt.shard_count <= 1 || opt.shard_rank == 0) launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
   launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Pt, nullptr, nullptr, dmax, stream);
@@ -654,6 +661,7 @@ void System::fill_result(pyfacc_result* r) {
   r->quartets_fp32 = (long long)st.quartets[1];
   r->flops_fock = st.flops_fock;
   r->flops_gradient = st.flops_grad;
+  r->task_width = task_width;
 }
 
 void System::set_coords(const double* coords) {

@@ -71,6 +71,7 @@ struct System {
   double* pstate = nullptr;                      // TC2 state, two buffers of 8 (device)
   bool orbitals_ready = false;
   bool grad_fp32 = false;  // FP32 derivative integrals for small quartets (mixed)
+  int task_width = TASK_WIDTH;  // kets per J/K task
   int purify_steps = 0, purify_fallbacks = 0;
   float* dmax = nullptr;
   std::vector<double*> diis_F, diis_E;

@@ -116,6 +116,7 @@ class ScfResult:
     flops: dict = field(default_factory=dict)
     last_delta_e: float = 0.0
     last_diis_error: float = 0.0
+    task_width: int = 32
 
 
 def _options(**kw) -> N.Options:
@@ -174,7 +175,7 @@ def _to_result(r: N.Result, keep: dict, status: int) -> ScfResult:
                         gradient=r.ms_gradient),
         quartets=dict(fp64=r.quartets_fp64, fp32=r.quartets_fp32),
         flops=dict(fock=r.flops_fock, gradient=r.flops_gradient),
-        last_delta_e=r.last_delta_e, last_diis_error=r.last_diis_error)
+        last_delta_e=r.last_delta_e, last_diis_error=r.last_diis_error, task_width=r.task_width)
 
 
 def _nbf_estimate(mol: Molecule) -> int:
@@ -216,6 +217,21 @@ def run_batch(mols: Sequence[Molecule], gradient: bool = False, check: bool = Tr
     if check:
         N.check(status, "pyfacc_run_batch", allow=(N.OK, N.ERR_NOT_CONVERGED))
     return [_to_result(results[i], res_keep[i], status) for i in range(len(mols))]
+
+
+_BATCH_STAT_KEYS = ("ms_total", "ms_setup", "ms_one_electron", "ms_tune", "ms_scf", "ms_polish", "ms_gradient",
+                    "iterations", "flops_fock", "flops_gradient", "quartets_fp64", "quartets_fp32")
+_QCLASS_NAMES = ("ss|ss", "ps|ss", "ps|ps", "pp|ss", "pp|ps", "pp|pp")
+
+
+def batch_stats() -> dict:
+    """Timings, counters and task widths of the last run_batch on this thread."""
+    n = len(_BATCH_STAT_KEYS) + len(_QCLASS_NAMES)
+    buf = (ctypes.c_double * n)()
+    N.check(lib().pyfacc_batch_last_stats(buf, n), "pyfacc_batch_last_stats")
+    out = {k: buf[i] for i, k in enumerate(_BATCH_STAT_KEYS)}
+    out["task_width"] = {q: int(buf[len(_BATCH_STAT_KEYS) + i]) for i, q in enumerate(_QCLASS_NAMES)}
+    return out
 
 
 def _torch():

@@ -45,7 +45,7 @@ class Options(ctypes.Structure):
         ("boys_mode", c_int), ("schwarz_thresh", c_double), ("fp32_thresh", c_double),
         ("incremental", c_int), ("rebuild_every", c_int), ("compute_gradient", c_int),
         ("device", c_int), ("verbose", c_int), ("shard_rank", c_int), ("shard_count", c_int),
-        ("data_dir", c_char_p), ("guess", c_int), ("incremental_thresh", c_double),
+        ("data_dir", c_char_p), ("guess", c_int), ("incremental_thresh", c_double), ("task_width", c_int),
     ]
 
 
@@ -67,7 +67,7 @@ class Result(ctypes.Structure):
         ("ms_total", c_double), ("ms_one_electron", c_double), ("ms_fock", c_double), ("ms_diag", c_double),
         ("ms_gradient", c_double),
         ("quartets_fp64", ctypes.c_longlong), ("quartets_fp32", ctypes.c_longlong),
-        ("flops_fock", c_double), ("flops_gradient", c_double),
+        ("flops_fock", c_double), ("flops_gradient", c_double), ("task_width", c_int),
     ]
 
 
@@ -85,6 +85,7 @@ SIGNATURES = {
     "pyfacc_default_options": (None, [ctypes.POINTER(Options)]),
     "pyfacc_run": (c_int, [ctypes.POINTER(MoleculeC), ctypes.POINTER(Options), ctypes.POINTER(Result)]),
     "pyfacc_run_batch": (c_int, [c_int, ctypes.POINTER(MoleculeC), ctypes.POINTER(Options), ctypes.POINTER(Result)]),
+    "pyfacc_batch_last_stats": (c_int, [P_double, c_int]),
     "pyfacc_system_create": (c_int, [ctypes.POINTER(MoleculeC), ctypes.POINTER(Options), ctypes.POINTER(c_void_p)]),
     "pyfacc_system_destroy": (None, [c_void_p]),
     "pyfacc_system_info": (c_int, [c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int), ctypes.POINTER(c_int),
