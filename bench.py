@@ -224,6 +224,12 @@ def run_ours(args):
                "delta_e": abs(res40["fp64"][1] - res40["mixed"][1]),
                "max_grad_diff": float(np.abs(res40["fp64"][2] - res40["mixed"][2]).max())}
 
+    # batch of 256 water clusters (H2O)n, n uniform in [4, 16], rank 0 only:
+    # one pyfacc_run_batch call = energies and gradients of all 256 molecules
+    batch = None
+    if rank == 0 and args.workload == "c20h42" and not args.no_batch:
+        batch = batch_measurement(pyfacc, local)
+
     # e2e through the C ABI with host buffers
     m, keep = mol._struct()
     opt = pyfacc._options(precision="mixed", compute_gradient=1, device=local)
@@ -289,6 +295,7 @@ def run_ours(args):
         "data": "synthetic, seeded (geometry builder pyfacc.geometry.alkane)",
         "config": {"workload": WORKLOADS[args.workload]["label"], "precision": "mixed",
                    "schwarz_thresh": 1e-12, "fp32_thresh": 1e-5, "scf": "dE<1e-10, DIIS err<1e-8",
+                   "mixed_energy": "last incremental mixed build (no FP64 polish build)",
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
         "fp64_s_per_step": step_64 / world,
         "mixed_speedup_vs_fp64": step_64 / step_mx,
@@ -298,6 +305,7 @@ def run_ours(args):
         "fock_builds_per_s": 1.0 / fock_s,
         "breakdown_ms": breakdown,
         "north_star_c40h82": c40,
+        "batch_water256": batch,
         "wall_bracket_ms": {"mixed": statistics.mean(ev_mx), "fp64": statistics.mean(ev_64)},
         "e2e": {"value": e2e_step / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "pyfacc_run (C ABI, host coordinates)"},
@@ -309,6 +317,51 @@ def run_ours(args):
     }
     out["gpu_launches"] = int(launches)
     print(json.dumps(out))
+
+
+def batch_measurement(pyfacc, device):
+    """256 water clusters (H2O)n, n ~ U{4..16} (rng seed 3), STO-3G RHF,
+    energies + gradients of all molecules in one pyfacc_run_batch call
+    (host coordinates in, host energies and gradients out), mixed precision
+    and FP64; a sample of the same molecules one by one through pyfacc_run
+    for comparison."""
+    import numpy as np
+    from pyfacc import geometry as G
+    clusters = G.water_clusters(count=256, seed=3)
+    mols = [pyfacc.Molecule(sp, xyz, "sto-3g") for sp, xyz in clusters]
+    out = {"workload": "256 water clusters (H2O)n, n in [4,16], 28-112 bf, STO-3G RHF, energy+gradient",
+           "molecules": len(mols)}
+    res = {}
+    for prec in ("mixed", "fp64"):
+        pyfacc.run_batch(mols, gradient=True, precision=prec, device=device)  # warm-up (task-width tuning)
+        ts = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            r = pyfacc.run_batch(mols, gradient=True, precision=prec, device=device)
+            ts.append(time.perf_counter() - t0)
+        st = pyfacc.batch_stats()
+        res[prec] = r
+        out[prec] = {"s_per_batch": min(ts), "ms_per_molecule": min(ts) * 1e3 / len(mols),
+                     "molecules_per_s": len(mols) / min(ts),
+                     "converged": int(sum(x.converged for x in r)),
+                     "breakdown_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_one_electron", "ms_scf",
+                                                                     "ms_polish", "ms_gradient")},
+                     "iterations": int(st["iterations"]), "task_width": st["task_width"],
+                     "fock_tflops": st["flops_fock"] / max(st["ms_scf"] + st["ms_polish"], 1e-9) / 1e9}
+    out["mixed_speedup_vs_fp64"] = out["fp64"]["s_per_batch"] / out["mixed"]["s_per_batch"]
+    out["delta_e_mixed_vs_fp64"] = max(abs(a.energy - b.energy) for a, b in zip(res["mixed"], res["fp64"]))
+    out["max_grad_diff_mixed_vs_fp64"] = max(float(np.abs(a.gradient - b.gradient).max())
+                                             for a, b in zip(res["mixed"], res["fp64"]))
+    sample = mols[:16]
+    for m in sample[:2]:
+        pyfacc.run(m, gradient=True, precision="mixed", device=device)
+    t0 = time.perf_counter()
+    for m in sample:
+        pyfacc.run(m, gradient=True, precision="mixed", device=device)
+    seq = (time.perf_counter() - t0) / len(sample)
+    out["one_by_one_ms_per_molecule"] = seq * 1e3
+    out["batch_speedup_vs_one_by_one"] = seq / (out["mixed"]["s_per_batch"] / len(mols))
+    return out
 
 
 def cpu_baseline(wl, n_iter, n_fock_builds):
@@ -372,6 +425,7 @@ def main():
     ap.add_argument("--workload", default="c20h42", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-c40", action="store_true", help="skip the C40H82 side measurement")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 256-water-cluster batch measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

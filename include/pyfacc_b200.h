@@ -66,6 +66,13 @@ typedef struct pyfacc_options {
   int task_width;           /* kets per J/K task (8, 16 or 32; a warp runs
                                32/task_width tasks); 0 = 32 for one molecule,
                                chosen by timing for a batch            (0)   */
+  int gradient_precision;   /* PYFACC_PRECISION_* of the derivative
+                               integrals; MIXED evaluates the quartets with
+                               Q_ab Q_cd < fp32_thresh in FP32         (FP64) */
+  int polish;               /* mixed: energy and F of the converged density
+                               from one more full FP64 build (1, |dE| vs
+                               FP64 ~1e-12), or from the last incremental
+                               mixed build (0, |dE| ~1e-8)              (0)   */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {

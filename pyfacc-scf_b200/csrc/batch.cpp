@@ -674,7 +674,7 @@ void Batch::run(bool gradient) {
   timing.iterations = std::min(it, dargs.max_iter);
   timing.ms_scf = wall_ms() - ts;
   // ---- FP64 polish of mixed precision: F and E of the final densities
-  if (mixed) {
+  if (mixed && opt.polish) {
     const double tp = wall_ms();
     launch_batch_polish_density(nmol, dargs, stream);
     fock_build(false, opt.schwarz_thresh, stats_dev);
@@ -730,8 +730,16 @@ void Batch::gradient_run() {
   g2.uhf = 0;
   g2.grad = grad_dev;
   g2.stats = gstats;
+  const bool split = opt.gradient_precision == PYFACC_PRECISION_MIXED;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
+    for (int kc = bc; kc >= 0; --kc) {
+      if (split) {
+        launch_grad2e(pd, tasks[bc][kc][1], bc, kc, false, g2, num_sms, stream);
+        launch_grad2e(pd, tasks[bc][kc][2], bc, kc, true, g2, num_sms, stream);
+      } else {
+        launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
+      }
+    }
   grad_host.assign(3 * (size_t)natoms_tot, 0.0);
   PF_CUDA(cudaMemcpyAsync(grad_host.data(), grad_dev, grad_host.size() * sizeof(double), cudaMemcpyDeviceToHost,
                           stream));

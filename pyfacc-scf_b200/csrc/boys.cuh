@@ -1,13 +1,20 @@
 // Boys function F_m(T) = int_0^1 t^(2m) exp(-T t^2) dt on the device.
 //
-// Accurate mode (default): F_mmax from an 8-term Taylor expansion about the
-// nearest point of a 0.1-spaced grid (|dT| <= 0.05, remainder < 1e-16
-// relative) for T < 36, or for T >= 36 from F_0 = sqrt(pi/T)/2
-// (erfc(6) ~ 2e-17) and the upward recursion
-//   F_{m+1} = ((2m+1) F_m - exp(-T)) / (2T)   (stable for T > m);
-// then the stable downward recursion F_m = (2T F_{m+1} + exp(-T)) / (2m+1).  The grid values are computed once on the host
+// Accurate mode (default): F_L (L = the highest order a class needs) from an
+// 8-term Taylor expansion about the nearest point T_k of a 0.1-spaced grid
+// (|dT| <= 0.05, remainder < 1e-16 relative), read as 8 coefficients
+// F_{L+j}(T_k) / j! per grid point (so the Horner step is one FMA), for
+// T < 36; for T >= 36 from F_0 = sqrt(pi/T)/2 (erfc(6) ~ 2e-17) and the
+// upward recursion F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T) (stable for
+// T > m).  The lower orders follow from the stable downward recursion
+// F_m = (2T F_{m+1} + e^{-T}) / (2m+1), with e^{-T} = e^{-T_k} e^{T_k - T}
+// from e^{-T_k} tabulated on the same 0.1 grid up to T = 100 and the
+// degree-8 Taylor polynomial of e^x on |x| <= 0.05 (remainder < 6e-18
+// relative); beyond T = 100, e^{-T} < 4e-44 and is dropped (a relative
+// change below 1e-29 of F_6).  The grid values are computed once on the host
 // in long double from the positive series (ensure_boys_tables, kernels.cu).
-// FP32 mode (mixed precision) uses the same grid in float with 5 Taylor terms.
+// FP32 mode (mixed precision) uses an unscaled grid in float with 5 Taylor
+// terms and expf.
 //
 // Reference mode: boys.f90:9-43 of PyFAcc-SCF -- Taylor 1/(2m+1) - x/(2m+3)
 // for x <= 1e-6, else the 1001-point trapezoid rule on [0,1].  It is used for
@@ -22,13 +29,18 @@
 #define PF_BOYS_MMAX 6       // highest order needed: (pp|pp) gradient = 5
 #define PF_BOYS_NT 8         // Taylor terms, FP64
 #define PF_BOYS_NTF 5        // Taylor terms, FP32
+#define PF_BOYS_EMAX 100.0   // e^{-T} table end
+#define PF_BOYS_NEXP 1001    // e^{-T_k}, T_k = 0.1 k <= PF_BOYS_EMAX
 #define PF_BOYS_NCOL (PF_BOYS_MMAX + PF_BOYS_NT)
 
 namespace pyfacc {
 
 // Grid tables (this header is included by exactly one translation unit,
-// kernels.cu, which fills them per device with cudaMemcpyToSymbol).
-__device__ double g_boys_tab[PF_BOYS_NGRID * PF_BOYS_NCOL];
+// kernels.cu, which fills them per device with cudaMemcpyToSymbol):
+// g_boys_tl[L][k][j] = F_{L+j}(T_k) / j!, g_boys_exp[k] = e^{-T_k},
+// g_boys_tabf[k][m] = F_m(T_k) in float.
+__device__ __align__(16) double g_boys_tl[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
+__device__ double g_boys_exp[PF_BOYS_NEXP];
 __device__ float g_boys_tabf[PF_BOYS_NGRID * PF_BOYS_NCOL];
 
 // Branch-free: every lane evaluates the Taylor value (from row 0 when T is
@@ -37,19 +49,35 @@ __device__ float g_boys_tabf[PF_BOYS_NGRID * PF_BOYS_NCOL];
 template <int L>
 __device__ __forceinline__ void boys_fp64(double T, double* __restrict__ F) {
   const bool tab = T < PF_BOYS_TMAX;
-  const int k = tab ? __double2int_rn(T * PF_BOYS_INV_STEP) : 0;
-  const double x = k * PF_BOYS_STEP - T;  // F_m(T) = sum_j F_{m+j}(T_k) x^j / j!
-  const double* row = g_boys_tab + k * PF_BOYS_NCOL + L;
-  double f = __ldg(row + PF_BOYS_NT - 1);
-#pragma unroll
-  for (int j = PF_BOYS_NT - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0 / (j + 1));
+  const int ke = __double2int_rn(fmin(T, PF_BOYS_EMAX) * PF_BOYS_INV_STEP);
+  const int k = tab ? ke : 0;
+  const double x = ke * PF_BOYS_STEP - T;  // F_L(T) = sum_j F_{L+j}(T_k) x^j / j! (T < 36)
+  const double2* row = reinterpret_cast<const double2*>(g_boys_tl + ((size_t)L * PF_BOYS_NGRID + k) * PF_BOYS_NT);
+  const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
+  double f = fma(c67.y, x, c67.x);
+  f = fma(f, x, c45.y);
+  f = fma(f, x, c45.x);
+  f = fma(f, x, c23.y);
+  f = fma(f, x, c23.x);
+  f = fma(f, x, c01.y);
+  f = fma(f, x, c01.x);
   const double rt = rsqrt(fmax(T, PF_BOYS_TMAX));
   double fa = 0.88622692545275801365 * rt;  // sqrt(pi/T)/2
   if (L == 0) {
     F[0] = tab ? f : fa;
     return;
   }
-  const double e = exp(-T);
+  // e^x on |x| <= 0.05, Taylor coefficients 1/j!, j = 8 .. 0
+  double ex = 1.0 / 40320.0;
+  ex = fma(ex, x, 1.0 / 5040.0);
+  ex = fma(ex, x, 1.0 / 720.0);
+  ex = fma(ex, x, 1.0 / 120.0);
+  ex = fma(ex, x, 1.0 / 24.0);
+  ex = fma(ex, x, 1.0 / 6.0);
+  ex = fma(ex, x, 0.5);
+  ex = fma(ex, x, 1.0);
+  ex = fma(ex, x, 1.0);
+  const double e = (T < PF_BOYS_EMAX) ? __ldg(g_boys_exp + ke) * ex : 0.0;
   const double o2t = 0.5 * rt * rt;
 #pragma unroll
   for (int m = 0; m < L; ++m) fa = ((2 * m + 1) * fa - e) * o2t;

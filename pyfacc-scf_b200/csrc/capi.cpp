@@ -101,6 +101,8 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->guess = PYFACC_GUESS_ATOMIC;
   o->incremental_thresh = 1e-11;
   o->task_width = 0;
+  o->gradient_precision = PYFACC_PRECISION_FP64;
+  o->polish = 0;
 }
 
 // scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.

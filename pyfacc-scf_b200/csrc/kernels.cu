@@ -44,23 +44,32 @@ static long double boys_series_ld(int m, long double x) {
 
 void ensure_boys_tables(int device) {
   static std::mutex mu;
-  static std::vector<double> tab;
+  static std::vector<double> tl, ex;
   static std::vector<float> tabf;
   static std::vector<int> done;
   std::lock_guard<std::mutex> lk(mu);
-  if (tab.empty()) {
-    tab.resize(PF_BOYS_NGRID * PF_BOYS_NCOL);
-    tabf.resize(tab.size());
+  if (tl.empty()) {
+    std::vector<long double> F((size_t)PF_BOYS_NGRID * PF_BOYS_NCOL);
     for (int k = 0; k < PF_BOYS_NGRID; ++k)
-      for (int m = 0; m < PF_BOYS_NCOL; ++m) {
-        long double v = boys_series_ld(m, (long double)k * 0.1L);
-        tab[k * PF_BOYS_NCOL + m] = (double)v;
-        tabf[k * PF_BOYS_NCOL + m] = (float)v;
+      for (int m = 0; m < PF_BOYS_NCOL; ++m) F[(size_t)k * PF_BOYS_NCOL + m] = boys_series_ld(m, (long double)k * 0.1L);
+    tl.resize((size_t)(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT);
+    for (int L = 0; L <= PF_BOYS_MMAX; ++L)
+      for (int k = 0; k < PF_BOYS_NGRID; ++k) {
+        long double fact = 1.0L;
+        for (int j = 0; j < PF_BOYS_NT; ++j) {
+          if (j > 0) fact *= j;
+          tl[((size_t)L * PF_BOYS_NGRID + k) * PF_BOYS_NT + j] = (double)(F[(size_t)k * PF_BOYS_NCOL + L + j] / fact);
+        }
       }
+    ex.resize(PF_BOYS_NEXP);
+    for (int k = 0; k < PF_BOYS_NEXP; ++k) ex[k] = (double)expl(-(long double)k * 0.1L);
+    tabf.resize((size_t)PF_BOYS_NGRID * PF_BOYS_NCOL);
+    for (size_t i = 0; i < tabf.size(); ++i) tabf[i] = (float)F[i];
   }
   if ((int)done.size() <= device) done.resize(device + 1, 0);
   if (!done[device]) {
-    PF_CUDA(cudaMemcpyToSymbol(g_boys_tab, tab.data(), tab.size() * sizeof(double)));
+    PF_CUDA(cudaMemcpyToSymbol(g_boys_tl, tl.data(), tl.size() * sizeof(double)));
+    PF_CUDA(cudaMemcpyToSymbol(g_boys_exp, ex.data(), ex.size() * sizeof(double)));
     PF_CUDA(cudaMemcpyToSymbol(g_boys_tabf, tabf.data(), tabf.size() * sizeof(float)));
     done[device] = 1;
   }

@@ -482,7 +482,7 @@ void System::run_scf() {
     PF_CUDA(cudaStreamSynchronize(stream));
     ms_diag += elapsed(a0, a1);
   }
-  if (mixed && st.converged) {
+  if (mixed && st.converged && opt.polish) {
     // FP64 polish: F and E of the converged density from one full FP64 build
     PF_CUDA(cudaEventRecord(a0, stream));
     double* Kp[2] = {K[0], K[1]};
@@ -583,10 +583,9 @@ void System::gradient(double* g_host) {
   unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
   PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
   g2.stats = gstats;
-  // The derivative integrals run in FP64 in both precisions: on B200 the
-  // FP32 instantiation (grad_fp32 option) measured no faster, being bound
-  // by memory latency rather than by the FP64 pipe.
-  const bool split = opt.precision == PYFACC_PRECISION_MIXED && grad_fp32;
+  // FP32 derivative integrals for the small quartets only on request
+  // (options.gradient_precision = MIXED).
+  const bool split = opt.gradient_precision == PYFACC_PRECISION_MIXED && pd.primf != nullptr;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (split) {

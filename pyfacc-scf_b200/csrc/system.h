@@ -70,7 +70,6 @@ struct System {
   double *Pu[4] = {nullptr, nullptr, nullptr, nullptr};  // purification work matrices
   double* pstate = nullptr;                      // TC2 state, two buffers of 8 (device)
   bool orbitals_ready = false;
-  bool grad_fp32 = false;  // FP32 derivative integrals for small quartets (mixed)
   int task_width = TASK_WIDTH;  // kets per J/K task
   int purify_steps = 0, purify_fallbacks = 0;
   float* dmax = nullptr;

@@ -125,6 +125,11 @@ def _options(**kw) -> N.Options:
         kw["precision"] = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED}[prec]
     elif prec is not None:
         kw["precision"] = prec
+    gp = kw.pop("gradient_precision", None)
+    if isinstance(gp, str):
+        kw["gradient_precision"] = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED}[gp]
+    elif gp is not None:
+        kw["gradient_precision"] = gp
     bm = kw.pop("boys_mode", None)
     if isinstance(bm, str):
         kw["boys_mode"] = {"accurate": N.BOYS_ACCURATE, "reference_trapezoid": N.BOYS_REFERENCE_TRAPEZOID}[bm]
