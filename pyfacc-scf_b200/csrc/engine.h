@@ -239,11 +239,19 @@ void launch_scale_columns(int n, double* U, const double* sv, cudaStream_t s);  
 void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
                  const double* C, float* dmax, cudaStream_t s);
 void launch_zero(void* p, size_t bytes, cudaStream_t s);
-// TC2 purification helpers (state: l_min, l_max, Tr X, Tr X^2, converged, steps)
+// TC2 purification one step per launch (large matrices): state = l_min,
+// l_max, Tr X, Tr X^2, converged, steps, remaining final steps.
 void launch_gersh(int n, const double* F, double* state, cudaStream_t s);
 void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s);
 void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, double* Xout, const double* sin,
                      double* sout, cudaStream_t s);
+// TC2 purification of Fp (n x n, symmetrised on entry) in one cooperative
+// launch: X <- projector on the nocc lowest eigenvectors (purify.cu).  X2
+// is n x n work space, part >= tc2_coop_scratch_doubles(num_sms) doubles,
+// bar two words; state[4] = converged, [5] = steps, [7] = barrier error.
+size_t tc2_coop_scratch_doubles(int num_sms);
+void launch_tc2_coop(int n, int nocc, const double* Fp, double* X, double* X2, double* part, unsigned* bar,
+                     double* state, int num_sms, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
 

@@ -1461,6 +1461,7 @@ void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const doub
   count_launch();
 }
 
+
 // ---------------------------------------------------------------------------
 // Trace-correcting density-matrix purification (TC2, Niklasson 2002) of the
 // orthogonalised Fock matrix: X_0 = (l_max I - F')/(l_max - l_min) with

@@ -192,39 +192,57 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   }
   double* Fp = Pu[0];
   double* Xa = Pu[1];
-  double* Xb = Pu[3];
   double* X2 = Pu[2];
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
-  double* S0 = pstate;
-  double* S1 = pstate + 8;
-  launch_gersh(nbf, Fp, S0, stream);
-  launch_tc2_init(nbf, Fp, S0, Xa, stream);
-  // check after 16 steps, then every 4 (TC2 converges quadratically once the
-  // eigenvalues approach 0 and 1; converged steps only copy X)
-  const int kmax = 200;
-  double st_h[8] = {0};
-  bool ok = false;
-  int k = 0;
-  double* cur = Xa;
-  double* nxt = Xb;
-  while (k < kmax) {
-    const int chunk = (k == 0) ? 16 : 4;
-    for (int j = 0; j < chunk; ++j, ++k) {
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, X2, nbf));
-      launch_tc2_step(nbf, (double)nocc, cur, X2, nxt, (k % 2) ? S1 : S0, (k % 2) ? S0 : S1, stream);
-      std::swap(cur, nxt);
-    }
-    PF_CUDA(cudaMemcpyAsync(st_h, (k % 2) ? S1 : S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  const double* Xp = Xa;
+  if (nbf <= 192) {
+    // small matrices: the whole TC2 iteration in one cooperative launch
+    // (purify.cu); above ~200 basis functions a cuBLAS DGEMM per step is
+    // faster than the grid-barrier-bound cooperative kernel on B200
+    const size_t npart = tc2_coop_scratch_doubles(num_sms);
+    coop_buf.ensure(npart * sizeof(double) + 256);
+    double* part = coop_buf.as<double>();
+    unsigned* bar = reinterpret_cast<unsigned*>(part + npart);
+    launch_tc2_coop(nbf, nocc, Fp, Xa, X2, part, bar, pstate, num_sms, stream);
+    double st_h[8] = {0};
+    PF_CUDA(cudaMemcpyAsync(st_h, pstate, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
-    if (st_h[4] != 0.0) {
-      ok = true;
-      break;
+    purify_steps += (int)st_h[5];
+    if (st_h[7] != 0.0 || st_h[4] == 0.0) return false;
+  } else {
+    // larger matrices: one cuBLAS DGEMM + one update kernel per step, the
+    // state double-buffered on the device; the host checks after 16 steps,
+    // then every 4 (converged steps only copy X)
+    double* S0 = pstate;
+    double* S1 = pstate + 8;
+    double* Xb = Pu[3];
+    launch_gersh(nbf, Fp, S0, stream);
+    launch_tc2_init(nbf, Fp, S0, Xa, stream);
+    const int kmax = 200;
+    double st_h[8] = {0};
+    bool ok = false;
+    int k = 0;
+    double* cur = Xa;
+    double* nxt = Xb;
+    while (k < kmax) {
+      const int chunk = (k == 0) ? 16 : 4;
+      for (int j = 0; j < chunk; ++j, ++k) {
+        PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, X2, nbf));
+        launch_tc2_step(nbf, (double)nocc, cur, X2, nxt, (k % 2) ? S1 : S0, (k % 2) ? S0 : S1, stream);
+        std::swap(cur, nxt);
+      }
+      PF_CUDA(cudaMemcpyAsync(st_h, (k % 2) ? S1 : S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      PF_CUDA(cudaStreamSynchronize(stream));
+      if (st_h[4] != 0.0) {
+        ok = true;
+        break;
+      }
     }
+    purify_steps += (int)st_h[5];
+    if (!ok) return false;
+    Xp = cur;
   }
-  purify_steps += (int)st_h[5];
-  if (!ok) return false;
-  double* Xp = cur;
   // P = scale * X Xp X^T
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));

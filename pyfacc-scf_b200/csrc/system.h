@@ -81,6 +81,7 @@ struct System {
   double* grad_dev = nullptr;
   DeviceBuf syev_work;
   DeviceBuf small_buf;
+  DeviceBuf coop_buf;   // cooperative TC2: per-block partial sums + barrier words
   int syev_lwork = 0;
 
   ScfState st;
