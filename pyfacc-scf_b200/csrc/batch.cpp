@@ -511,6 +511,7 @@ void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stat
   a.ns_ld = ns_max;
   a.thresh = thresh;
   a.stats = stats;
+  a.prim_thresh = thresh * PRIM_QUARTET_REL;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (mixed_lists) {
@@ -554,6 +555,7 @@ void Batch::tune() {
     a.ns_ld = ns_max;
     a.thresh = opt.schwarz_thresh;
     a.stats = nullptr;
+    a.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL;
     cudaEvent_t e0 = ctx.ev0, e1 = ctx.ev1;
     auto run_class = [&](int wi, int bc, int kc) {
       if (mixed) {
@@ -727,6 +729,7 @@ void Batch::gradient_run() {
   g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
   g2.ns_ld = ns_max;
   g2.thresh = opt.schwarz_thresh;
+  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
   g2.uhf = 0;
   g2.grad = grad_dev;
   g2.stats = gstats;

@@ -40,6 +40,14 @@ struct Error : std::runtime_error {
 
 constexpr int NCLASS = 3;        // ss, ps, pp
 constexpr int NQCLASS = 6;       // (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|pp)
+// primitive-quartet cut relative to the quartet screening threshold:
+// |K_ab K_cd| max|D| < PRIM_QUARTET_REL * thresh skips a primitive quartet
+// (its integral is at most ~1.5 |K_ab K_cd|, as F_m <= 1 and p + q > 0.4
+// for STO-nG exponents)
+constexpr double PRIM_QUARTET_REL = 1e-4;
+// the same for derivative integrals, which carry factors 2 alpha (<= ~200
+// for STO-nG exponents)
+constexpr double PRIM_QUARTET_REL_GRAD = 1e-6;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis
@@ -165,6 +173,9 @@ struct JkArgs {
   int ns_ld;             // leading dimension of dmax
   double thresh;         // density-weighted Schwarz threshold
   unsigned long long* stats;  // JkStats layout (device) or null
+  // primitive quartets with |K_ab K_cd| max|D| below this are skipped (the
+  // primitive pairs of a shell pair are sorted by |K|); 0 = none
+  double prim_thresh = 0.0;
 };
 void launch_jk(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, int nk,
                const JkArgs& a, int num_sms, cudaStream_t s);
@@ -192,6 +203,7 @@ struct GradArgs {
   int uhf;
   double* grad;  // natoms*3 (packed over a batch via the pair's atom index)
   unsigned long long* stats;  // [0..5] quartets, [6..11] primitive quartets per class, or null
+  double prim_thresh = 0.0;   // as JkArgs::prim_thresh
 };
 void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, const GradArgs& a,
                    int num_sms, cudaStream_t s);

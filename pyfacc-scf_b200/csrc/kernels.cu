@@ -218,32 +218,41 @@ template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
 
 // Contracted (ab|cd) for one bra pair and one ket pair (records of the
 // kernel's precision: double4 for FP64 quartets, float4 for FP32 ones).
+// Primitive pairs are stored in order of decreasing |K|, so with kcut > 0
+// both loops stop at the first primitive quartet with |K_ab K_cd| < kcut.
 template <typename R, int LA, int LB, int LC, int LD>
-__device__ __forceinline__ void contracted_quartet(const typename Rec<R>::T* __restrict__ prim, int4 bi0, int4 ki0,
-                                                   const double4& bgeo, const double4& kgeo,
-                                                   R out[EriClass<R, LA, LB, LC, LD>::NOUT]) {
+__device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __restrict__ prim, int4 bi0, int4 ki0,
+                                                  const double4& bgeo, const double4& kgeo,
+                                                  R out[EriClass<R, LA, LB, LC, LD>::NOUT], double kcut = 0.0) {
   using C = EriClass<R, LA, LB, LC, LD>;
   using V = typename Rec<R>::T;
   R acc[C::NACC];
 #pragma unroll
   for (int i = 0; i < C::NACC; ++i) acc[i] = (R)0;
+  const double kab_max = fabs((double)prim[3 * (size_t)bi0.z].z);
+  int nprim = 0;
   for (int kq = 0; kq < ki0.w; ++kq) {
     const V* kr = prim + 3 * (size_t)(ki0.z + kq);
     const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const double kcd = fabs((double)k0.z);
+    if (kab_max * kcd < kcut) break;
     const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
 #pragma unroll 1
     for (int kp = 0; kp < bi0.w; ++kp) {
       const V* br = prim + 3 * (size_t)(bi0.z + kp);
       const V b0 = br[0], b1 = br[1], b2 = br[2];
+      if (fabs((double)b0.z) * kcd < kcut) break;
       const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
       PrimGeo<R> g;
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
       C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.rp, g.o2q, g.rq, g.o2pq, acc);
+      ++nprim;
     }
   }
   const R AB[3] = {(R)bgeo.x, (R)bgeo.y, (R)bgeo.z};
   const R CD[3] = {(R)kgeo.x, (R)kgeo.y, (R)kgeo.z};
   C::hrr(acc, AB, CD, out);
+  return nprim;
 }
 
 // Schwarz factor of every pair of one class: Q = sqrt(max |(ab|ab)|).
@@ -294,8 +303,32 @@ __global__ void gather_pairs_kernel(int npair, const int* __restrict__ perm, con
   int4 a = i0[j];
   const int old_ps = a.z, old_np = a.w;
   a.z = new_ps[i];
+  // kept primitive pairs in order of decreasing |K| (so that a loop over
+  // them can stop at a cut); pairs with more than 64 primitive pairs keep
+  // the input order
+  int order[64];
   int nk = 0;
-  for (int k = 0; k < old_np; ++k) {
+  for (int k = 0; k < old_np; ++k)
+    if (fabs(pr[3 * (size_t)(old_ps + k)].z) >= cut) {
+      if (old_np <= 64) order[nk] = k;
+      ++nk;
+    }
+  if (old_np <= 64) {
+    for (int x = 1; x < nk; ++x) {
+      const int v = order[x];
+      const double kv = fabs(pr[3 * (size_t)(old_ps + v)].z);
+      int y = x - 1;
+      while (y >= 0 && fabs(pr[3 * (size_t)(old_ps + order[y])].z) < kv) {
+        order[y + 1] = order[y];
+        --y;
+      }
+      order[y + 1] = v;
+    }
+  }
+  const int nkept = nk;
+  nk = 0;
+  for (int kk = 0; kk < (old_np <= 64 ? nkept : old_np); ++kk) {
+    const int k = (old_np <= 64) ? order[kk] : kk;
     const double4* src = pr + 3 * (size_t)(old_ps + k);
     const double4 r0 = src[0];
     if (fabs(r0.z) < cut) continue;
@@ -412,32 +445,35 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     const double4 bg = args.geom[bp];
     int4 ki0 = bi0, ki1 = bi1;
     double4 kg = bg;
+    double kcut = 0.0;
     if (active) {
       ki0 = args.info0[kp];
       ki1 = args.info1[kp];
       kg = args.geom[kp];
       if (A.dmax) {
-        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
-        active = bound >= (float)A.thresh;
+        const float dm = dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        active = (float)(bg.w * kg.w) * dm >= (float)A.thresh;
+        if (A.prim_thresh > 0.0) kcut = A.prim_thresh / fmax((double)dm, 1e-300);
       }
     }
     const unsigned amask = __ballot_sync(0xffffffffu, active);
     if (amask == 0u) continue;
-    if (A.stats) {
-      unsigned long long tot = active ? (unsigned long long)(bi0.w * ki0.w) : 0ull;
+    R out[C::NOUT];
+    int nprim = 0;
+    if (active) {
+      nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut);
+    } else {
+#pragma unroll
+      for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
+    }
+    if (A.stats) {  // contracted and evaluated primitive quartets
+      unsigned long long tot = (unsigned long long)nprim;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
       if (lane == 0) {
         atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
         atomicAdd(A.stats + (2 + args.prec) * NQCLASS + args.qclass, tot);
       }
-    }
-    R out[C::NOUT];
-    if (active) {
-      contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out);
-    } else {
-#pragma unroll
-      for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
     }
     // degeneracy factor of the canonical quartet
     double fac = active ? 1.0 : 0.0;
@@ -784,27 +820,20 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
     const double4 bg = args.geom[bp];
     int4 ki0 = bi0, ki1 = bi1;
     double4 kg = bg;
+    double kcut = 0.0;
     if (active) {
       ki0 = args.info0[kp];
       ki1 = args.info1[kp];
       kg = args.geom[kp];
       if (A.dmax) {
-        float bound = (float)(bg.w * kg.w) * dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
-        active = bound >= (float)A.thresh;
+        const float dm = dmax_bound(A.dmax + bi2.w, A.ns_ld, bi1.x, bi1.y, ki1.x, ki1.y);
+        active = (float)(bg.w * kg.w) * dm >= (float)A.thresh;
+        if (A.prim_thresh > 0.0) kcut = A.prim_thresh / fmax((double)dm, 1e-300);
       }
     }
     const unsigned amask = __ballot_sync(0xffffffffu, active);
     if (amask == 0u) continue;
-    if (A.stats) {
-      const unsigned long long np = active ? (unsigned long long)(bi0.w * ki0.w) : 0ull;
-      unsigned long long tot = np;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-      if (lane == 0) {
-        atomicAdd(A.stats + args.qclass, (unsigned long long)__popc(amask));
-        atomicAdd(A.stats + NQCLASS + args.qclass, tot);
-      }
-    }
+    int nprim = 0;
     double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (active) {
       const size_t mo = (size_t)bi2.x;
@@ -839,13 +868,18 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const R CD[3] = {(R)kg.x, (R)kg.y, (R)kg.z};
       R gr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       const V* prim = grecords<R>(args);
+      const double kab_max = fabs((double)prim[3 * (size_t)bi0.z].z);
       for (int kq = 0; kq < ki0.w; ++kq) {
         const V* kr = prim + 3 * (size_t)(ki0.z + kq);
         const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+        const double kcd = fabs((double)k0.z);
+        if (kab_max * kcd < kcut) break;
         const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
         for (int kpp = 0; kpp < bi0.w; ++kpp) {
           const V* br = prim + 3 * (size_t)(bi0.z + kpp);
           const V b0 = br[0], b1 = br[1], b2 = br[2];
+          if (fabs((double)b0.z) * kcd < kcut) break;
+          ++nprim;
           const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
           PrimGeo<R> pg;
           prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
@@ -863,6 +897,15 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       if (args.same_class && bp == kp) fac *= 0.5;
 #pragma unroll
       for (int i = 0; i < 9; ++i) g[i] = fac * (double)gr[i];
+    }
+    if (A.stats) {  // contracted and evaluated primitive quartets
+      unsigned long long tot = (unsigned long long)nprim;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+      if (lane == 0) {
+        atomicAdd(A.stats + args.qclass, (unsigned long long)__popc(amask));
+        atomicAdd(A.stats + NQCLASS + args.qclass, tot);
+      }
     }
     // centre A and B are the bra's, uniform across a task's lanes
     double* G = A.grad;

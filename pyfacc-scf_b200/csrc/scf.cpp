@@ -68,6 +68,7 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   a.ns_ld = ns;
   a.thresh = thresh;
   a.stats = stats_dev;
+  a.prim_thresh = thresh * PRIM_QUARTET_REL;
   const bool mixed = precision == PYFACC_PRECISION_MIXED;
   if (opt.shard_count > 1) dynamic = false;  // shards use their static sub-lists
   if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? opt.fp32_thresh : 0.0, dyn, stream);
@@ -596,6 +597,7 @@ void System::gradient(double* g_host) {
   g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
   g2.ns_ld = ns;
   g2.thresh = opt.schwarz_thresh;
+  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
   g2.uhf = uhf ? 1 : 0;
   g2.grad = grad_dev;
   unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
