@@ -114,6 +114,7 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
 System::~System() {
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
+  for (auto& g : tc2_graphs) cudaGraphExecDestroy(g.second);
   release_extra();
   context_release(ctx);  // stream and handles go back to the per-device pool
 }

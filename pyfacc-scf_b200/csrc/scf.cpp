@@ -213,33 +213,30 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
     if (st_h[7] != 0.0 || st_h[4] == 0.0) return false;
   } else {
     // larger matrices: one cuBLAS DGEMM + one update kernel per step, the
-    // state double-buffered on the device; the host checks after 16 steps,
-    // then every 4 (converged steps only copy X)
+    // state double-buffered on the device, four steps per graph replay; the
+    // host checks after 16 steps, then every 4 (converged steps only copy X)
     double* S0 = pstate;
-    double* S1 = pstate + 8;
-    double* Xb = Pu[3];
     launch_gersh(nbf, Fp, S0, stream);
     launch_tc2_init(nbf, Fp, S0, Xa, stream);
+    cudaGraphExec_t g4 = tc2_graph(nocc);
     const int kmax = 200;
     double st_h[8] = {0};
     bool ok = false;
     int k = 0;
-    double* cur = Xa;
-    double* nxt = Xb;
     while (k < kmax) {
       const int chunk = (k == 0) ? 16 : 4;
-      for (int j = 0; j < chunk; ++j, ++k) {
-        PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, X2, nbf));
-        launch_tc2_step(nbf, (double)nocc, cur, X2, nxt, (k % 2) ? S1 : S0, (k % 2) ? S0 : S1, stream);
-        std::swap(cur, nxt);
+      for (int j = 0; j < chunk; j += 4, k += 4) {
+        PF_CUDA(cudaGraphLaunch(g4, stream));
+        count_launches(4);
       }
-      PF_CUDA(cudaMemcpyAsync(st_h, (k % 2) ? S1 : S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      PF_CUDA(cudaMemcpyAsync(st_h, S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
       PF_CUDA(cudaStreamSynchronize(stream));
       if (st_h[4] != 0.0) {
         ok = true;
         break;
       }
     }
+    double* cur = Xa;
     purify_steps += (int)st_h[5];
     if (!ok) return false;
     Xp = cur;
@@ -248,6 +245,39 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));
   return true;
+}
+
+// Four TC2 steps X_a -> X_b -> X_a -> X_b -> X_a (state S0 -> S1 -> S0 ...),
+// captured once per occupation number: after four steps the iterate and the
+// state are back in X_a and S0, so the graph can be replayed.
+cudaGraphExec_t System::tc2_graph(int nocc) {
+  for (auto& g : tc2_graphs)
+    if (g.first == nocc) return g.second;
+  const double one = 1.0, zero = 0.0;
+  double* bufs[2] = {Pu[1], Pu[3]};
+  double* st[2] = {pstate, pstate + 8};
+  cudaGraph_t graph = nullptr;
+  PF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (int k = 0; k < 4; ++k) {
+      double* cur = bufs[k % 2];
+      double* nxt = bufs[(k + 1) % 2];
+      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, Pu[2],
+                            nbf));
+      launch_tc2_step(nbf, (double)nocc, cur, Pu[2], nxt, st[k % 2], st[(k + 1) % 2], stream);
+    }
+  } catch (...) {
+    cudaStreamEndCapture(stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  PF_CUDA(cudaStreamEndCapture(stream, &graph));
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (rc != cudaSuccess) throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
+  tc2_graphs.emplace_back(nocc, exec);
+  return exec;
 }
 
 // New density from a Fock matrix: purification, or eigenvectors when the
