@@ -257,13 +257,6 @@ void launch_gersh(int n, const double* F, double* state, cudaStream_t s);
 void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s);
 void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, double* Xout, const double* sin,
                      double* sout, cudaStream_t s);
-// TC2 purification of Fp (n x n, symmetrised on entry) in one cooperative
-// launch: X <- projector on the nocc lowest eigenvectors (purify.cu).  X2
-// is n x n work space, part >= tc2_coop_scratch_doubles(num_sms) doubles,
-// bar two words; state[4] = converged, [5] = steps, [7] = barrier error.
-size_t tc2_coop_scratch_doubles(int num_sms);
-void launch_tc2_coop(int n, int nocc, const double* Fp, double* X, double* X2, double* part, unsigned* bar,
-                     double* state, int num_sms, cudaStream_t s);
 
 double probe_fp64(int device, double* fp32);
 

@@ -193,54 +193,35 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   }
   double* Fp = Pu[0];
   double* Xa = Pu[1];
-  double* X2 = Pu[2];
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
-  const double* Xp = Xa;
-  if (nbf <= 192) {
-    // small matrices: the whole TC2 iteration in one cooperative launch
-    // (purify.cu); above ~200 basis functions a cuBLAS DGEMM per step is
-    // faster than the grid-barrier-bound cooperative kernel on B200
-    const size_t npart = tc2_coop_scratch_doubles(num_sms);
-    coop_buf.ensure(npart * sizeof(double) + 256);
-    double* part = coop_buf.as<double>();
-    unsigned* bar = reinterpret_cast<unsigned*>(part + npart);
-    launch_tc2_coop(nbf, nocc, Fp, Xa, X2, part, bar, pstate, num_sms, stream);
-    double st_h[8] = {0};
-    PF_CUDA(cudaMemcpyAsync(st_h, pstate, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PF_CUDA(cudaStreamSynchronize(stream));
-    purify_steps += (int)st_h[5];
-    if (st_h[7] != 0.0 || st_h[4] == 0.0) return false;
-  } else {
-    // larger matrices: one cuBLAS DGEMM + one update kernel per step, the
-    // state double-buffered on the device, four steps per graph replay; the
-    // host checks after 16 steps, then every 4 (converged steps only copy X)
-    double* S0 = pstate;
-    launch_gersh(nbf, Fp, S0, stream);
-    launch_tc2_init(nbf, Fp, S0, Xa, stream);
-    cudaGraphExec_t g4 = tc2_graph(nocc);
-    const int kmax = 200;
-    double st_h[8] = {0};
-    bool ok = false;
-    int k = 0;
-    while (k < kmax) {
-      const int chunk = (k == 0) ? 16 : 4;
-      for (int j = 0; j < chunk; j += 4, k += 4) {
-        PF_CUDA(cudaGraphLaunch(g4, stream));
-        count_launches(4);
-      }
-      PF_CUDA(cudaMemcpyAsync(st_h, S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-      PF_CUDA(cudaStreamSynchronize(stream));
-      if (st_h[4] != 0.0) {
-        ok = true;
-        break;
-      }
+  // one cuBLAS DGEMM + one update kernel per step, the state double-buffered
+  // on the device, four steps per graph replay; the host checks after 16
+  // steps, then every 4 (converged steps only copy X)
+  double* S0 = pstate;
+  launch_gersh(nbf, Fp, S0, stream);
+  launch_tc2_init(nbf, Fp, S0, Xa, stream);
+  cudaGraphExec_t g4 = tc2_graph(nocc);
+  const int kmax = 200;
+  double st_h[8] = {0};
+  bool ok = false;
+  int k = 0;
+  while (k < kmax) {
+    const int chunk = (k == 0) ? 16 : 4;
+    for (int j = 0; j < chunk; j += 4, k += 4) {
+      PF_CUDA(cudaGraphLaunch(g4, stream));
+      count_launches(4);
     }
-    double* cur = Xa;
-    purify_steps += (int)st_h[5];
-    if (!ok) return false;
-    Xp = cur;
+    PF_CUDA(cudaMemcpyAsync(st_h, S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    if (st_h[4] != 0.0) {
+      ok = true;
+      break;
+    }
   }
+  purify_steps += (int)st_h[5];
+  if (!ok) return false;
+  const double* Xp = Xa;  // after a multiple of four steps the iterate is back in Xa
   // P = scale * X Xp X^T
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));
@@ -249,7 +230,9 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
 
 // Four TC2 steps X_a -> X_b -> X_a -> X_b -> X_a (state S0 -> S1 -> S0 ...),
 // captured once per occupation number: after four steps the iterate and the
-// state are back in X_a and S0, so the graph can be replayed.
+// state are back in X_a and S0, so the graph can be replayed.  (A single
+// cooperative launch for the whole iteration, grid barriers between steps,
+// measured slower than these replays at every size tried on B200.)
 cudaGraphExec_t System::tc2_graph(int nocc) {
   for (auto& g : tc2_graphs)
     if (g.first == nocc) return g.second;

@@ -81,7 +81,6 @@ struct System {
   double* grad_dev = nullptr;
   DeviceBuf syev_work;
   DeviceBuf small_buf;
-  DeviceBuf coop_buf;   // cooperative TC2: per-block partial sums + barrier words
   // four TC2 steps (cuBLAS DGEMM + update, ping-pong buffers) as one CUDA
   // graph per occupation number, replayed by purify() for nbf > 192
   std::vector<std::pair<int, cudaGraphExec_t>> tc2_graphs;
