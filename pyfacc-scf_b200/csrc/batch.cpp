@@ -730,6 +730,7 @@ void Batch::gradient_run() {
   g2.ns_ld = ns_max;
   g2.thresh = opt.schwarz_thresh;
   g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
+  g2.natoms_total = natoms_tot;
   g2.uhf = 0;
   g2.grad = grad_dev;
   g2.stats = gstats;

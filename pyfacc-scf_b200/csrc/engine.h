@@ -204,6 +204,7 @@ struct GradArgs {
   double* grad;  // natoms*3 (packed over a batch via the pair's atom index)
   unsigned long long* stats;  // [0..5] quartets, [6..11] primitive quartets per class, or null
   double prim_thresh = 0.0;   // as JkArgs::prim_thresh
+  int natoms_total = 0;       // length of grad / 3; per-block shared-memory sums when small
 };
 void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, bool fp32, const GradArgs& a,
                    int num_sms, cudaStream_t s);

@@ -792,6 +792,7 @@ struct GradKernelArgs {
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, task_begin;
   int lwidth;
+  int smem_atoms;  // atoms summed in shared memory (0: global atomics)
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
@@ -807,6 +808,13 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   const int nw = (gridDim.x * blockDim.x) >> 5;
   const GradArgs& A = args.a;
   const int lw = args.lwidth, W = 1 << lw, sub = lane & (W - 1), tpw = 32 >> lw;
+  // per-atom sums of the block in shared memory (one global add per atom
+  // and block at the end) when the gradient is small enough
+  extern __shared__ double gsh[];
+  const int nsm = args.smem_atoms * 3;
+  for (int i = threadIdx.x; i < nsm; i += blockDim.x) gsh[i] = 0.0;
+  if (nsm) __syncthreads();
+  double* G = nsm ? gsh : A.grad;
   for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < args.ntasks; tb += nw * tpw) {
     const int tl = tb + (lane >> lw);
     const bool valid = tl < args.ntasks;
@@ -908,7 +916,6 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       }
     }
     // centre A and B are the bra's, uniform across a task's lanes
-    double* G = A.grad;
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
       const double sa = group_sum(g[x], W);
@@ -926,17 +933,30 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       }
     }
   }
+  if (nsm) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsm; i += blockDim.x)
+      if (gsh[i] != 0.0) atomicAdd(A.grad + i, gsh[i]);
+  }
+}
+
+template <typename R, int LA, int LB, int LC, int LD>
+static void grad2e_launch(dim3 grid, dim3 block, size_t smem, cudaStream_t s, const GradKernelArgs& k) {
+  if (smem > 48 * 1024)
+    PF_CUDA(cudaFuncSetAttribute(grad2e_kernel<R, LA, LB, LC, LD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+  grad2e_kernel<R, LA, LB, LC, LD><<<grid, block, smem, s>>>(k);
 }
 
 template <typename R>
-static void grad2e_dispatch(int qc, dim3 grid, dim3 block, cudaStream_t s, const GradKernelArgs& k) {
+static void grad2e_dispatch(int qc, dim3 grid, dim3 block, size_t smem, cudaStream_t s, const GradKernelArgs& k) {
   switch (qc) {
-    case 0: grad2e_kernel<R, 0, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 1: grad2e_kernel<R, 1, 0, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 2: grad2e_kernel<R, 1, 0, 1, 0><<<grid, block, 0, s>>>(k); break;
-    case 3: grad2e_kernel<R, 1, 1, 0, 0><<<grid, block, 0, s>>>(k); break;
-    case 4: grad2e_kernel<R, 1, 1, 1, 0><<<grid, block, 0, s>>>(k); break;
-    default: grad2e_kernel<R, 1, 1, 1, 1><<<grid, block, 0, s>>>(k); break;
+    case 0: grad2e_launch<R, 0, 0, 0, 0>(grid, block, smem, s, k); break;
+    case 1: grad2e_launch<R, 1, 0, 0, 0>(grid, block, smem, s, k); break;
+    case 2: grad2e_launch<R, 1, 0, 1, 0>(grid, block, smem, s, k); break;
+    case 3: grad2e_launch<R, 1, 1, 0, 0>(grid, block, smem, s, k); break;
+    case 4: grad2e_launch<R, 1, 1, 1, 0>(grid, block, smem, s, k); break;
+    default: grad2e_launch<R, 1, 1, 1, 1>(grid, block, smem, s, k); break;
   }
 }
 
@@ -954,9 +974,13 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   k.same_class = (bc == kc);
   k.qclass = qclass_of(bc, kc);
   k.lwidth = width_log2(tl.width);
+  // up to 256 atoms (6 KB of per-block sums; above that the end-of-block
+  // flush costs more than the contention it saves)
+  k.smem_atoms = (a.natoms_total > 0 && a.natoms_total <= 256) ? a.natoms_total : 0;
+  const size_t smem = 3 * (size_t)k.smem_atoms * sizeof(double);
   dim3 grid(grid_for((tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width), num_sms)), block(128);
-  if (fp32) grad2e_dispatch<float>(k.qclass, grid, block, s, k);
-  else grad2e_dispatch<double>(k.qclass, grid, block, s, k);
+  if (fp32) grad2e_dispatch<float>(k.qclass, grid, block, smem, s, k);
+  else grad2e_dispatch<double>(k.qclass, grid, block, smem, s, k);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }

@@ -611,6 +611,7 @@ void System::gradient(double* g_host) {
   g2.ns_ld = ns;
   g2.thresh = opt.schwarz_thresh;
   g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
+  g2.natoms_total = natoms;
   g2.uhf = uhf ? 1 : 0;
   g2.grad = grad_dev;
   unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
