@@ -240,7 +240,8 @@ void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pair
                    int num_sms, cudaStream_t s);
 
 // Small dense helpers.
-void launch_symmetrize_add(int n, double* A, cudaStream_t s);             // A = A + A^T
+void launch_symmetrize_add(int n, double* A, cudaStream_t s);
+void launch_identity(int n, double* A, cudaStream_t s);                  // A = I (n x n)             // A = A + A^T
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
                  cudaStream_t s);                                          // F = H + J - kf K
@@ -248,7 +249,6 @@ void launch_dot_many(long long n, const double* x, int m, const double* const* y
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb,
                        const double* Fa, const double* Fb, const double* Ea, const double* Eb,
                        const double* Pa_old, const double* Pb_old, double* out, cudaStream_t s);
-void launch_scale_columns(int n, double* U, const double* sv, cudaStream_t s);  // U[:,j] /= sqrt(s_j)
 void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
                  const double* C, float* dmax, cudaStream_t s);
 void launch_zero(void* p, size_t bytes, cudaStream_t s);

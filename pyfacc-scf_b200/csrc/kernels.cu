@@ -1383,6 +1383,18 @@ __global__ void symmetrize_add_kernel(int n, double* A) {
   A[(size_t)i * n + j] = s;
   A[(size_t)j * n + i] = s;
 }
+__global__ void identity_kernel(long long n2, int n, double* A) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += (long long)gridDim.x * blockDim.x)
+    A[k] = (k % (n + 1) == 0) ? 1.0 : 0.0;
+}
+void launch_identity(int n, double* A, cudaStream_t s) {
+  const long long n2 = (long long)n * n;
+  const int g = (int)std::min<long long>((n2 + 255) / 256, 2048);
+  identity_kernel<<<std::max(g, 1), 256, 0, s>>>(n2, n, A);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
 void launch_symmetrize_add(int n, double* A, cudaStream_t s) {
   dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
   symmetrize_add_kernel<<<g, b, 0, s>>>(n, A);
@@ -1492,17 +1504,6 @@ void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, 
   count_launch();
 }
 
-__global__ void scale_columns_kernel(int n, double* U, const double* s) {
-  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || j >= n) return;
-  U[(size_t)j * n + i] *= rsqrt(s[j]);  // column-major: column j
-}
-void launch_scale_columns(int n, double* U, const double* s, cudaStream_t st) {
-  dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
-  scale_columns_kernel<<<g, b, 0, st>>>(n, U, s);
-  PF_CUDA(cudaGetLastError());
-  count_launch();
-}
 
 // dmax[a][b] = max |A|, |B| over the (a, b) shell block.
 __global__ void dmax_kernel(int ns, const int* __restrict__ bf_off, const int* __restrict__ nfun, int nbf,

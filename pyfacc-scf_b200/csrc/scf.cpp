@@ -110,21 +110,29 @@ void System::eri_tensor(double* eri) {
 
 // X = U s^-1/2 from S (la.f90:28-57).  cuSOLVER works column-major; S is
 // symmetric, and U comes back with eigenvector j in column j.
+// X with X^T S X = I from the Cholesky factor S = L L^T: X = L^{-T}
+// (cuSOLVER potrf + cuBLAS trsm).  Any S-orthonormalising X gives the same
+// density, energy and orbital energies; la.f90:7-57 uses U s^{-1/2}, which
+// costs a full eigendecomposition.  A non-positive-definite S is reported
+// as PYFACC_ERR_LINDEP, as before.
 void System::orthogonalizer() {
   const size_t n2 = (size_t)nbf * nbf;
-  PF_CUDA(cudaMemcpyAsync(X, S, n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-  PF_CUSOLVER(cusolverDnDsyevd(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, X, nbf, eps_dev,
-                               syev_work.as<double>(), syev_lwork, info_dev));
-  std::vector<double> s(nbf);
+  double* L = W3;
+  PF_CUDA(cudaMemcpyAsync(L, S, n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  int lwork = 0;
+  PF_CUSOLVER(cusolverDnDpotrf_bufferSize(cusolver, CUBLAS_FILL_MODE_LOWER, nbf, L, nbf, &lwork));
+  if ((size_t)lwork * sizeof(double) > syev_work.bytes) syev_work.ensure((size_t)lwork * sizeof(double));
+  PF_CUSOLVER(cusolverDnDpotrf(cusolver, CUBLAS_FILL_MODE_LOWER, nbf, L, nbf, syev_work.as<double>(), lwork,
+                               info_dev));
   int info = 0;
-  PF_CUDA(cudaMemcpyAsync(s.data(), eps_dev, nbf * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaMemcpyAsync(&info, info_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
-  if (info != 0) throw Error(PYFACC_ERR_CUDA, "overlap diagonalisation failed");
-  if (!(s[0] > 0.0)) throw Error(PYFACC_ERR_LINDEP, "overlap matrix is not positive definite");
-  if (s[0] < 1.0e-8 && opt.verbose)
-    std::fprintf(stderr, "pyfacc: small overlap eigenvalue %g\n", s[0]);  // la.f90:40-44
-  launch_scale_columns(nbf, X, eps_dev, stream);
+  if (info > 0) throw Error(PYFACC_ERR_LINDEP, "overlap matrix is not positive definite");
+  if (info < 0) throw Error(PYFACC_ERR_CUDA, "overlap factorisation failed");
+  launch_identity(nbf, X, stream);
+  const double one = 1.0;
+  PF_CUBLAS(cublasDtrsm(cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nbf, nbf,
+                        &one, L, nbf, X, nbf));
 }
 
 // F' = X^T F X, eigenpairs, C = X C' (all column-major).
@@ -333,7 +341,11 @@ void System::run_scf() {
   PF_CUDA(cudaEventRecord(a1, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   st.ms_1e = elapsed(a0, a1);
+  PF_CUDA(cudaEventRecord(a0, stream));
   orthogonalizer();
+  PF_CUDA(cudaEventRecord(a1, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  const float ms_orth = elapsed(a0, a1);
   orbitals_ready = false;
   purify_steps = purify_fallbacks = 0;
   if (opt.guess == PYFACC_GUESS_CORE) {
@@ -542,6 +554,10 @@ void System::run_scf() {
   st.ms_total = elapsed(t0, t1);
   st.ms_fock = ms_fock;
   st.ms_diag = ms_diag;
+  if (opt.verbose)
+    std::fprintf(stderr, "pyfacc phases (ms): total %.3f  one-electron %.3f  orthogonaliser %.3f  Fock %.3f  "
+                 "density %.3f  rest (DIIS, energy, guess) %.3f\n", st.ms_total, st.ms_1e, ms_orth, ms_fock, ms_diag,
+                 st.ms_total - st.ms_1e - ms_orth - ms_fock - ms_diag);
   JkStats js;
   PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
   st.quartets[0] = st.quartets[1] = 0;
