@@ -7,6 +7,7 @@
 #include <array>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -103,11 +104,18 @@ Batch::Batch(const std::vector<BatchMolHost>& ms, const pyfacc_options& o) : opt
   mtot = mo;
   if (mtot >= (1LL << 31) || (long long)nmol * ns_max * ns_max >= (1LL << 31))
     throw Error(PYFACC_ERR_INVALID, "batch too large: split it into several calls");
+  const double t1 = wall_ms();
   upload();
+  const double t2 = wall_ms();
   build_pairs();
+  const double t3 = wall_ms();
   build_tasks();
+  const double t4 = wall_ms();
   alloc();
   timing.ms_setup = wall_ms() - t0;
+  if (opt.verbose)
+    std::fprintf(stderr, "pyfacc batch setup (ms): context %.2f  shells %.2f  pairs %.2f  tasks %.2f  matrices %.2f\n",
+                 t1 - t0, t2 - t1, t3 - t2, t4 - t3, wall_ms() - t4);
 }
 
 Batch::~Batch() {
@@ -115,7 +123,6 @@ Batch::~Batch() {
   if (stream) cudaStreamSynchronize(stream);
   if (graph_full) cudaGraphExecDestroy(graph_full);
   if (graph_inc) cudaGraphExecDestroy(graph_inc);
-  if (active_host) cudaFreeHost(active_host);
   context_release(ctx);
 }
 
@@ -289,13 +296,17 @@ void Batch::build_pairs() {
   pd.cls_host.clear();
   pd.mol_host.clear();
   for (int c = 0; c < NCLASS; ++c) {
+    // the pairs of a class are generated molecule by molecule: sort each
+    // molecule's segment by Q (descending; ties by index, deterministic)
     std::vector<int> idx;
     for (int k = off[c]; k < off[c + 1]; ++k)
       if (thr <= 0 || q[k] * qmax[allm[k]] >= thr) idx.push_back(k);
-    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
-      if (allm[x] != allm[y]) return allm[x] < allm[y];
-      return q[x] > q[y];
-    });
+    for (size_t a = 0; a < idx.size();) {
+      size_t b = a;
+      while (b < idx.size() && allm[idx[b]] == allm[idx[a]]) ++b;
+      std::sort(idx.begin() + a, idx.begin() + b, [&](int x, int y) { return q[x] > q[y] || (q[x] == q[y] && x < y); });
+      a = b;
+    }
     seg[c].assign(nmol + 1, 0);
     for (int k : idx) {
       perm.push_back(k);
@@ -340,6 +351,17 @@ void Batch::build_pairs() {
 void Batch::build_tasks() {
   const double thr = std::max(opt.schwarz_thresh, 0.0);
   const double t32 = opt.fp32_thresh;
+  // which task widths are needed per class: all three for the tuner, else
+  // the fixed width or the cached tuner result
+  std::array<int, NQCLASS> fixed{};
+  bool have = false;
+  if (opt.task_width) {
+    fixed.fill(opt.task_width);
+    have = true;
+  } else {
+    have = tuned_widths(&fixed);
+  }
+  auto wanted = [&](int q, int wi) { return !have || fixed[q] == kWidths[wi]; };
   struct Pending { int bc, kc, prec; size_t lo_off, toff_off[3]; int nbra; };
   std::vector<Pending> pend;
   std::vector<int> hostbuf;
@@ -382,6 +404,10 @@ void Batch::build_tasks() {
         hostbuf.insert(hostbuf.end(), hi.begin(), hi.end());
         for (int wi = 0; wi < 3; ++wi) {
           const int w = kWidths[wi];
+          if (!wanted(qclass_index(bc, kc), wi)) {
+            p.toff_off[wi] = (size_t)-1;
+            continue;
+          }
           p.toff_off[wi] = hostbuf.size();
           int ntask = 0;
           for (int i = 0; i < nb; ++i) {
@@ -403,18 +429,19 @@ void Batch::build_tasks() {
   PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
   for (auto& p : pend)
     for (int wi = 0; wi < 3; ++wi) {
+      if (p.toff_off[wi] == (size_t)-1) continue;
       TaskList& tl = tasks_w[wi][p.bc][p.kc][p.prec];
       tl.ket_lo = d + p.lo_off;
       tl.ket_hi = d + p.lo_off + p.nbra;
       tl.task_off = d + p.toff_off[wi];
     }
-  int wi0 = 0;
-  if (opt.task_width == 16) wi0 = 1;
-  if (opt.task_width == 8) wi0 = 2;
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
-      for (int p = 0; p < 3; ++p) tasks[bc][kc][p] = tasks_w[wi0][bc][kc][p];
-      timing.width[qclass_index(bc, kc)] = kWidths[wi0];
+      const int q = qclass_index(bc, kc);
+      const int w = have ? fixed[q] : 32;
+      const int wi = w == 32 ? 0 : (w == 16 ? 1 : 2);
+      for (int p = 0; p < 3; ++p) tasks[bc][kc][p] = tasks_w[wi][bc][kc][p];
+      timing.width[q] = w;
     }
   PF_CUDA(cudaStreamSynchronize(stream));
 }
@@ -494,7 +521,6 @@ void Batch::alloc() {
   a.active = active_dev;
   a.smem_nmax = nbf_max;  // nbf <= 160: at most 200 KB of shared memory
   batch_set_smem(a);
-  PF_CUDA(cudaMallocHost(&active_host, sizeof(int)));
   PF_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -527,23 +553,29 @@ void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stat
 // and 8 kets on the first (full) build of this batch, and the fastest width
 // is kept per class.  Results are cached per batch shape (precision and the
 // molecules' sizes), so repeated batches of the same shape skip the timing.
-void Batch::tune() {
-  static std::mutex mu;
-  static std::map<std::string, std::array<int, NQCLASS>> cache;
-  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+static std::mutex g_tune_mu;
+static std::map<std::string, std::array<int, NQCLASS>> g_tune_cache;
+
+std::string Batch::tune_key() const {
   std::ostringstream key;
-  key << device << ':' << (mixed ? 'm' : 'd') << ':' << opt.schwarz_thresh << ':' << opt.fp32_thresh;
+  key << device << ':' << (opt.precision == PYFACC_PRECISION_MIXED ? 'm' : 'd') << ':' << opt.schwarz_thresh << ':'
+      << opt.fp32_thresh;
   for (const auto& m : mols) key << ',' << m.nbf << '/' << m.natoms;
+  return key.str();
+}
+
+bool Batch::tuned_widths(std::array<int, NQCLASS>* w) const {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune_cache.find(tune_key());
+  if (it == g_tune_cache.end()) return false;
+  *w = it->second;
+  return true;
+}
+
+void Batch::tune() {
+  const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
   std::array<int, NQCLASS> best{};
-  bool have = false;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(key.str());
-    if (it != cache.end()) {
-      best = it->second;
-      have = true;
-    }
-  }
+  const bool have = tuned_widths(&best);
   if (!have) {
     const double t0 = wall_ms();
     launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.Db, dmax, stream);
@@ -589,8 +621,8 @@ void Batch::tune() {
     launch_zero(dargs.Kd, (size_t)mtot * sizeof(double), stream);
     PF_CUDA(cudaStreamSynchronize(stream));
     timing.ms_tune = wall_ms() - t0;
-    std::lock_guard<std::mutex> lk(mu);
-    cache[key.str()] = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[tune_key()] = best;
   }
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
@@ -669,9 +701,9 @@ void Batch::run(bool gradient) {
     const bool full = !dargs.incremental || it == 1 || ((it - 1) % dargs.rebuild_every) == 0;
     PF_CUDA(cudaGraphLaunch(full ? graph_full : graph_inc, stream));
     count_launches(full ? graph_launches[0] : graph_launches[1]);
-    PF_CUDA(cudaMemcpyAsync(active_host, active_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaMemcpyAsync(&active_host, active_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
-    if (*active_host == 0) break;
+    if (active_host == 0) break;
   }
   timing.iterations = std::min(it, dargs.max_iter);
   timing.ms_scf = wall_ms() - ts;
@@ -707,6 +739,9 @@ void Batch::run(bool gradient) {
 // kernel and the two-electron gradient over the FP64 task lists.
 void Batch::gradient_run() {
   const double t0 = wall_ms();
+  cudaEvent_t ev[4];
+  for (auto& e : ev) PF_CUDA(cudaEventCreate(&e));
+  PF_CUDA(cudaEventRecord(ev[0], stream));
   launch_batch_wdens(nmol, dargs, W, stream);
   launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.P, dmax, stream);
   launch_zero(grad_dev, 3 * (size_t)natoms_tot * sizeof(double), stream);
@@ -719,7 +754,9 @@ void Batch::gradient_run() {
   g1.nbf = 0;
   g1.grad = grad_dev;
   g1.natoms_total = natoms_tot;
+  PF_CUDA(cudaEventRecord(ev[1], stream));
   launch_grad1e(shd, n1e, pairs1e, g1, num_sms, stream);
+  PF_CUDA(cudaEventRecord(ev[2], stream));
   unsigned long long* gstats = stats_dev + sizeof(JkStats) / sizeof(unsigned long long);
   PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
   GradArgs g2;
@@ -744,12 +781,21 @@ void Batch::gradient_run() {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }
     }
+  PF_CUDA(cudaEventRecord(ev[3], stream));
   grad_host.assign(3 * (size_t)natoms_tot, 0.0);
   PF_CUDA(cudaMemcpyAsync(grad_host.data(), grad_dev, grad_host.size() * sizeof(double), cudaMemcpyDeviceToHost,
                           stream));
   unsigned long long cnt[2 * NQCLASS];
   PF_CUDA(cudaMemcpyAsync(cnt, gstats, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
+  if (opt.verbose) {
+    float a = 0, b = 0, c = 0;
+    PF_CUDA(cudaEventElapsedTime(&a, ev[0], ev[1]));
+    PF_CUDA(cudaEventElapsedTime(&b, ev[1], ev[2]));
+    PF_CUDA(cudaEventElapsedTime(&c, ev[2], ev[3]));
+    std::fprintf(stderr, "pyfacc batch gradient (ms): W + dmax %.3f  one-electron %.3f  two-electron %.3f\n", a, b, c);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
   timing.flops_grad = 0.0;
   for (int q = 0; q < NQCLASS; ++q)
     timing.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false));

@@ -15,6 +15,7 @@
 // purification and the next build density, all on chip).  Converged
 // molecules get a zero build density, so later builds skip their quartets.
 #pragma once
+#include <array>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -143,7 +144,7 @@ class Batch {
   unsigned long long* stats_dev = nullptr;
   double* grad_dev = nullptr;
   int* active_dev = nullptr;
-  int* active_host = nullptr;   // pinned
+  int active_host = 0;          // copy of *active_dev after each iteration
   cudaGraphExec_t graph_full = nullptr, graph_inc = nullptr;
   long long graph_launches[2] = {0, 0};   // kernels per replay of graph_full / graph_inc
   std::vector<BatchMolState> st_host;
@@ -157,6 +158,8 @@ class Batch {
   void alloc();
   // J/K of Db into Jd/Kd: FP64 lists, or the FP64 + FP32 halves of mixed mode
   void fock_build(bool mixed_lists, double thresh, unsigned long long* stats);
+  bool tuned_widths(std::array<int, NQCLASS>* w) const;  // cached tuner result for this batch shape
+  std::string tune_key() const;
   void tune();
   cudaGraphExec_t capture(bool full, long long* launches);
   void gradient_run();

@@ -1,4 +1,5 @@
 // C ABI of libpyfacc_b200.so (declared in include/pyfacc_b200.h).
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -170,6 +171,7 @@ int pyfacc_run_batch(int nmol, const pyfacc_molecule* mols, const pyfacc_options
   if (opt) o = *opt; else pyfacc_default_options(&o);
   std::vector<int> status(nmol, PYFACC_OK), single, in_batch;
   std::vector<pyfacc::BatchMolHost> hosts;
+  const auto tp0 = std::chrono::steady_clock::now();
   for (int i = 0; i < nmol; ++i) {
     pyfacc_result* r = res ? &res[i] : nullptr;
     const bool wants_matrices = r && (r->S || r->T || r->V || r->P || r->C_alpha || r->C_beta || r->eps_alpha ||
@@ -189,6 +191,9 @@ int pyfacc_run_batch(int nmol, const pyfacc_molecule* mols, const pyfacc_options
       hosts.push_back(std::move(h));
     }
   }
+  if (o.verbose)
+    std::fprintf(stderr, "pyfacc batch parse (ms): %.2f\n",
+                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count());
   if (!hosts.empty()) {
     const int st = guarded([&] {
       pyfacc::Batch b(hosts, o);
