@@ -1,9 +1,10 @@
 // Dense per-molecule work of the batched engine.  One thread block per
-// molecule; every n x n product is computed by the block itself with 4 x 4
-// register tiles from L1/L2-resident operands (the matrices of a molecule of
-// up to 160 basis functions are at most 200 KB), the TC2 iterate stays in
-// shared memory, reductions go through shared memory, and nothing returns
-// to the host between the Fock build and the next build density.
+// molecule; every n x n product is computed by the block itself on the FP64
+// tensor cores (mma.sync m8n8k4) from L1/L2-resident operands (the
+// matrices of a molecule of up to 160 basis functions are at most 200 KB),
+// the TC2 iterate stays in shared memory, reductions go through shared
+// memory, and nothing returns to the host between the Fock build and the
+// next build density.
 //
 // The SCF step follows the single-molecule engine (rscf.f90:118-156 with
 // DIIS and purification): F = H + J - K/2, E = 1/2 sum P (H + F), the DIIS
@@ -43,36 +44,50 @@ __device__ double blk_reduce(double v, bool mx) {
 }
 
 // C = alpha A B (+ beta C) for n x n row-major matrices with leading
-// dimension n.  C must not alias A or B.  Ends with a block barrier.
+// dimension n, on the FP64 tensor cores: each warp owns 8 x 8 output tiles
+// and runs mma.sync.m8n8k4 (f64) over k in steps of 4; elements beyond n
+// are read as zero and not written.  A, B, C may be global or shared; C
+// must not alias A or B.  Ends with a block barrier.
+//
+// Fragments of m8n8k4 (f64, row.col): lane l holds A[l/4][l%4],
+// B[l%4][l/4] and C[l/4][2(l%4)], C[l/4][2(l%4)+1].
 __device__ void bgemm(int n, const double* A, const double* B, double* C, double alpha, double beta) {
-  const int nt = (n + 3) >> 2;
-  for (int tile = threadIdx.x; tile < nt * nt; tile += blockDim.x) {
-    const int i0 = (tile / nt) << 2, j0 = (tile % nt) << 2;
-    const int ni = min(4, n - i0), nj = min(4, n - j0);
-    double acc[4][4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-    for (int k = 0; k < n; ++k) {
-      double a[4], b[4];
-#pragma unroll
-      for (int r = 0; r < 4; ++r) a[r] = r < ni ? A[(size_t)(i0 + r) * n + k] : 0.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) b[c] = c < nj ? B[(size_t)k * n + j0 + c] : 0.0;
-#pragma unroll
-      for (int r = 0; r < 4; ++r)
-#pragma unroll
-        for (int c = 0; c < 4; ++c) acc[r][c] = fma(a[r], b[c], acc[r][c]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int nt = (n + 7) >> 3;
+  for (int tile = warp; tile < nt * nt; tile += nwarp) {
+    const int i0 = (tile / nt) << 3, j0 = (tile % nt) << 3;
+    const int ra = i0 + g;          // row of A this lane reads
+    const int cb = j0 + g;          // column of B this lane reads
+    // two accumulator chains (even and odd k-steps) so that consecutive
+    // MMAs do not wait on each other
+    double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+    for (int k0 = 0; k0 < n; k0 += 8) {
+      const int ka = k0 + t, kb = k0 + 4 + t;
+      const double a = (ra < n && ka < n) ? A[(size_t)ra * n + ka] : 0.0;
+      const double b = (ka < n && cb < n) ? B[(size_t)ka * n + cb] : 0.0;
+      const double a2 = (ra < n && kb < n) ? A[(size_t)ra * n + kb] : 0.0;
+      const double b2 = (kb < n && cb < n) ? B[(size_t)kb * n + cb] : 0.0;
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                   : "+d"(d0), "+d"(d1)
+                   : "d"(a), "d"(b));
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                   : "+d"(e0), "+d"(e1)
+                   : "d"(a2), "d"(b2));
     }
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-#pragma unroll
-      for (int c = 0; c < 4; ++c)
-        if (r < ni && c < nj) {
-          const size_t idx = (size_t)(i0 + r) * n + j0 + c;
-          C[idx] = (beta == 0.0) ? alpha * acc[r][c] : alpha * acc[r][c] + beta * C[idx];
-        }
+    d0 += e0;
+    d1 += e1;
+    const int r = i0 + g, c = j0 + 2 * t;
+    if (r < n) {
+      if (c < n) {
+        const size_t q = (size_t)r * n + c;
+        C[q] = (beta == 0.0) ? alpha * d0 : alpha * d0 + beta * C[q];
+      }
+      if (c + 1 < n) {
+        const size_t q = (size_t)r * n + c + 1;
+        C[q] = (beta == 0.0) ? alpha * d1 : alpha * d1 + beta * C[q];
+      }
+    }
   }
   __syncthreads();
 }
