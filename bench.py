@@ -48,6 +48,7 @@ WORKLOADS = {
     "c20h42": dict(n=20, seed=1, basis="sto-3g", label="C20H42 RHF STO-3G (142 bf)"),
     "c40h82": dict(n=40, seed=40, basis="sto-3g", label="C40H82 RHF STO-3G (282 bf)"),
     "c10h22": dict(n=10, seed=1, basis="sto-3g", label="C10H22 RHF STO-3G (72 bf)"),
+    "c100h202": dict(n=100, seed=4, basis="sto-3g", label="C100H202 RHF STO-3G (702 bf)"),
 }
 
 
@@ -181,21 +182,29 @@ def run_ours(args):
         step_mx, step_64 = t.tolist()
         dist.barrier()
 
-    # Fock builds per second: full FP64 J/K builds on the converged density
-    n = s_fp64.nbf
-    Pdev = ctypes.c_void_p()
-    N.lib().pyfacc_system_density_dev(s_fp64.handle, ctypes.byref(Pdev))
-    J = torch.zeros(n, n, dtype=torch.float64, device="cuda")
-    K = torch.zeros(n, n, dtype=torch.float64, device="cuda")
-    for _ in range(3):
-        N.lib().pyfacc_system_jk(s_fp64.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), 0)
-    nb = 20
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(nb):
-        N.lib().pyfacc_system_jk(s_fp64.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), 0)
-    torch.cuda.synchronize()
-    fock_s = (time.perf_counter() - t0) / nb
+    # Fock builds per second: J/K builds on the converged density (FP64
+    # lists, and the FP64 + FP32 lists of mixed mode), mean of 20
+    def fock_rates(sy):
+        n = sy.nbf
+        Pdev = ctypes.c_void_p()
+        N.lib().pyfacc_system_density_dev(sy.handle, ctypes.byref(Pdev))
+        J = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+        K = torch.zeros(n, n, dtype=torch.float64, device="cuda")
+        out = {}
+        for name, prec in (("fp64", N.PRECISION_FP64), ("mixed", N.PRECISION_MIXED)):
+            for _ in range(3):
+                N.lib().pyfacc_system_jk(sy.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), prec)
+            nb = 20
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(nb):
+                N.lib().pyfacc_system_jk(sy.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), prec)
+            torch.cuda.synchronize()
+            out[name] = nb / (time.perf_counter() - t0)
+        return out
+
+    rates = {WORKLOADS[args.workload]["label"]: fock_rates(s_fp64)}
+    fock_s = 1.0 / rates[WORKLOADS[args.workload]["label"]]["fp64"]
     breakdown = {}
     for name, sy in (("mixed", s_mixed), ("fp64", s_fp64)):
         rr = sy.result()
@@ -218,11 +227,19 @@ def run_ours(args):
                 r, g = device_step(sy)
                 ts.append((r.timings_ms["total"] + sy.result().timings_ms["gradient"]) / 1e3)
             res40[prec] = (min(ts), r.energy, g)
+            if prec == "fp64":
+                rates[WORKLOADS["c40h82"]["label"]] = fock_rates(sy)
             sy.close()
         c40 = {"workload": WORKLOADS["c40h82"]["label"], "fp64_s": res40["fp64"][0], "mixed_s": res40["mixed"][0],
                "mixed_speedup_vs_fp64": res40["fp64"][0] / res40["mixed"][0],
                "delta_e": abs(res40["fp64"][1] - res40["mixed"][1]),
                "max_grad_diff": float(np.abs(res40["fp64"][2] - res40["mixed"][2]).max())}
+
+    if rank == 0 and args.workload == "c20h42" and not args.no_c40:
+        sy = pyfacc.System(molecule("c100h202", 0), precision="fp64", device=local)
+        sy.scf(check=False)
+        rates[WORKLOADS["c100h202"]["label"]] = fock_rates(sy)
+        sy.close()
 
     # batch of 256 water clusters (H2O)n, n uniform in [4, 16], rank 0 only:
     # one pyfacc_run_batch call = energies and gradients of all 256 molecules
@@ -307,6 +324,7 @@ def run_ours(args):
         "max_grad_diff_mixed_vs_fp64": dG,
         "scf_iterations": {"mixed": it_mx[0], "fp64": it_64[0]},
         "fock_builds_per_s": 1.0 / fock_s,
+        "fock_builds_per_s_by_workload": rates,
         "breakdown_ms": breakdown,
         "north_star_c40h82": c40,
         "batch_water256": batch,
