@@ -4,8 +4,11 @@
   F_m(x) = 1F1(m+1/2; m+3/2; -x) / (2m+1)
 * h2o_sto3g.json   -- the oracle's converged H2O/STO-3G energy (data/molecules/
   h2o.xyz) and its V matrix with the reference's trapezoid Boys function.
+* c20h42_sto3g.json -- the oracle's converged energy and analytic gradient of
+  the C20H42/STO-3G benchmark molecule (pyfacc.geometry.alkane(20, seed=1),
+  142 basis functions); several minutes of CPU time, hence a fixture.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [c20h42]
 """
 import json
 import os
@@ -44,5 +47,22 @@ def main():
                    "S": S.tolist(), "T": T.tolist(), "V_trapezoid": V.tolist()}, fh)
 
 
+def c20h42():
+    import oracle as O
+    sys.path.insert(0, os.path.join(ROOT, "pyfacc-scf_b200"))
+    from pyfacc import geometry as G
+    sp, xyz = G.alkane(20, seed=1)
+    mol = O.molecule(sp, xyz, os.path.join(ROOT, "pyfacc-scf_b200", "data", "basis_set", "sto-3g.txt"))
+    r = O.scf(mol)
+    g = O.gradient(mol, r)
+    with open(os.path.join(HERE, "c20h42_sto3g.json"), "w") as fh:
+        json.dump({"source": "oracle, alkane(20, seed=1), STO-3G RHF, dE<1e-10, DIIS err<1e-8, Schwarz 1e-12",
+                   "nbf": int(mol.shells.nbf), "energy": r.energy, "converged": bool(r.converged),
+                   "gradient": np.asarray(g).tolist()}, fh)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "c20h42":
+        c20h42()
+    else:
+        main()
