@@ -68,7 +68,9 @@ typedef struct pyfacc_options {
                                chosen by timing for a batch            (0)   */
   int gradient_precision;   /* PYFACC_PRECISION_* of the derivative
                                integrals; MIXED evaluates the quartets with
-                               Q_ab Q_cd < fp32_thresh in FP32         (FP64) */
+                               Q_ab Q_cd < fp32_thresh in FP32; -1 = MIXED for
+                               a mixed-precision SCF of >= 200 basis
+                               functions (where it is faster), else FP64 (-1) */
   int polish;               /* mixed: energy and F of the converged density
                                from one more full FP64 build (1, |dE| vs
                                FP64 ~1e-12), or from the last incremental

@@ -771,6 +771,7 @@ void Batch::gradient_run() {
   g2.uhf = 0;
   g2.grad = grad_dev;
   g2.stats = gstats;
+  // the batch's molecules are small: FP32 derivative integrals only on request
   const bool split = opt.gradient_precision == PYFACC_PRECISION_MIXED;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {

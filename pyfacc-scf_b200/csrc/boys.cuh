@@ -13,8 +13,8 @@
 // relative); beyond T = 100, e^{-T} < 4e-44 and is dropped (a relative
 // change below 1e-29 of F_6).  The grid values are computed once on the host
 // in long double from the positive series (ensure_boys_tables, kernels.cu).
-// FP32 mode (mixed precision) uses an unscaled grid in float with 5 Taylor
-// terms and expf.
+// FP32 mode (mixed precision) uses the same per-order scaled grid in float
+// with 5 Taylor terms, and expf.
 //
 // Reference mode: boys.f90:9-43 of PyFAcc-SCF -- Taylor 1/(2m+1) - x/(2m+3)
 // for x <= 1e-6, else the 1001-point trapezoid rule on [0,1].  It is used for
@@ -38,10 +38,10 @@ namespace pyfacc {
 // Grid tables (this header is included by exactly one translation unit,
 // kernels.cu, which fills them per device with cudaMemcpyToSymbol):
 // g_boys_tl[L][k][j] = F_{L+j}(T_k) / j!, g_boys_exp[k] = e^{-T_k},
-// g_boys_tabf[k][m] = F_m(T_k) in float.
+// g_boys_tlf[L][k][j] = F_{L+j}(T_k) / j! in float (j < 5 used).
 __device__ __align__(16) double g_boys_tl[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
 __device__ double g_boys_exp[PF_BOYS_NEXP];
-__device__ float g_boys_tabf[PF_BOYS_NGRID * PF_BOYS_NCOL];
+__device__ __align__(16) float g_boys_tlf[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
 
 // Branch-free: every lane evaluates the Taylor value (from row 0 when T is
 // beyond the grid) and the asymptotic value and selects, so a warp whose
@@ -92,10 +92,12 @@ __device__ __forceinline__ void boys_fp32(float T, float* __restrict__ F) {
   const bool tab = T < (float)PF_BOYS_TMAX;
   const int k = tab ? __float2int_rn(T * (float)PF_BOYS_INV_STEP) : 0;
   const float x = k * (float)PF_BOYS_STEP - T;
-  const float* row = g_boys_tabf + k * PF_BOYS_NCOL + L;
-  float f = __ldg(row + PF_BOYS_NTF - 1);
-#pragma unroll
-  for (int j = PF_BOYS_NTF - 2; j >= 0; --j) f = __ldg(row + j) + f * x * (1.0f / (j + 1));
+  const float4* row = reinterpret_cast<const float4*>(g_boys_tlf + ((size_t)L * PF_BOYS_NGRID + k) * PF_BOYS_NT);
+  const float4 c0 = __ldg(row), c1 = __ldg(row + 1);
+  float f = fmaf(c1.x, x, c0.w);  // 5 terms: F_{L+j}(T_k) / j!, j = 4 .. 0
+  f = fmaf(f, x, c0.z);
+  f = fmaf(f, x, c0.y);
+  f = fmaf(f, x, c0.x);
   const float rt = rsqrtf(fmaxf(T, (float)PF_BOYS_TMAX));
   float fa = 0.88622692545275801365f * rt;
   if (L == 0) {

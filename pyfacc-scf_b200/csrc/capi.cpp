@@ -102,7 +102,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->guess = PYFACC_GUESS_ATOMIC;
   o->incremental_thresh = 1e-11;
   o->task_width = 0;
-  o->gradient_precision = PYFACC_PRECISION_FP64;
+  o->gradient_precision = -1;
   o->polish = 0;
 }
 

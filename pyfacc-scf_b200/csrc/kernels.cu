@@ -63,14 +63,14 @@ void ensure_boys_tables(int device) {
       }
     ex.resize(PF_BOYS_NEXP);
     for (int k = 0; k < PF_BOYS_NEXP; ++k) ex[k] = (double)expl(-(long double)k * 0.1L);
-    tabf.resize((size_t)PF_BOYS_NGRID * PF_BOYS_NCOL);
-    for (size_t i = 0; i < tabf.size(); ++i) tabf[i] = (float)F[i];
+    tabf.resize(tl.size());
+    for (size_t i = 0; i < tl.size(); ++i) tabf[i] = (float)tl[i];
   }
   if ((int)done.size() <= device) done.resize(device + 1, 0);
   if (!done[device]) {
     PF_CUDA(cudaMemcpyToSymbol(g_boys_tl, tl.data(), tl.size() * sizeof(double)));
     PF_CUDA(cudaMemcpyToSymbol(g_boys_exp, ex.data(), ex.size() * sizeof(double)));
-    PF_CUDA(cudaMemcpyToSymbol(g_boys_tabf, tabf.data(), tabf.size() * sizeof(float)));
+    PF_CUDA(cudaMemcpyToSymbol(g_boys_tlf, tabf.data(), tabf.size() * sizeof(float)));
     done[device] = 1;
   }
 }

@@ -633,9 +633,12 @@ void System::gradient(double* g_host) {
   unsigned long long* gstats = stats_dev;  // reuse the J/K counters' space
   PF_CUDA(cudaMemsetAsync(gstats, 0, 2 * NQCLASS * sizeof(unsigned long long), stream));
   g2.stats = gstats;
-  // FP32 derivative integrals for the small quartets only on request
-  // (options.gradient_precision = MIXED).
-  const bool split = opt.gradient_precision == PYFACC_PRECISION_MIXED && pd.primf != nullptr;
+  // FP32 derivative integrals for the small quartets on request, or by
+  // default in mixed mode from 200 basis functions on (below that the extra
+  // launches cost more than the FP32 arithmetic saves on B200)
+  const bool split = pd.primf != nullptr &&
+                     (opt.gradient_precision == PYFACC_PRECISION_MIXED ||
+                      (opt.gradient_precision < 0 && opt.precision == PYFACC_PRECISION_MIXED && nbf >= 200));
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (split) {
