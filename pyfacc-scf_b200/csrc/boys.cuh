@@ -49,9 +49,14 @@ __device__ __align__(16) float g_boys_tlf[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * P
 template <int L>
 __device__ __forceinline__ void boys_fp64(double T, double* __restrict__ F) {
   const bool tab = T < PF_BOYS_TMAX;
-  const int ke = __double2int_rn(fmin(T, PF_BOYS_EMAX) * PF_BOYS_INV_STEP);
+  // nearest grid point by adding and subtracting 1.5 * 2^52 (round to
+  // nearest in the FMA pipe, no conversion instructions): kd = round(10 T),
+  // the integer sits in the low word of the biased value
+  const double biased = fmin(T, PF_BOYS_EMAX) * PF_BOYS_INV_STEP + 6755399441055744.0;
+  const int ke = __double2loint(biased);
+  const double kd = biased - 6755399441055744.0;
   const int k = tab ? ke : 0;
-  const double x = ke * PF_BOYS_STEP - T;  // F_L(T) = sum_j F_{L+j}(T_k) x^j / j! (T < 36)
+  const double x = kd * PF_BOYS_STEP - T;  // F_L(T) = sum_j F_{L+j}(T_k) x^j / j! (T < 36)
   const double2* row = reinterpret_cast<const double2*>(g_boys_tl + ((size_t)L * PF_BOYS_NGRID + k) * PF_BOYS_NT);
   const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3);
   double f = fma(c67.y, x, c67.x);
@@ -90,8 +95,10 @@ __device__ __forceinline__ void boys_fp64(double T, double* __restrict__ F) {
 template <int L>
 __device__ __forceinline__ void boys_fp32(float T, float* __restrict__ F) {
   const bool tab = T < (float)PF_BOYS_TMAX;
-  const int k = tab ? __float2int_rn(T * (float)PF_BOYS_INV_STEP) : 0;
-  const float x = k * (float)PF_BOYS_STEP - T;
+  // nearest grid point by adding and subtracting 1.5 * 2^23 (see boys_fp64)
+  const float biased = fminf(T, (float)PF_BOYS_TMAX) * (float)PF_BOYS_INV_STEP + 12582912.0f;
+  const int k = tab ? (__float_as_int(biased) & 0x7fffff) - 0x400000 : 0;
+  const float x = (biased - 12582912.0f) * (float)PF_BOYS_STEP - T;
   const float4* row = reinterpret_cast<const float4*>(g_boys_tlf + ((size_t)L * PF_BOYS_NGRID + k) * PF_BOYS_NT);
   const float4 c0 = __ldg(row), c1 = __ldg(row + 1);
   float f = fmaf(c1.x, x, c0.w);  // 5 terms: F_{L+j}(T_k) / j!, j = 4 .. 0
