@@ -229,19 +229,22 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
   R acc[C::NACC];
 #pragma unroll
   for (int i = 0; i < C::NACC; ++i) acc[i] = (R)0;
-  const double kab_max = fabs((double)prim[3 * (size_t)bi0.z].z);
+  // the cut is compared in the records' precision (no FP64 work in the FP32
+  // loop); a cut beyond the float range becomes +inf, which skips everything
+  const R cut = (R)kcut;
+  const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
   int nprim = 0;
   for (int kq = 0; kq < ki0.w; ++kq) {
     const V* kr = prim + 3 * (size_t)(ki0.z + kq);
     const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
-    const double kcd = fabs((double)k0.z);
-    if (kab_max * kcd < kcut) break;
+    const R kcd = fabs((R)k0.z);
+    if (kab_max * kcd < cut) break;
     const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
 #pragma unroll 1
     for (int kp = 0; kp < bi0.w; ++kp) {
       const V* br = prim + 3 * (size_t)(bi0.z + kp);
       const V b0 = br[0], b1 = br[1], b2 = br[2];
-      if (fabs((double)b0.z) * kcd < kcut) break;
+      if (fabs((R)b0.z) * kcd < cut) break;
       const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
       PrimGeo<R> g;
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
@@ -876,17 +879,18 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const R CD[3] = {(R)kg.x, (R)kg.y, (R)kg.z};
       R gr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       const V* prim = grecords<R>(args);
-      const double kab_max = fabs((double)prim[3 * (size_t)bi0.z].z);
+      const R cut = (R)kcut;
+      const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
       for (int kq = 0; kq < ki0.w; ++kq) {
         const V* kr = prim + 3 * (size_t)(ki0.z + kq);
         const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
-        const double kcd = fabs((double)k0.z);
-        if (kab_max * kcd < kcut) break;
+        const R kcd = fabs((R)k0.z);
+        if (kab_max * kcd < cut) break;
         const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
         for (int kpp = 0; kpp < bi0.w; ++kpp) {
           const V* br = prim + 3 * (size_t)(bi0.z + kpp);
           const V b0 = br[0], b1 = br[1], b2 = br[2];
-          if (fabs((double)b0.z) * kcd < kcut) break;
+          if (fabs((R)b0.z) * kcd < cut) break;
           ++nprim;
           const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
           PrimGeo<R> pg;
