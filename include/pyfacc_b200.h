@@ -75,6 +75,10 @@ typedef struct pyfacc_options {
                                from one more full FP64 build (1, |dE| vs
                                FP64 ~1e-12), or from the last incremental
                                mixed build (0, |dE| ~1e-8)              (0)   */
+  double gradient_fp32_thresh; /* mixed gradient: derivative quartets with
+                               Q_ab Q_cd max|P| below this run in FP32
+                               (|dG| ~3e-9 Ha/bohr at 1e-3 for C20H42..
+                               C100H202); <= 0: fp32_thresh            (1e-3) */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {

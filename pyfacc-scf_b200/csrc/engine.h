@@ -43,11 +43,15 @@ constexpr int NQCLASS = 6;       // (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|
 // primitive-quartet cut relative to the quartet screening threshold:
 // |K_ab K_cd| max|D| < PRIM_QUARTET_REL * thresh skips a primitive quartet
 // (its integral is at most ~1.5 |K_ab K_cd|, as F_m <= 1 and p + q > 0.4
-// for STO-nG exponents)
-constexpr double PRIM_QUARTET_REL = 1e-4;
-// the same for derivative integrals, which carry factors 2 alpha (<= ~200
-// for STO-nG exponents)
-constexpr double PRIM_QUARTET_REL_GRAD = 1e-6;
+// for STO-nG exponents).  1e-2 moves FP64 energies of C20H42..C100H202 by
+// 2e-11..1e-10 Ha; 1 moves them by ~1e-8 and stalls the incremental builds
+// of mixed precision.
+constexpr double PRIM_QUARTET_REL = 1e-2;
+// the same for derivative integrals (factors 2 alpha <= ~200 for STO-nG
+// exponents): the screening threshold itself moves the gradient of
+// C20H42..C100H202 by ~1e-9 Ha/bohr and leaves it translationally invariant
+// (the fourth centre is minus the sum of the other three)
+constexpr double PRIM_QUARTET_REL_GRAD = 1.0;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis

@@ -793,6 +793,7 @@ struct GradKernelArgs {
   const int* task_off;
   const int* ket_lo;
   const int* ket_hi;
+  const int* ntasks_dev;  // device count of a list built on the GPU (else ntasks)
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, task_begin;
   int lwidth;
   int smem_atoms;  // atoms summed in shared memory (0: global atomics)
@@ -818,10 +819,11 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   for (int i = threadIdx.x; i < nsm; i += blockDim.x) gsh[i] = 0.0;
   if (nsm) __syncthreads();
   double* G = nsm ? gsh : A.grad;
-  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < args.ntasks; tb += nw * tpw) {
+  const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
+  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < ntasks; tb += nw * tpw) {
     const int tl = tb + (lane >> lw);
-    const bool valid = tl < args.ntasks;
-    const int t = args.task_begin + (valid ? tl : args.ntasks - 1);
+    const bool valid = tl < ntasks;
+    const int t = args.task_begin + (valid ? tl : ntasks - 1);
     const int ib = find_bra(args.task_off, args.nbra, t);
     const int ket = __ldg(args.ket_lo + ib) + (t - __ldg(args.task_off + ib)) * W + sub;
     const int bp = args.bra_base + ib;
@@ -881,12 +883,14 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const V* prim = grecords<R>(args);
       const R cut = (R)kcut;
       const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
+#pragma unroll 1
       for (int kq = 0; kq < ki0.w; ++kq) {
         const V* kr = prim + 3 * (size_t)(ki0.z + kq);
         const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
         const R kcd = fabs((R)k0.z);
         if (kab_max * kcd < cut) break;
         const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+#pragma unroll 1
         for (int kpp = 0; kpp < bi0.w; ++kpp) {
           const V* br = prim + 3 * (size_t)(bi0.z + kpp);
           const V b0 = br[0], b1 = br[1], b2 = br[2];
@@ -973,6 +977,7 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   k.geom = pd.geom; k.prim = pd.prim; k.primf = pd.primf;
   if (fp32 && !pd.primf) throw Error(PYFACC_ERR_INVALID, "FP32 quartets need float primitive records");
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
+  k.ntasks_dev = tl.ntasks_dev;
   k.nbra = tl.nbra; k.ntasks = tl.ntasks; k.task_begin = tl.task_begin;
   k.bra_base = pd.class_off[bc] + tl.bra_offset; k.ket_base = pd.class_off[kc];
   k.same_class = (bc == kc);

@@ -635,13 +635,23 @@ void System::gradient(double* g_host) {
   g2.stats = gstats;
   // FP32 derivative integrals for the small quartets on request, or by
   // default in mixed mode from 200 basis functions on (below that the extra
-  // launches cost more than the FP32 arithmetic saves on B200)
+  // launches cost more than the FP32 arithmetic saves on B200).  One
+  // process splits at Q_ab Q_cd max|P| = gradient_fp32_thresh with lists
+  // built on the device; shards use their static lists (split at fp32_thresh).
   const bool split = pd.primf != nullptr &&
                      (opt.gradient_precision == PYFACC_PRECISION_MIXED ||
                       (opt.gradient_precision < 0 && opt.precision == PYFACC_PRECISION_MIXED && nbf >= 200));
+  const bool dyn_split = split && opt.shard_count <= 1;
+  if (dyn_split)
+    launch_dyn_tasks(pd, dmax, ns, opt.schwarz_thresh,
+                     opt.gradient_fp32_thresh > 0 ? opt.gradient_fp32_thresh : opt.fp32_thresh, dyn, stream);
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
-      if (split) {
+      if (dyn_split) {
+        const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
+        launch_grad2e(pd, dyn.lists[2 * qc], bc, kc, false, g2, num_sms, stream);
+        launch_grad2e(pd, dyn.lists[2 * qc + 1], bc, kc, true, g2, num_sms, stream);
+      } else if (split) {
         launch_grad2e(pd, tasks[bc][kc][1], bc, kc, false, g2, num_sms, stream);
         launch_grad2e(pd, tasks[bc][kc][2], bc, kc, true, g2, num_sms, stream);
       } else {
