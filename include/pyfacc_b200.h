@@ -79,6 +79,10 @@ typedef struct pyfacc_options {
                                Q_ab Q_cd max|P| below this run in FP32
                                (|dG| ~3e-9 Ha/bohr at 1e-3 for C20H42..
                                C100H202); <= 0: fp32_thresh            (1e-3) */
+  double coarse_err;        /* mixed: while the DIIS error is above this every
+                               quartet runs in FP32; the first build below it
+                               is a full mixed build that restarts the
+                               incremental chain; 0 = off             (1e-3) */
 } pyfacc_options;
 
 typedef struct pyfacc_molecule {

@@ -105,6 +105,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->gradient_precision = -1;
   o->polish = 0;
   o->gradient_fp32_thresh = 1e-3;
+  o->coarse_err = 1e-3;
 }
 
 // scf_interface.c:9-14 -> main.f90:15-64: species/coords/z in, energy out.

@@ -52,6 +52,10 @@ constexpr double PRIM_QUARTET_REL = 1e-2;
 // C20H42..C100H202 by ~1e-9 Ha/bohr and leaves it translationally invariant
 // (the fourth centre is minus the sum of the other three)
 constexpr double PRIM_QUARTET_REL_GRAD = 1.0;
+// quartet screening threshold of the all-FP32 builds of the first mixed
+// iterations (their error is discarded by the full build that ends them);
+// 1e-8 costs C100H202 an extra iteration
+constexpr double COARSE_SCREEN = 1e-9;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis

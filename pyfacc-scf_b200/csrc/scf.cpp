@@ -51,7 +51,7 @@ void System::one_electron() {
 // density-weighted Schwarz test, the six class kernels (FP64 task lists, or
 // the FP64 and FP32 halves of the mixed lists), then J = Jh + Jh^T.
 void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-                bool dynamic, double thresh) {
+                bool dynamic, double thresh, double fp32_thresh) {
   if (thresh <= 0) thresh = opt.schwarz_thresh;
   const size_t n2 = (size_t)nbf * nbf;
   launch_zero(Jo, n2 * sizeof(double), stream);
@@ -71,7 +71,8 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   a.prim_thresh = thresh * PRIM_QUARTET_REL;
   const bool mixed = precision == PYFACC_PRECISION_MIXED;
   if (opt.shard_count > 1) dynamic = false;  // shards use their static sub-lists
-  if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? opt.fp32_thresh : 0.0, dyn, stream);
+  const double t32 = fp32_thresh >= 0 ? fp32_thresh : opt.fp32_thresh;
+  if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? t32 : 0.0, dyn, stream);
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
@@ -379,20 +380,34 @@ void System::run_scf() {
   double E_old = 0.0;
   double ms_fock = 0.0, ms_diag = 0.0;
   int since_full = 0;
+  // Dynamic precision (Luehr, Ufimtsev and Martinez, JCTC 7, 949 (2011)):
+  // while the DIIS error is above coarse_err every quartet runs in FP32;
+  // the first build after that is a full mixed build, so the incremental
+  // chain that produces the converged density starts afresh and carries no
+  // error of the coarse builds.
+  bool coarse = mixed && opt.coarse_err > 0 && opt.shard_count <= 1;
+  bool restart = false;
+  const double t32_coarse = 1e300;
+  const double coarse_screen = std::max(COARSE_SCREEN, opt.schwarz_thresh);
   const double* Pspin[2] = {P[0], P[1]};
   for (int it = 1; it <= opt.max_iter; ++it) {
     st.n_iter = it;
     // ---- Fock build
     PF_CUDA(cudaEventRecord(a0, stream));
-    const bool full = !incremental || it == 1 || since_full + 1 >= std::max(opt.rebuild_every, 1);
+    const bool full = !incremental || it == 1 || restart || since_full + 1 >= std::max(opt.rebuild_every, 1);
+    const bool coarse_build = coarse;
+    const double t32 = coarse_build ? t32_coarse : -1.0;
+    const double full_thresh = coarse_build ? coarse_screen : -1.0;
+    const double step_thresh = coarse_build ? std::max(coarse_screen, inc_thresh) : inc_thresh;
+    restart = false;
     double* Kp[2] = {K[0], K[1]};
     if (full) {
       if (uhf) {
         launch_axpby((long long)n2, 1.0, P[0], 0.0, W3, stream);
         launch_axpby((long long)n2, 1.0, P[1], 1.0, W3, stream);
-        jk(W3, 2, Pspin, J, Kp, opt.precision, mixed);
+        jk(W3, 2, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32);
       } else {
-        jk(P[0], 1, Pspin, J, Kp, opt.precision, mixed);
+        jk(P[0], 1, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32);
       }
       since_full = 0;
     } else {
@@ -407,9 +422,9 @@ void System::run_scf() {
       if (uhf) {
         launch_axpby((long long)n2, 1.0, dP[0], 0.0, Wm, stream);
         launch_axpby((long long)n2, 1.0, dP[1], 1.0, Wm, stream);
-        jk(Wm, 2, dPc, W1, dK, opt.precision, mixed, inc_thresh);
+        jk(Wm, 2, dPc, W1, dK, opt.precision, mixed, step_thresh, t32);
       } else {
-        jk(dP[0], 1, dPc, W1, dK, opt.precision, mixed, inc_thresh);
+        jk(dP[0], 1, dPc, W1, dK, opt.precision, mixed, step_thresh, t32);
       }
       launch_axpby((long long)n2, 1.0, W1, 1.0, J, stream);
       for (int s = 0; s < nsp; ++s) launch_axpby((long long)n2, 1.0, dK[s], 1.0, K[s], stream);
@@ -447,7 +462,8 @@ void System::run_scf() {
     double red[8 + 64];
     PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
-    ms_fock += elapsed(a0, a1);
+    const float ms_build = elapsed(a0, a1);
+    ms_fock += ms_build;
     const double E = 0.5 * red[0];
     const double err = red[1];
     const double dD = std::sqrt(red[2]);
@@ -457,14 +473,18 @@ void System::run_scf() {
     st.e_elec = E;
     st.energy = E + e_nuc;
     if (opt.verbose)
-      std::fprintf(stderr, "pyfacc iter %3d  E = %.12f  dE = %.3e  err = %.3e  |dD| = %.3e\n", it, E + e_nuc, dE,
-                   err, dD);
+      std::fprintf(stderr, "pyfacc iter %3d  E = %.12f  dE = %.3e  err = %.3e  |dD| = %.3e  %s%s build %.3f ms\n", it,
+                   E + e_nuc, dE, err, dD, coarse_build ? "FP32 " : "", full ? "full" : "incremental", ms_build);
     // In mixed precision the energy of incremental FP32/FP64 builds carries
     // a ~1e-10 noise floor; the density is converged on the commutator and
     // the energy is then taken from one full FP64 build (below).
     const double e_tol = mixed ? std::max(opt.eps_energy, 1e-8) : opt.eps_energy;
-    bool conv = dE < e_tol && err < opt.eps_diis;
+    bool conv = !coarse_build && dE < e_tol && err < opt.eps_diis;
     if (opt.eps_density > 0) conv = conv && it > 1 && dD < opt.eps_density;
+    if (coarse && err < opt.coarse_err) {
+      coarse = false;
+      restart = true;
+    }
     if (conv) {
       st.converged = true;
       break;

@@ -109,8 +109,9 @@ struct System {
   void one_electron();
   // J = J[Dj], K[k] = K[Dk[k]] (precision 0 = fp64, 1 = mixed); screening by
   // Q_ab Q_cd max|D| with the density(ies) given.
+  // fp32_thresh < 0: opt.fp32_thresh (mixed precision only)
   void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-          bool dynamic = false, double thresh = -1.0);
+          bool dynamic = false, double thresh = -1.0, double fp32_thresh = -1.0);
   void eri_tensor(double* eri);
   void orthogonalizer();
   void diagonalize(const double* Fm, double* C, double* eps);

@@ -47,6 +47,7 @@ class Options(ctypes.Structure):
         ("device", c_int), ("verbose", c_int), ("shard_rank", c_int), ("shard_count", c_int),
         ("data_dir", c_char_p), ("guess", c_int), ("incremental_thresh", c_double), ("task_width", c_int),
         ("gradient_precision", c_int), ("polish", c_int), ("gradient_fp32_thresh", c_double),
+        ("coarse_err", c_double),
     ]
 
 
