@@ -15,6 +15,9 @@
 #include <cctype>
 #include <cstdlib>
 #include <fstream>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <sstream>
 
 #include "engine.h"
@@ -86,8 +89,8 @@ static std::vector<std::string> read_lines(const std::string& path) {
   return lines;
 }
 
-Basis build_basis(const std::string& basis_file, const std::vector<std::string>& species,
-                  const std::vector<double>& xyz) {
+// Shells of the given atoms without their centres (every shell's c is 0).
+static Basis basis_template(const std::string& basis_file, const std::vector<std::string>& species) {
   const auto text = basis_lines(basis_file, &read_lines);
   const std::vector<std::string>& lines = *text;
   Basis B;
@@ -130,7 +133,6 @@ Basis build_basis(const std::string& basis_file, const std::vector<std::string>&
           Shell s;
           s.l = l;
           s.atom = a;
-          for (int x = 0; x < 3; ++x) s.c[x] = xyz[3 * a + x];
           s.ex = ex;
           s.co = c;
           B.shells.push_back(std::move(s));
@@ -153,6 +155,39 @@ Basis build_basis(const std::string& basis_file, const std::vector<std::string>&
     B.bf_off[s + 1] = B.bf_off[s] + (l + 1) * (l + 2) / 2;
   }
   B.nbf = B.bf_off.back();
+  return B;
+}
+
+// The shell list depends on the basis file and the species sequence only,
+// so it is parsed once per (file, species) and copied with the centres
+// filled in: batches of many molecules of few compositions (water clusters
+// of 4..16 monomers) parse the file a dozen times instead of once per
+// molecule.  Failed parses are not kept, so their errors repeat.
+Basis build_basis(const std::string& basis_file, const std::vector<std::string>& species,
+                  const std::vector<double>& xyz) {
+  static std::mutex mu;
+  static std::map<std::string, std::shared_ptr<const Basis>> cache;
+  std::string key = basis_file;
+  key.push_back('\n');
+  for (const auto& s : species) {
+    key += s;
+    key.push_back(' ');
+  }
+  std::shared_ptr<const Basis> t;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) t = it->second;
+  }
+  if (!t) {
+    t = std::make_shared<const Basis>(basis_template(basis_file, species));
+    std::lock_guard<std::mutex> lk(mu);
+    if (cache.size() >= 256) cache.clear();
+    cache[key] = t;
+  }
+  Basis B = *t;
+  for (auto& s : B.shells)
+    for (int x = 0; x < 3; ++x) s.c[x] = xyz[3 * s.atom + x];
   return B;
 }
 

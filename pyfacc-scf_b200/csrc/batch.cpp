@@ -5,7 +5,9 @@
 
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +22,25 @@ namespace pyfacc {
 static double wall_ms() {
   using namespace std::chrono;
   return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+
+// f(0) .. f(n - 1) on up to 16 host threads (f must not throw).
+template <typename F>
+static void parallel_for(int n, F&& f) {
+  int nt = (int)std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  nt = std::min(nt, n / 8);
+  if (nt <= 1) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next(0);
+  std::vector<std::thread> th;
+  th.reserve(nt);
+  for (int t = 0; t < nt; ++t)
+    th.emplace_back([&] {
+      for (int i; (i = next.fetch_add(1)) < n;) f(i);
+    });
+  for (auto& x : th) x.join();
 }
 
 static int qclass_index(int bc, int kc) { return (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc); }
@@ -212,8 +233,25 @@ void Batch::upload() {
 // class sorted by (molecule, Q descending); pairs that cannot reach the
 // threshold against the largest Q of their molecule are dropped.
 void Batch::build_pairs() {
+  double tp[8];
+  tp[0] = wall_ms();
   std::vector<int4> pl0[NCLASS], pl1[NCLASS];
   std::vector<int> pm[NCLASS];
+  {
+    size_t cnt[NCLASS] = {0, 0, 0};
+    for (const auto& M : mols) {
+      int nl[2] = {0, 0};
+      for (const auto& sh : M.basis.shells) nl[sh.l > 0 ? 1 : 0]++;
+      cnt[0] += (size_t)nl[0] * (nl[0] + 1) / 2;
+      cnt[1] += (size_t)nl[0] * nl[1];
+      cnt[2] += (size_t)nl[1] * (nl[1] + 1) / 2;
+    }
+    for (int c = 0; c < NCLASS; ++c) {
+      pl0[c].reserve(cnt[c]);
+      pl1[c].reserve(cnt[c]);
+      pm[c].reserve(cnt[c]);
+    }
+  }
   std::vector<int> nprim_of(ns_tot);
   for (int m = 0; m < nmol; ++m)
     for (int s = 0; s < mols[m].ns; ++s) nprim_of[mols[m].shell_off + s] = (int)mols[m].basis.shells[s].ex.size();
@@ -231,6 +269,10 @@ void Batch::build_pairs() {
   }
   std::vector<int4> all0, all1;
   std::vector<int> allm;
+  const size_t np_total = pl0[0].size() + pl0[1].size() + pl0[2].size();
+  all0.reserve(np_total);
+  all1.reserve(np_total);
+  allm.reserve(np_total);
   int off[NCLASS + 1] = {0, 0, 0, 0};
   long long nprim_tot = 0;
   for (int c = 0; c < NCLASS; ++c) {
@@ -252,6 +294,7 @@ void Batch::build_pairs() {
     o += (bytes + 255) / 256 * 256;
     return r;
   };
+  tp[1] = wall_ms();
   const size_t s_pl0 = carve(np_all * sizeof(int4)), s_pl1 = carve(np_all * sizeof(int4)),
                s_i0 = carve(np_all * sizeof(int4)), s_i1 = carve(np_all * sizeof(int4)),
                s_i2 = carve(np_all * sizeof(int4)), s_g = carve(np_all * sizeof(double4)),
@@ -260,6 +303,8 @@ void Batch::build_pairs() {
                s_ps = carve(np_all * sizeof(int)), s_kept = carve(np_all * sizeof(int));
   DeviceBuf scratch;
   scratch.ensure(o);
+  const double scratch_mb = (double)o / 1048576.0;
+  tp[2] = wall_ms();
   char* sb = scratch.as<char>();
   int4* d_pl0 = reinterpret_cast<int4*>(sb + s_pl0);
   int4* d_pl1 = reinterpret_cast<int4*>(sb + s_pl1);
@@ -286,6 +331,7 @@ void Batch::build_pairs() {
   PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaMemcpyAsync(kept.data(), d_kept, np_all * sizeof(int), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
+  tp[3] = wall_ms();
   std::vector<double> qmax(nmol, 0.0);
   for (int k = 0; k < np_all; ++k) qmax[allm[k]] = std::max(qmax[allm[k]], q[k]);
   const double thr = opt.schwarz_thresh;
@@ -299,14 +345,21 @@ void Batch::build_pairs() {
     // the pairs of a class are generated molecule by molecule: sort each
     // molecule's segment by Q (descending; ties by index, deterministic)
     std::vector<int> idx;
+    idx.reserve(off[c + 1] - off[c]);
     for (int k = off[c]; k < off[c + 1]; ++k)
       if (thr <= 0 || q[k] * qmax[allm[k]] >= thr) idx.push_back(k);
+    std::vector<size_t> starts;
     for (size_t a = 0; a < idx.size();) {
+      starts.push_back(a);
       size_t b = a;
       while (b < idx.size() && allm[idx[b]] == allm[idx[a]]) ++b;
-      std::sort(idx.begin() + a, idx.begin() + b, [&](int x, int y) { return q[x] > q[y] || (q[x] == q[y] && x < y); });
       a = b;
     }
+    starts.push_back(idx.size());
+    parallel_for((int)starts.size() - 1, [&](int g) {
+      std::sort(idx.begin() + starts[g], idx.begin() + starts[g + 1],
+                [&](int x, int y) { return q[x] > q[y] || (q[x] == q[y] && x < y); });
+    });
     seg[c].assign(nmol + 1, 0);
     for (int k : idx) {
       perm.push_back(k);
@@ -322,6 +375,7 @@ void Batch::build_pairs() {
   }
   pd.npair = (int)perm.size();
   pd.nprim = (int)nprim_new;
+  tp[4] = wall_ms();
   o = 0;
   const size_t f_i0 = carve(pd.npair * sizeof(int4)), f_i1 = carve(pd.npair * sizeof(int4)),
                f_i2 = carve(pd.npair * sizeof(int4)), f_g = carve(pd.npair * sizeof(double4)),
@@ -335,6 +389,7 @@ void Batch::build_pairs() {
   pd.geom = reinterpret_cast<double4*>(pb + f_g);
   pd.prim = reinterpret_cast<double4*>(pb + f_pr);
   pd.primf = reinterpret_cast<float4*>(pb + f_prf);
+  tp[5] = wall_ms();
   if (pd.npair > 0) {
     PF_CUDA(cudaMemcpyAsync(d_perm, perm.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
     PF_CUDA(cudaMemcpyAsync(d_ps, new_ps.data(), pd.npair * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -342,15 +397,23 @@ void Batch::build_pairs() {
                         pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, pd.primf, stream);
   }
   PF_CUDA(cudaStreamSynchronize(stream));
+  tp[6] = wall_ms();
+  scratch.release();
+  tp[7] = wall_ms();
+  if (opt.verbose)
+    std::fprintf(stderr,
+                 "pyfacc batch pairs (ms): host lists %.2f  scratch alloc %.2f (%.0f MB)  records+Q %.2f  sort %.2f"
+                 "  buffer alloc %.2f (%.0f MB)  gather %.2f  free %.2f\n",
+                 tp[1] - tp[0], tp[2] - tp[1], scratch_mb, tp[3] - tp[2], tp[4] - tp[3], tp[5] - tp[4],
+                 (double)pd.buf.bytes / 1048576.0, tp[6] - tp[5], tp[7] - tp[6]);
 }
 
-// Ket ranges per bra inside the bra's molecule (the segment of the ket
-// class): prefix with Q_bra Q_ket >= thresh, the FP64 part the prefix with
-// Q_bra Q_ket >= fp32_thresh; for equal classes only kets up to the bra.
-// The ranges are shared by the three task widths, whose task offsets differ.
+// Task lists of every (bra class, ket class) combination, precision part
+// and wanted task width, built on the device (batch_tasks.cu): ket ranges
+// inside the bra's molecule, then per width the task offsets.  The host
+// reads back only the task and quartet counts.
 void Batch::build_tasks() {
-  const double thr = std::max(opt.schwarz_thresh, 0.0);
-  const double t32 = opt.fp32_thresh;
+  const double tt0 = wall_ms();
   // which task widths are needed per class: all three for the tuner, else
   // the fixed width or the cached tuner result
   std::array<int, NQCLASS> fixed{};
@@ -362,79 +425,105 @@ void Batch::build_tasks() {
     have = tuned_widths(&fixed);
   }
   auto wanted = [&](int q, int wi) { return !have || fixed[q] == kWidths[wi]; };
-  struct Pending { int bc, kc, prec; size_t lo_off, toff_off[3]; int nbra; };
-  std::vector<Pending> pend;
-  std::vector<int> hostbuf;
+  // device layout: class segments, then per combination 3 x (lo, hi), then
+  // the task offsets of each wanted (precision, width)
+  size_t n = 0;
+  size_t seg_off[NCLASS];
+  for (int c = 0; c < NCLASS; ++c) {
+    seg_off[c] = n;
+    n += (size_t)nmol + 1;
+  }
+  struct Range { int bc, kc, nb; size_t lo[3], hi[3]; };
+  struct Scan { int bc, kc, prec, wi; size_t toff; };
+  std::vector<Range> ranges;
+  std::vector<Scan> scans;
+  int nb_max = 0;
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
       const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
-      const double* qb = pd.q_host.data() + pd.class_off[bc];
-      const double* qk = pd.q_host.data() + pd.class_off[kc];
-      const int* mb = pd.mol_host.data() + pd.class_off[bc];
-      auto prefix = [&](double qbra, const double* q0, int nk, double t) {
-        if (t <= 0) return nk;
-        int lo = 0, hi = nk;
-        while (lo < hi) {
-          int mid = (lo + hi) / 2;
-          if (qbra * q0[mid] >= t) lo = mid + 1; else hi = mid;
-        }
-        return lo;
-      };
-      std::vector<int> full_hi(nb), split(nb), kstart(nb);
-      for (int i = 0; i < nb; ++i) {
-        const int m = mb[i];
-        const int ks = seg[kc][m], nk = seg[kc][m + 1] - ks;
-        int mm = prefix(qb[i], qk + ks, nk, thr);
-        if (bc == kc) mm = std::min(mm, i - seg[bc][m] + 1);
-        const int m64 = std::min(prefix(qb[i], qk + ks, nk, t32), mm);
-        kstart[i] = ks;
-        full_hi[i] = ks + mm;
-        split[i] = ks + m64;
+      for (int wi = 0; wi < 3; ++wi)
+        for (int prec = 0; prec < 3; ++prec) tasks_w[wi][bc][kc][prec] = TaskList();
+      if (nb == 0) continue;
+      Range r{bc, kc, nb, {0, 0, 0}, {0, 0, 0}};
+      for (int p = 0; p < 3; ++p) {
+        r.lo[p] = n;
+        n += nb;
+        r.hi[p] = n;
+        n += nb;
       }
-      for (int prec = 0; prec < 3; ++prec) {
-        Pending p{bc, kc, prec, hostbuf.size(), {0, 0, 0}, nb};
-        std::vector<int> lo(nb), hi(nb);
-        long long quart = 0;
-        for (int i = 0; i < nb; ++i) {
-          lo[i] = (prec == 2) ? split[i] : kstart[i];
-          hi[i] = (prec == 1) ? split[i] : full_hi[i];
-          quart += hi[i] - lo[i];
-        }
-        hostbuf.insert(hostbuf.end(), lo.begin(), lo.end());
-        hostbuf.insert(hostbuf.end(), hi.begin(), hi.end());
+      ranges.push_back(r);
+      nb_max = std::max(nb_max, nb);
+      for (int p = 0; p < 3; ++p)
         for (int wi = 0; wi < 3; ++wi) {
-          const int w = kWidths[wi];
-          if (!wanted(qclass_index(bc, kc), wi)) {
-            p.toff_off[wi] = (size_t)-1;
-            continue;
-          }
-          p.toff_off[wi] = hostbuf.size();
-          int ntask = 0;
-          for (int i = 0; i < nb; ++i) {
-            hostbuf.push_back(ntask);
-            ntask += (hi[i] - lo[i] + w - 1) / w;
-          }
-          hostbuf.push_back(ntask);
-          TaskList& tl = tasks_w[wi][bc][kc][prec];
-          tl.width = w;
-          tl.nbra = nb;
-          tl.ntasks = ntask;
-          tl.nquartets = quart;
+          if (!wanted(qclass_index(bc, kc), wi)) continue;
+          scans.push_back(Scan{bc, kc, p, wi, n});
+          n += (size_t)nb + 1;
         }
-        pend.push_back(p);
-      }
     }
-  task_buf.ensure(std::max<size_t>(hostbuf.size() * sizeof(int), 256));
+  const size_t cnt_off = (n * sizeof(int) + 255) / 256 * 256;
+  const size_t bytes = cnt_off + scans.size() * (sizeof(int) + sizeof(long long)) + 256;
+  task_buf.ensure(std::max<size_t>(bytes, 256));
   int* d = task_buf.as<int>();
-  PF_CUDA(cudaMemcpyAsync(d, hostbuf.data(), hostbuf.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
-  for (auto& p : pend)
-    for (int wi = 0; wi < 3; ++wi) {
-      if (p.toff_off[wi] == (size_t)-1) continue;
-      TaskList& tl = tasks_w[wi][p.bc][p.kc][p.prec];
-      tl.ket_lo = d + p.lo_off;
-      tl.ket_hi = d + p.lo_off + p.nbra;
-      tl.task_off = d + p.toff_off[wi];
+  int* d_nt = reinterpret_cast<int*>(task_buf.as<char>() + cnt_off);
+  long long* d_nq = reinterpret_cast<long long*>(task_buf.as<char>() + cnt_off +
+                                                 (scans.size() * sizeof(int) + 7) / 8 * 8);
+  std::vector<int> segs((size_t)NCLASS * (nmol + 1));
+  for (int c = 0; c < NCLASS; ++c) std::copy(seg[c].begin(), seg[c].end(), segs.begin() + (size_t)c * (nmol + 1));
+  PF_CUDA(cudaMemcpyAsync(d, segs.data(), segs.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+  const double tt1 = wall_ms();
+  BatchRangeArgs ra{};
+  ra.geom = pd.geom;
+  ra.info2 = pd.info2;
+  ra.thresh = std::max(opt.schwarz_thresh, 0.0);
+  ra.fp32_thresh = opt.fp32_thresh;
+  for (size_t k = 0; k < ranges.size(); ++k) {
+    const Range& r = ranges[k];
+    BatchRangeList& L = ra.l[k];
+    L.bra_base = pd.class_off[r.bc];
+    L.ket_base = pd.class_off[r.kc];
+    L.nb = r.nb;
+    L.same = r.bc == r.kc;
+    L.seg_b = d + seg_off[r.bc];
+    L.seg_k = d + seg_off[r.kc];
+    for (int p = 0; p < 3; ++p) {
+      L.lo[p] = d + r.lo[p];
+      L.hi[p] = d + r.hi[p];
     }
+  }
+  launch_batch_ranges(ra, (int)ranges.size(), nb_max, stream);
+  BatchScanArgs sa{};
+  sa.ntasks = d_nt;
+  sa.nquartets = d_nq;
+  auto range_of = [&](int bc, int kc) -> const Range& {
+    for (const auto& r : ranges)
+      if (r.bc == bc && r.kc == kc) return r;
+    throw Error(PYFACC_ERR_INVALID, "internal: missing task range");
+  };
+  for (size_t k = 0; k < scans.size(); ++k) {
+    const Scan& sc = scans[k];
+    const Range& r = range_of(sc.bc, sc.kc);
+    sa.l[k] = BatchScanList{d + r.lo[sc.prec], d + r.hi[sc.prec], d + sc.toff, r.nb, kWidths[sc.wi]};
+  }
+  launch_batch_scans(sa, (int)scans.size(), stream);
+  std::vector<int> nt(scans.size());
+  std::vector<long long> nq(scans.size());
+  if (!scans.empty()) {
+    PF_CUDA(cudaMemcpyAsync(nt.data(), d_nt, nt.size() * sizeof(int), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaMemcpyAsync(nq.data(), d_nq, nq.size() * sizeof(long long), cudaMemcpyDeviceToHost, stream));
+  }
+  PF_CUDA(cudaStreamSynchronize(stream));
+  for (size_t k = 0; k < scans.size(); ++k) {
+    const Scan& sc = scans[k];
+    const Range& r = range_of(sc.bc, sc.kc);
+    TaskList& tl = tasks_w[sc.wi][sc.bc][sc.kc][sc.prec];
+    tl.width = kWidths[sc.wi];
+    tl.nbra = r.nb;
+    tl.ntasks = nt[k];
+    tl.nquartets = nq[k];
+    tl.ket_lo = d + r.lo[sc.prec];
+    tl.ket_hi = d + r.hi[sc.prec];
+    tl.task_off = d + sc.toff;
+  }
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
       const int q = qclass_index(bc, kc);
@@ -443,7 +532,9 @@ void Batch::build_tasks() {
       for (int p = 0; p < 3; ++p) tasks[bc][kc][p] = tasks_w[wi][bc][kc][p];
       timing.width[q] = w;
     }
-  PF_CUDA(cudaStreamSynchronize(stream));
+  if (opt.verbose)
+    std::fprintf(stderr, "pyfacc batch tasks (ms): layout %.2f  device build %.2f (%.1f MB, %zu lists)\n", tt1 - tt0,
+                 wall_ms() - tt1, (double)bytes / 1048576.0, scans.size());
 }
 
 void Batch::alloc() {

@@ -80,6 +80,38 @@ void launch_batch_wdens(int nmol, const BatchDenseArgs& a, double* out, cudaStre
 void launch_batch_dmax(int nmol, int ns_max, const int4* mt, const int* bf_off, const int* nfun, const double* D,
                        float* dm, cudaStream_t s);
 
+// Device-built task lists (batch_tasks.cu).  A range list covers one
+// (bra class, ket class) combination: per bra its ket range [lo, hi) for the
+// full list (0), the FP64 part (1) and the FP32 part (2) of mixed precision.
+struct BatchRangeList {
+  int bra_base, ket_base, nb, same;
+  const int* seg_b;  // nmol + 1 offsets of the molecules' bra pairs (relative to the class start)
+  const int* seg_k;  // the same for the ket class
+  int* lo[3];
+  int* hi[3];
+};
+struct BatchRangeArgs {
+  BatchRangeList l[NQCLASS];
+  const double4* geom;  // .w = Schwarz factor Q of the pair
+  const int4* info2;    // .z = molecule of the pair
+  double thresh, fp32_thresh;
+};
+// One task list: offsets of ceil((hi - lo) / width) tasks per bra.
+struct BatchScanList {
+  const int* lo;
+  const int* hi;
+  int* toff;  // nb + 1
+  int nb, width;
+};
+constexpr int BATCH_MAX_SCANS = NQCLASS * 3 * 3;
+struct BatchScanArgs {
+  BatchScanList l[BATCH_MAX_SCANS];
+  int* ntasks;           // per list
+  long long* nquartets;  // per list
+};
+void launch_batch_ranges(const BatchRangeArgs& a, int nlists, int nb_max, cudaStream_t s);
+void launch_batch_scans(const BatchScanArgs& a, int nlists, cudaStream_t s);
+
 struct BatchMolHost {
   int natoms = 0, nbf = 0, ns = 0, nalpha = 0, nbeta = 0, nocc = 0;
   int atom_off = 0, shell_off = 0;
