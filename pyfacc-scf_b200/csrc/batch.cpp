@@ -9,6 +9,7 @@
 #include <chrono>
 #include <thread>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -142,8 +143,8 @@ Batch::Batch(const std::vector<BatchMolHost>& ms, const pyfacc_options& o) : opt
 Batch::~Batch() {
   cudaSetDevice(device);
   if (stream) cudaStreamSynchronize(stream);
-  if (graph_full) cudaGraphExecDestroy(graph_full);
-  if (graph_inc) cudaGraphExecDestroy(graph_inc);
+  for (auto& g : graphs)
+    if (g) cudaGraphExecDestroy(g);
   context_release(ctx);
 }
 
@@ -553,7 +554,7 @@ void Batch::alloc() {
   const size_t o_dmax = carve((size_t)nmol * ns_max * ns_max * sizeof(float));
   const size_t o_stats = carve(sizeof(JkStats) + 2 * NQCLASS * sizeof(unsigned long long));
   const size_t o_grad = carve(3 * (size_t)natoms_tot * sizeof(double));
-  const size_t o_act = carve(sizeof(int));
+  const size_t o_act = carve(sizeof(StepReport));
   mats.ensure(o);
   char* b = mats.as<char>();
   double* mp[nmat];
@@ -610,12 +611,16 @@ void Batch::alloc() {
   a.eps_diis = opt.eps_diis;
   a.eps_density = opt.eps_density;
   a.active = active_dev;
+  a.max_err = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(active_dev) +
+                                                    offsetof(StepReport, max_err));
+  a.built_full = 1;
+  a.coarse = 0;
   a.smem_nmax = nbf_max;  // nbf <= 160: at most 200 KB of shared memory
   batch_set_smem(a);
   PF_CUDA(cudaStreamSynchronize(stream));
 }
 
-void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stats) {
+void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32) {
   launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.Db, dmax, stream);
   JkArgs a;
   a.Dj = dargs.Db;
@@ -631,7 +636,9 @@ void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stat
   a.prim_thresh = thresh * PRIM_QUARTET_REL;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
-      if (mixed_lists) {
+      if (all_fp32) {
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, true, 1, a, num_sms, stream);
+      } else if (mixed_lists) {
         launch_jk(pd, tasks[bc][kc][1], bc, kc, false, 1, a, num_sms, stream);
         launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, stream);
       } else {
@@ -727,18 +734,28 @@ void Batch::tune() {
 // One SCF iteration of the batch as a CUDA graph: density maxima of Db, the
 // J/K class kernels (full builds screen at schwarz_thresh, incremental ones
 // at incremental_thresh), the count reset and the dense step.
-cudaGraphExec_t Batch::capture(bool full, long long* launches) {
+cudaGraphExec_t Batch::capture(int variant, long long* launches) {
   const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
   const double inc_thresh = (mixed && opt.incremental_thresh > 0)
                                 ? std::max(opt.incremental_thresh, opt.schwarz_thresh)
                                 : opt.schwarz_thresh;
+  const bool full = variant == G_FULL || variant == G_CFULL;
+  const bool coarse = variant == G_CFULL || variant == G_CINC;
+  BatchDenseArgs da = dargs;
+  da.built_full = full ? 1 : 0;
+  da.coarse = coarse ? 1 : 0;
+  const double thresh =
+      coarse ? std::max(COARSE_SCREEN, opt.schwarz_thresh) : (full ? opt.schwarz_thresh : inc_thresh);
   const long long c0 = launch_count();
   cudaGraph_t g = nullptr;
   PF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
   try {
-    fock_build(mixed, full ? opt.schwarz_thresh : inc_thresh, stats_dev);
-    PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(int), stream));
-    launch_batch_step(nmol, dargs, stream);
+    // a full rebuild of an incremental run builds P itself (the previous
+    // step left P_new - P in Db); the first full build has Db = P already
+    if (variant == G_FULL && dargs.incremental) launch_batch_full_density(nmol, da, stream);
+    fock_build(mixed, thresh, stats_dev, coarse);
+    PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(StepReport), stream));
+    launch_batch_step(nmol, da, stream);
   } catch (...) {
     cudaStreamEndCapture(stream, &g);
     if (g) cudaGraphDestroy(g);
@@ -785,16 +802,40 @@ void Batch::run(bool gradient) {
   // ---- task widths, graphs
   if (opt.task_width == 0) tune();
   const double ts = wall_ms();
-  if (!graph_full) graph_full = capture(true, &graph_launches[0]);
-  if (dargs.incremental && !graph_inc) graph_inc = capture(false, &graph_launches[1]);
-  int it = 0;
+  // Mixed precision starts with all-FP32 builds while the largest DIIS error
+  // of the batch is above coarse_err (dynamic precision, as the single-
+  // molecule engine); the next build is a full mixed one, which restarts the
+  // incremental chain.
+  bool coarse = mixed && dargs.incremental && opt.coarse_err > 0;
+  if (!graphs[G_FULL]) graphs[G_FULL] = capture(G_FULL, &graph_launches[G_FULL]);
+  if (dargs.incremental && !graphs[G_INC]) graphs[G_INC] = capture(G_INC, &graph_launches[G_INC]);
+  if (coarse && !graphs[G_CFULL]) graphs[G_CFULL] = capture(G_CFULL, &graph_launches[G_CFULL]);
+  if (coarse && !graphs[G_CINC]) graphs[G_CINC] = capture(G_CINC, &graph_launches[G_CINC]);
+  int it = 0, since_full = 0;
+  bool restart = false;
   for (it = 1; it <= dargs.max_iter; ++it) {
-    const bool full = !dargs.incremental || it == 1 || ((it - 1) % dargs.rebuild_every) == 0;
-    PF_CUDA(cudaGraphLaunch(full ? graph_full : graph_inc, stream));
-    count_launches(full ? graph_launches[0] : graph_launches[1]);
-    PF_CUDA(cudaMemcpyAsync(&active_host, active_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    int v;
+    if (coarse) {
+      v = it == 1 ? G_CFULL : G_CINC;
+    } else {
+      const bool full = !dargs.incremental || it == 1 || restart || since_full + 1 >= dargs.rebuild_every;
+      v = full ? G_FULL : G_INC;
+      since_full = full ? 0 : since_full + 1;
+      restart = false;
+    }
+    PF_CUDA(cudaGraphLaunch(graphs[v], stream));
+    count_launches(graph_launches[v]);
+    PF_CUDA(cudaMemcpyAsync(&report, active_dev, sizeof(StepReport), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
-    if (active_host == 0) break;
+    if (report.active == 0) break;
+    if (coarse) {
+      double err;
+      std::memcpy(&err, &report.max_err, sizeof(err));
+      if (err < opt.coarse_err || it >= COARSE_MAX_ITER) {
+        coarse = false;
+        restart = true;
+      }
+    }
   }
   timing.iterations = std::min(it, dargs.max_iter);
   timing.ms_scf = wall_ms() - ts;

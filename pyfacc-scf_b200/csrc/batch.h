@@ -53,6 +53,11 @@ struct BatchDenseArgs {
   double e_tol, eps_diis, eps_density;
   int* active;     // molecules still iterating after this step (atomic count)
   int smem_nmax;   // molecules with nbf <= smem_nmax keep the TC2 iterate in shared memory
+  // per graph variant: the build just done was a full one (J, K replaced,
+  // not accumulated); it was an all-FP32 build of the first iterations
+  // (no molecule may converge on it)
+  int built_full, coarse;
+  unsigned long long* max_err;  // largest DIIS error of the step (bits of a non-negative double)
 };
 
 // X = S^{-1/2} of every molecule (coupled Newton-Schulz), into Xout; F, T1..T3
@@ -68,6 +73,8 @@ void launch_batch_guess(int nmol, const BatchDenseArgs& a, const double* occ, cu
 void launch_batch_init(int nmol, const BatchDenseArgs& a, int core_guess, cudaStream_t s);
 // One SCF step after a J/K build of Db into Jd/Kd.
 void launch_batch_step(int nmol, const BatchDenseArgs& a, cudaStream_t s);
+// Db = P of every molecule still iterating (before a full rebuild).
+void launch_batch_full_density(int nmol, const BatchDenseArgs& a, cudaStream_t s);
 // Db = P of the finished molecules (0 for the others) before the FP64 polish build.
 void launch_batch_polish_density(int nmol, const BatchDenseArgs& a, cudaStream_t s);
 // F and E of the final density after a full FP64 build (mixed precision);
@@ -175,10 +182,17 @@ class Batch {
   float* dmax = nullptr;
   unsigned long long* stats_dev = nullptr;
   double* grad_dev = nullptr;
-  int* active_dev = nullptr;
-  int active_host = 0;          // copy of *active_dev after each iteration
-  cudaGraphExec_t graph_full = nullptr, graph_inc = nullptr;
-  long long graph_launches[2] = {0, 0};   // kernels per replay of graph_full / graph_inc
+  int* active_dev = nullptr;     // followed by the step's largest DIIS error (8 bytes further)
+  struct StepReport {
+    int active;                  // molecules still iterating after the step
+    int pad;
+    unsigned long long max_err;  // bits of the largest DIIS error
+  } report{};
+  // iteration graphs: full and incremental builds, and the all-FP32 full
+  // and incremental builds of the first mixed iterations
+  enum { G_FULL, G_INC, G_CFULL, G_CINC, G_N };
+  cudaGraphExec_t graphs[G_N] = {nullptr, nullptr, nullptr, nullptr};
+  long long graph_launches[G_N] = {0, 0, 0, 0};  // kernels per replay
   std::vector<BatchMolState> st_host;
   std::vector<double> grad_host;
   std::vector<double> occ_host;          // atomic-occupation guess, all molecules' diagonals
@@ -189,11 +203,12 @@ class Batch {
   void build_tasks();
   void alloc();
   // J/K of Db into Jd/Kd: FP64 lists, or the FP64 + FP32 halves of mixed mode
-  void fock_build(bool mixed_lists, double thresh, unsigned long long* stats);
+  // (all_fp32: every quartet of the full lists in FP32, the coarse builds)
+  void fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32 = false);
   bool tuned_widths(std::array<int, NQCLASS>* w) const;  // cached tuner result for this batch shape
   std::string tune_key() const;
   void tune();
-  cudaGraphExec_t capture(bool full, long long* launches);
+  cudaGraphExec_t capture(int variant, long long* launches);
   void gradient_run();
 };
 

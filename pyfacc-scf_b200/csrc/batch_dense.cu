@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_step_kernel(const BatchDe
   const int n = p.n, n2 = p.n2;
   const int it = st.iter + 1;
   const double E_prev = st.E_prev, dD_prev = st.dD;
-  const bool built_full = !a.incremental || it == 1 || ((it - 1) % a.rebuild_every) == 0;
+  const bool built_full = a.built_full != 0;
   // ---- J, K (J = Jh + Jh^T of the build), F and the energy of P
   double e = 0.0;
   for (int idx = threadIdx.x; idx < n2; idx += blockDim.x) {
@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_step_kernel(const BatchDe
   for (int idx = threadIdx.x; idx < n2; idx += blockDim.x) em = fmax(em, fabs(p.T1[idx]));
   em = blk_reduce(em, true);
   const double dE = fabs(E - E_prev);
-  bool conv = dE < a.e_tol && em < a.eps_diis;
+  if (threadIdx.x == 0 && a.max_err) atomicMax(a.max_err, (unsigned long long)__double_as_longlong(em));
+  bool conv = !a.coarse && dE < a.e_tol && em < a.eps_diis;
   if (a.eps_density > 0) conv = conv && it > 1 && dD_prev < a.eps_density;
   if (threadIdx.x == 0) {
     st.E = E;
@@ -468,8 +469,9 @@ __global__ void __launch_bounds__(BATCH_THREADS) batch_step_kernel(const BatchDe
     for (int idx = threadIdx.x; idx < n2; idx += blockDim.x) p.Db[idx] = 0.0;
     return;
   }
-  // ---- next build density: the full P for a full rebuild, else P_new - P
-  const bool next_full = !a.incremental || (it % a.rebuild_every) == 0;
+  // ---- next build density: P_new - P for an incremental build, else P_new
+  // (a full rebuild of an incremental run sets Db = P before its build)
+  const bool next_full = !a.incremental;
   double dd = 0.0;
   for (int idx = threadIdx.x; idx < n2; idx += blockDim.x) {
     const double pn = Pn[idx], diff = pn - p.P[idx];
@@ -559,6 +561,24 @@ void batch_set_smem(const BatchDenseArgs& a) {
   const int sm = (int)xs_bytes(a);
   PF_CUDA(cudaFuncSetAttribute(batch_init_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   PF_CUDA(cudaFuncSetAttribute(batch_step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+}
+
+__global__ void __launch_bounds__(BATCH_THREADS) batch_full_density_kernel(const BatchDenseArgs a) {
+  const int m = blockIdx.x;
+  const BatchMolState& st = a.st[m];
+  if (st.done || st.failed) return;
+  const BatchMolDev d = a.mol[m];
+  const size_t n2 = (size_t)d.nbf * d.nbf;
+  const double* P = a.P + d.mat_off;
+  double* Db = a.Db + d.mat_off;
+  for (size_t idx = threadIdx.x; idx < n2; idx += blockDim.x) Db[idx] = P[idx];
+}
+
+void launch_batch_full_density(int nmol, const BatchDenseArgs& a, cudaStream_t s) {
+  if (nmol <= 0) return;
+  batch_full_density_kernel<<<nmol, BATCH_THREADS, 0, s>>>(a);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
 }
 
 void launch_batch_lowdin(int nmol, const BatchDenseArgs& a, double* Xout, cudaStream_t s) {

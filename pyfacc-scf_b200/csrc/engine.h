@@ -56,6 +56,10 @@ constexpr double PRIM_QUARTET_REL_GRAD = 1.0;
 // iterations (their error is discarded by the full build that ends them);
 // 1e-8 costs C100H202 an extra iteration
 constexpr double COARSE_SCREEN = 1e-9;
+// the all-FP32 phase ends after this many builds even if the DIIS error
+// stays above coarse_err (an oscillating start must still reach the
+// mixed builds, on which alone the SCF may converge)
+constexpr int COARSE_MAX_ITER = 20;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis

@@ -481,7 +481,7 @@ void System::run_scf() {
     const double e_tol = mixed ? std::max(opt.eps_energy, 1e-8) : opt.eps_energy;
     bool conv = !coarse_build && dE < e_tol && err < opt.eps_diis;
     if (opt.eps_density > 0) conv = conv && it > 1 && dD < opt.eps_density;
-    if (coarse && err < opt.coarse_err) {
+    if (coarse && (err < opt.coarse_err || it >= COARSE_MAX_ITER)) {
       coarse = false;
       restart = true;
     }
