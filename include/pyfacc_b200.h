@@ -68,15 +68,18 @@ typedef struct pyfacc_options {
                                chosen by timing for a batch            (0)   */
   int gradient_precision;   /* PYFACC_PRECISION_* of the derivative
                                integrals; MIXED evaluates the quartets with
-                               Q_ab Q_cd < fp32_thresh in FP32; -1 = MIXED for
-                               a mixed-precision SCF of >= 200 basis
-                               functions (where it is faster), else FP64 (-1) */
+                               Q_ab Q_cd (max|P|) below gradient_fp32_thresh
+                               in FP32; -1 = MIXED for a mixed-precision SCF
+                               of >= 200 basis functions and for every
+                               mixed-precision batch (where it is faster),
+                               else FP64                               (-1) */
   int polish;               /* mixed: energy and F of the converged density
                                from one more full FP64 build (1, |dE| vs
                                FP64 ~1e-12), or from the last incremental
                                mixed build (0, |dE| ~1e-8)              (0)   */
   double gradient_fp32_thresh; /* mixed gradient: derivative quartets with
-                               Q_ab Q_cd max|P| below this run in FP32
+                               Q_ab Q_cd max|P| (in a batch: Q_ab Q_cd)
+                               below this run in FP32
                                (|dG| ~3e-9 Ha/bohr at 1e-3 for C20H42..
                                C100H202); <= 0: fp32_thresh            (1e-3) */
   double coarse_err;        /* mixed: while the DIIS error is above this every

@@ -89,19 +89,22 @@ void launch_batch_dmax(int nmol, int ns_max, const int4* mt, const int* bf_off, 
 
 // Device-built task lists (batch_tasks.cu).  A range list covers one
 // (bra class, ket class) combination: per bra its ket range [lo, hi) for the
-// full list (0), the FP64 part (1) and the FP32 part (2) of mixed precision.
+// full list (0), the FP64 part (1) and the FP32 part (2) of mixed precision
+// (split at Q_bra Q_ket = fp32_thresh), and the FP64 (3) and FP32 (4) parts
+// of the mixed-precision gradient (split at grad_fp32_thresh).
+constexpr int BATCH_NPARTS = 5;
 struct BatchRangeList {
   int bra_base, ket_base, nb, same;
   const int* seg_b;  // nmol + 1 offsets of the molecules' bra pairs (relative to the class start)
   const int* seg_k;  // the same for the ket class
-  int* lo[3];
-  int* hi[3];
+  int* lo[BATCH_NPARTS];
+  int* hi[BATCH_NPARTS];
 };
 struct BatchRangeArgs {
   BatchRangeList l[NQCLASS];
   const double4* geom;  // .w = Schwarz factor Q of the pair
   const int4* info2;    // .z = molecule of the pair
-  double thresh, fp32_thresh;
+  double thresh, fp32_thresh, grad_fp32_thresh;
 };
 // One task list: offsets of ceil((hi - lo) / width) tasks per bra.
 struct BatchScanList {
@@ -110,7 +113,7 @@ struct BatchScanList {
   int* toff;  // nb + 1
   int nb, width;
 };
-constexpr int BATCH_MAX_SCANS = NQCLASS * 3 * 3;
+constexpr int BATCH_MAX_SCANS = NQCLASS * BATCH_NPARTS * 3;
 struct BatchScanArgs {
   BatchScanList l[BATCH_MAX_SCANS];
   int* ntasks;           // per list
@@ -173,8 +176,8 @@ class Batch {
   int4* mt_dev = nullptr;
   PairData pd;
   std::vector<int> seg[NCLASS];   // per class: nmol + 1 pair offsets (relative to the class start)
-  TaskList tasks_w[3][NCLASS][NCLASS][3];  // per width (32, 16, 8)
-  TaskList tasks[NCLASS][NCLASS][3];       // the widths in use
+  TaskList tasks_w[3][NCLASS][NCLASS][BATCH_NPARTS];  // per width (32, 16, 8)
+  TaskList tasks[NCLASS][NCLASS][BATCH_NPARTS];       // the widths in use
   DeviceBuf task_buf;
   DeviceBuf mats, state_buf;
   BatchDenseArgs dargs{};

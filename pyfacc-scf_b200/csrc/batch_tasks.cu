@@ -3,8 +3,9 @@
 // Pairs of a class are sorted by molecule, then by Schwarz factor Q
 // (descending), so the kets a bra reaches are a prefix of its molecule's
 // segment of the ket class: Q_bra Q_ket >= thresh, and in mixed precision
-// the FP64 part the prefix with Q_bra Q_ket >= fp32_thresh; for equal
-// classes only kets up to the bra itself are canonical.  One thread per bra
+// the FP64 part the prefix with Q_bra Q_ket >= fp32_thresh (for the
+// gradient, >= grad_fp32_thresh); for equal classes only kets up to the bra
+// itself are canonical.  One thread per bra
 // finds the prefixes by binary search (batch_ranges_kernel); one block per
 // (class combination, precision, task width) turns the ket ranges into task
 // offsets with a block-wide exclusive scan (batch_scan_kernel) and reports
@@ -38,6 +39,11 @@ __global__ void __launch_bounds__(256) batch_ranges_kernel(const BatchRangeArgs 
   int mm = q_prefix(A.geom, L.ket_base + ks, nk, qb, A.thresh);
   if (L.same) mm = min(mm, i - L.seg_b[m] + 1);
   const int m64 = min(q_prefix(A.geom, L.ket_base + ks, nk, qb, A.fp32_thresh), mm);
+  const int mg = min(q_prefix(A.geom, L.ket_base + ks, nk, qb, A.grad_fp32_thresh), mm);
+  L.lo[3][i] = ks;
+  L.hi[3][i] = ks + mg;
+  L.lo[4][i] = ks + mg;
+  L.hi[4][i] = ks + mm;
   L.lo[0][i] = ks;
   L.hi[0][i] = ks + mm;
   L.lo[1][i] = ks;
