@@ -70,9 +70,8 @@ typedef struct pyfacc_options {
                                integrals; MIXED evaluates the quartets with
                                Q_ab Q_cd (max|P|) below gradient_fp32_thresh
                                in FP32; -1 = MIXED for a mixed-precision SCF
-                               of >= 200 basis functions and for every
-                               mixed-precision batch (where it is faster),
-                               else FP64                               (-1) */
+                               (single molecules and batches), else FP64
+                                                                       (-1) */
   int polish;               /* mixed: energy and F of the converged density
                                from one more full FP64 build (1, |dE| vs
                                FP64 ~1e-12), or from the last incremental

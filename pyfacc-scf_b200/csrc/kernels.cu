@@ -220,10 +220,13 @@ template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
 // kernel's precision: double4 for FP64 quartets, float4 for FP32 ones).
 // Primitive pairs are stored in order of decreasing |K|, so with kcut > 0
 // both loops stop at the first primitive quartet with |K_ab K_cd| < kcut.
+// With kq_step > 1 only the ket primitives kq0, kq0 + kq_step, ... are
+// summed (a share of the quartet; the shares add up to the integral).
 template <typename R, int LA, int LB, int LC, int LD>
 __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __restrict__ prim, int4 bi0, int4 ki0,
                                                   const double4& bgeo, const double4& kgeo,
-                                                  R out[EriClass<R, LA, LB, LC, LD>::NOUT], double kcut = 0.0) {
+                                                  R out[EriClass<R, LA, LB, LC, LD>::NOUT], double kcut = 0.0,
+                                                  int kq0 = 0, int kq_step = 1) {
   using C = EriClass<R, LA, LB, LC, LD>;
   using V = typename Rec<R>::T;
   R acc[C::NACC];
@@ -234,7 +237,7 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
   const R cut = (R)kcut;
   const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
   int nprim = 0;
-  for (int kq = 0; kq < ki0.w; ++kq) {
+  for (int kq = kq0; kq < ki0.w; kq += kq_step) {
     const V* kr = prim + 3 * (size_t)(ki0.z + kq);
     const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
     const R kcd = fabs((R)k0.z);
@@ -408,7 +411,18 @@ struct JkKernelArgs {
   const int* ket_hi;
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec, task_begin;
   int lwidth;  // log2 of the task width: one warp runs 32 >> lwidth tasks of (1 bra) x (1 << lwidth kets)
+  int psplit;  // warps per task (each takes every psplit-th ket primitive)
 };
+
+// Warps per task for a list of the given length: lists with too few warps
+// to fill the GPU (the (pp|pp) class: one quartet per lane and up to 81
+// primitive quartets each) spread each task's ket primitives over up to 8
+// warps; the grid is then even, so that 4-warp blocks keep groups whole.
+static int primitive_split(long long warps, int num_sms) {
+  int ps = 1;
+  while (ps < 8 && warps * ps < (long long)num_sms * 32) ps *= 2;
+  return ps;
+}
 
 // Whether any lane of this lane's aligned group of w lanes is active.
 __device__ __forceinline__ bool active_any(unsigned mask, int lane, int w) {
@@ -435,7 +449,13 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
   const JkArgs& A = args.a;
   const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
   const int lw = args.lwidth, W = 1 << lw, sub = lane & (W - 1), tpw = 32 >> lw;
-  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < ntasks; tb += nw * tpw) {
+  // (pp|pp) only: a task is shared by psplit consecutive warps, each summing
+  // every psplit-th ket primitive and digesting its share (J and K are
+  // linear in the integrals); the other classes compile with a unit stride
+  constexpr bool kSplit = C::L == 4;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ps = kSplit ? args.psplit : 1, slice = kSplit ? gw % ps : 0;
+  for (int tb = (gw / ps) * tpw; tb < ntasks; tb += (nw / ps) * tpw) {
     const int tl = tb + (lane >> lw);
     const bool valid = tl < ntasks;
     const int t = args.task_begin + (valid ? tl : ntasks - 1);
@@ -464,7 +484,7 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     R out[C::NOUT];
     int nprim = 0;
     if (active) {
-      nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut);
+      nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut, slice, ps);
     } else {
 #pragma unroll
       for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
@@ -474,7 +494,7 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
       if (lane == 0) {
-        atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
+        if (slice == 0) atomicAdd(A.stats + args.prec * NQCLASS + args.qclass, (unsigned long long)__popc(amask));
         atomicAdd(A.stats + (2 + args.prec) * NQCLASS + args.qclass, tot);
       }
     }
@@ -640,7 +660,11 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   k.qclass = qclass_of(bc, kc);
   k.prec = fp32 ? 1 : 0;
   k.lwidth = width_log2(tl.width);
-  dim3 grid(grid_for((tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width), num_sms)), block(128);
+  const long long warps = (tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width);
+  k.psplit = k.qclass == NQCLASS - 1 ? primitive_split(warps, num_sms) : 1;
+  int nblk = grid_for((int)std::min<long long>(warps * k.psplit, 1LL << 30), num_sms);
+  nblk = (nblk + 1) / 2 * 2;
+  dim3 grid(nblk), block(128);
   if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, s, k);
   else jk_dispatch<double>(k.qclass, nk, grid, block, s, k);
   PF_CUDA(cudaGetLastError());
@@ -797,6 +821,7 @@ struct GradKernelArgs {
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, task_begin;
   int lwidth;
   int smem_atoms;  // atoms summed in shared memory (0: global atomics)
+  int psplit;      // warps per task: warp k of a group takes ket primitives k, k + psplit, ...
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
@@ -820,7 +845,11 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   if (nsm) __syncthreads();
   double* G = nsm ? gsh : A.grad;
   const int ntasks = args.ntasks_dev ? *args.ntasks_dev : args.ntasks;
-  for (int tb = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * tpw; tb < ntasks; tb += nw * tpw) {
+  // a task is shared by psplit consecutive warps (the gradient is a sum over
+  // primitive quartets, so each warp adds its share with the same atomics)
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int ps = args.psplit, slice = gw % ps;
+  for (int tb = (gw / ps) * tpw; tb < ntasks; tb += (nw / ps) * tpw) {
     const int tl = tb + (lane >> lw);
     const bool valid = tl < ntasks;
     const int t = args.task_begin + (valid ? tl : ntasks - 1);
@@ -884,7 +913,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const R cut = (R)kcut;
       const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
 #pragma unroll 1
-      for (int kq = 0; kq < ki0.w; ++kq) {
+      for (int kq = slice; kq < ki0.w; kq += ps) {
         const V* kr = prim + 3 * (size_t)(ki0.z + kq);
         const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
         const R kcd = fabs((R)k0.z);
@@ -919,7 +948,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
       if (lane == 0) {
-        atomicAdd(A.stats + args.qclass, (unsigned long long)__popc(amask));
+        if (slice == 0) atomicAdd(A.stats + args.qclass, (unsigned long long)__popc(amask));
         atomicAdd(A.stats + NQCLASS + args.qclass, tot);
       }
     }
@@ -987,7 +1016,12 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   // flush costs more than the contention it saves)
   k.smem_atoms = (a.natoms_total > 0 && a.natoms_total <= 256) ? a.natoms_total : 0;
   const size_t smem = 3 * (size_t)k.smem_atoms * sizeof(double);
-  dim3 grid(grid_for((tl.ntasks + (32 / tl.width) - 1) / (32 / tl.width), num_sms)), block(128);
+  const int tpw = 32 / tl.width;
+  const long long warps = (tl.ntasks + tpw - 1) / tpw;
+  k.psplit = primitive_split(warps, num_sms);
+  int nblk = grid_for((int)std::min<long long>(warps * k.psplit, 1LL << 30), num_sms);
+  nblk = (nblk + 1) / 2 * 2;
+  dim3 grid(nblk), block(128);
   if (fp32) grad2e_dispatch<float>(k.qclass, grid, block, smem, s, k);
   else grad2e_dispatch<double>(k.qclass, grid, block, smem, s, k);
   PF_CUDA(cudaGetLastError());
@@ -1038,6 +1072,7 @@ void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bc, int kc, i
                        cudaStream_t s) {
   if (tl.ntasks <= 0) return;
   JkKernelArgs k{};
+  k.psplit = 1;
   k.info0 = pd.info0; k.info1 = pd.info1; k.info2 = pd.info2;
   k.geom = pd.geom; k.prim = pd.prim;
   k.task_off = tl.task_off; k.ket_lo = tl.ket_lo; k.ket_hi = tl.ket_hi;
