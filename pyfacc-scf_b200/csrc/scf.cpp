@@ -205,8 +205,11 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
   // one cuBLAS DGEMM + one update kernel per step, the state double-buffered
-  // on the device, four steps per graph replay; the host checks after 16
-  // steps, then every 4 (converged steps only copy X)
+  // on the device, four steps per graph replay; the host checks first after
+  // as many steps as the last purification of this occupation took (16 the
+  // first time), then every 4 (converged steps only copy X).  Successive SCF
+  // iterations need about the same number of steps, so most purifications
+  // cost one host round trip instead of four.
   double* S0 = pstate;
   launch_gersh(nbf, Fp, S0, stream);
   launch_tc2_init(nbf, Fp, S0, Xa, stream);
@@ -215,8 +218,16 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   double st_h[8] = {0};
   bool ok = false;
   int k = 0;
+  int* last = nullptr;
+  for (auto& e : tc2_last)
+    if (e.first == nocc) last = &e.second;
+  if (!last) {
+    tc2_last.emplace_back(nocc, 16);
+    last = &tc2_last.back().second;
+  }
+  const int first = std::min(std::max((*last + 3) / 4 * 4, 4), 64);
   while (k < kmax) {
-    const int chunk = (k == 0) ? 16 : 4;
+    const int chunk = (k == 0) ? first : 4;
     for (int j = 0; j < chunk; j += 4, k += 4) {
       PF_CUDA(cudaGraphLaunch(g4, stream));
       count_launches(4);
@@ -230,6 +241,7 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   }
   purify_steps += (int)st_h[5];
   if (!ok) return false;
+  *last = (int)st_h[5];
   const double* Xp = Xa;  // after a multiple of four steps the iterate is back in Xa
   // P = scale * X Xp X^T
   PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));

@@ -84,6 +84,7 @@ struct System {
   // four TC2 steps (cuBLAS DGEMM + update, ping-pong buffers) as one CUDA
   // graph per occupation number, replayed by purify() for nbf > 192
   std::vector<std::pair<int, cudaGraphExec_t>> tc2_graphs;
+  std::vector<std::pair<int, int>> tc2_last;  // per occupation number: TC2 steps of the last purification
   cudaGraphExec_t tc2_graph(int nocc);
   int syev_lwork = 0;
 

@@ -206,6 +206,36 @@ def test_mixed_precision_delta_e(engine):
     assert np.abs(emx.gradient - e64.gradient).max() <= 1e-5
 
 
+@pytest.mark.parametrize("coarse_err", [0.0, 1e-3, 1e-1])
+def test_mixed_coarse_phase(engine, coarse_err):
+    """The all-FP32 builds of the first mixed iterations only shorten the
+    way to the converged density: with the phase off (0), at its default
+    and ended early, energy and gradient stay within the mixed-precision
+    budget of FP64, and gradient FP32 splitting keeps translational
+    invariance."""
+    from pyfacc import geometry as G
+    mol = engine.Molecule(*G.alkane(12, seed=3))
+    e64 = engine.run(mol, gradient=True)
+    emx = engine.run(mol, precision="mixed", gradient=True, coarse_err=coarse_err)
+    assert emx.converged
+    assert abs(emx.energy - e64.energy) <= 1e-6
+    assert np.abs(emx.gradient - e64.gradient).max() <= 1e-5
+    assert np.abs(emx.gradient.sum(0)).max() < 1e-8
+
+
+def test_batch_mixed_coarse_phase(engine):
+    from pyfacc import geometry as G
+    clusters = G.water_clusters(count=6, seed=5)
+    mols = [engine.Molecule(sp, xyz) for sp, xyz in clusters]
+    ref = engine.run_batch(mols, gradient=True)
+    for ce in (0.0, 1e-3):
+        r = engine.run_batch(mols, gradient=True, precision="mixed", coarse_err=ce)
+        for a, b in zip(r, ref):
+            assert a.converged
+            assert abs(a.energy - b.energy) <= 1e-6
+            assert np.abs(a.gradient - b.gradient).max() <= 1e-5
+
+
 def test_autograd_energy(engine):
     import torch
     em, _ = _h2o(engine, __import__("oracle"))
