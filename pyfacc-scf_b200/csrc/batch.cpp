@@ -236,59 +236,49 @@ void Batch::upload() {
 void Batch::build_pairs() {
   double tp[8];
   tp[0] = wall_ms();
-  std::vector<int4> pl0[NCLASS], pl1[NCLASS];
-  std::vector<int> pm[NCLASS];
-  {
-    size_t cnt[NCLASS] = {0, 0, 0};
-    for (const auto& M : mols) {
-      int nl[2] = {0, 0};
-      for (const auto& sh : M.basis.shells) nl[sh.l > 0 ? 1 : 0]++;
-      cnt[0] += (size_t)nl[0] * (nl[0] + 1) / 2;
-      cnt[1] += (size_t)nl[0] * nl[1];
-      cnt[2] += (size_t)nl[1] * (nl[1] + 1) / 2;
-    }
-    for (int c = 0; c < NCLASS; ++c) {
-      pl0[c].reserve(cnt[c]);
-      pl1[c].reserve(cnt[c]);
-      pm[c].reserve(cnt[c]);
-    }
-  }
-  std::vector<int> nprim_of(ns_tot);
-  for (int m = 0; m < nmol; ++m)
-    for (int s = 0; s < mols[m].ns; ++s) nprim_of[mols[m].shell_off + s] = (int)mols[m].basis.shells[s].ex.size();
+  // pairs of class c of molecule m occupy [moff[c][m], moff[c][m + 1]) of
+  // the class-major list, in (i, j <= i) shell order (as one molecule's
+  // engine lists them); every molecule fills its own ranges
+  std::vector<int> moff[NCLASS];
+  int off[NCLASS + 1] = {0, 0, 0, 0};
+  for (int c = 0; c < NCLASS; ++c) moff[c].assign(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) {
+    int nl[2] = {0, 0};
+    for (const auto& sh : mols[m].basis.shells) nl[sh.l > 0 ? 1 : 0]++;
+    moff[0][m + 1] = nl[0] * (nl[0] + 1) / 2;
+    moff[1][m + 1] = nl[0] * nl[1];
+    moff[2][m + 1] = nl[1] * (nl[1] + 1) / 2;
+  }
+  for (int c = 0; c < NCLASS; ++c) {
+    moff[c][0] = off[c];
+    for (int m = 0; m < nmol; ++m) moff[c][m + 1] += moff[c][m];
+    off[c + 1] = moff[c][nmol];
+  }
+  const int np_all = off[NCLASS];
+  std::vector<int4> all0(np_all), all1(np_all);
+  std::vector<int> allm(np_all);
+  std::vector<long long> np_of(np_all);  // primitive pairs of each pair
+  parallel_for(nmol, [&](int m) {
     const BatchMolHost& M = mols[m];
+    int pos[NCLASS] = {moff[0][m], moff[1][m], moff[2][m]};
     for (int i = 0; i < M.ns; ++i)
       for (int j = 0; j <= i; ++j) {
         int a = i, b = j;
         if (M.basis.shells[a].l < M.basis.shells[b].l) std::swap(a, b);
         const int c = M.basis.shells[a].l + M.basis.shells[b].l;
-        pl0[c].push_back(make_int4(M.shell_off + a, M.shell_off + b, 0, M.shell_off));
-        pl1[c].push_back(make_int4((int)M.mat_off, M.nbf, m, m * ns_max * ns_max));
-        pm[c].push_back(m);
+        const int k = pos[c]++;
+        all0[k] = make_int4(M.shell_off + a, M.shell_off + b, 0, M.shell_off);
+        all1[k] = make_int4((int)M.mat_off, M.nbf, m, m * ns_max * ns_max);
+        allm[k] = m;
+        np_of[k] = (long long)M.basis.shells[a].ex.size() * (long long)M.basis.shells[b].ex.size();
       }
-  }
-  std::vector<int4> all0, all1;
-  std::vector<int> allm;
-  const size_t np_total = pl0[0].size() + pl0[1].size() + pl0[2].size();
-  all0.reserve(np_total);
-  all1.reserve(np_total);
-  allm.reserve(np_total);
-  int off[NCLASS + 1] = {0, 0, 0, 0};
+  });
   long long nprim_tot = 0;
-  for (int c = 0; c < NCLASS; ++c) {
-    off[c + 1] = off[c] + (int)pl0[c].size();
-    for (size_t k = 0; k < pl0[c].size(); ++k) {
-      int4 p = pl0[c][k];
-      p.z = (int)nprim_tot;
-      nprim_tot += (long long)nprim_of[p.x] * nprim_of[p.y];
-      all0.push_back(p);
-      all1.push_back(pl1[c][k]);
-      allm.push_back(pm[c][k]);
-    }
+  for (int k = 0; k < np_all; ++k) {
+    all0[k].z = (int)std::min<long long>(nprim_tot, INT32_MAX);
+    nprim_tot += np_of[k];
   }
   if (nprim_tot >= (1LL << 31)) throw Error(PYFACC_ERR_INVALID, "batch too large: split it into several calls");
-  const int np_all = off[NCLASS];
   size_t o = 0;
   auto carve = [&](size_t bytes) {
     size_t r = o;
@@ -336,44 +326,51 @@ void Batch::build_pairs() {
   std::vector<double> qmax(nmol, 0.0);
   for (int k = 0; k < np_all; ++k) qmax[allm[k]] = std::max(qmax[allm[k]], q[k]);
   const double thr = opt.schwarz_thresh;
-  std::vector<int> perm, new_ps;
-  pd.class_off[0] = 0;
-  long long nprim_new = 0;
+  // every (class, molecule) segment: the pairs that pass the screening,
+  // sorted by Q (descending; ties by index, deterministic), then the
+  // segments concatenated class by class, molecule by molecule
+  const int nseg = NCLASS * nmol;
+  std::vector<int> sorted(np_all), cnt(nseg);
+  std::vector<long long> psum(nseg);
+  parallel_for(nseg, [&](int g) {
+    const int c = g / nmol, m = g % nmol;
+    int* out = sorted.data() + moff[c][m];
+    int n = 0;
+    for (int k = moff[c][m]; k < moff[c][m + 1]; ++k)
+      if (thr <= 0 || q[k] * qmax[m] >= thr) out[n++] = k;
+    std::sort(out, out + n, [&](int x, int y) { return q[x] > q[y] || (q[x] == q[y] && x < y); });
+    long long ps = 0;
+    for (int i = 0; i < n; ++i) ps += kept[out[i]];
+    cnt[g] = n;
+    psum[g] = ps;
+  });
+  std::vector<int> pos(nseg + 1, 0);
+  std::vector<long long> ppos(nseg + 1, 0);
+  for (int g = 0; g < nseg; ++g) {
+    pos[g + 1] = pos[g] + cnt[g];
+    ppos[g + 1] = ppos[g] + psum[g];
+  }
+  for (int c = 0; c < NCLASS; ++c) {
+    pd.class_off[c] = pos[c * nmol];
+    seg[c].assign(nmol + 1, 0);
+    for (int m = 0; m <= nmol; ++m) seg[c][m] = pos[c * nmol + m] - pos[c * nmol];
+  }
+  pd.class_off[NCLASS] = pos[nseg];
+  std::vector<int> perm(pos[nseg]), new_ps(pos[nseg]);
+  parallel_for(nseg, [&](int g) {
+    const int c = g / nmol, m = g % nmol;
+    const int* in = sorted.data() + moff[c][m];
+    long long pp = ppos[g];
+    for (int i = 0; i < cnt[g]; ++i) {
+      perm[pos[g] + i] = in[i];
+      new_ps[pos[g] + i] = (int)pp;
+      pp += kept[in[i]];
+    }
+  });
+  const long long nprim_new = ppos[nseg];
   pd.q_host.clear();
   pd.cls_host.clear();
   pd.mol_host.clear();
-  for (int c = 0; c < NCLASS; ++c) {
-    // the pairs of a class are generated molecule by molecule: sort each
-    // molecule's segment by Q (descending; ties by index, deterministic)
-    std::vector<int> idx;
-    idx.reserve(off[c + 1] - off[c]);
-    for (int k = off[c]; k < off[c + 1]; ++k)
-      if (thr <= 0 || q[k] * qmax[allm[k]] >= thr) idx.push_back(k);
-    std::vector<size_t> starts;
-    for (size_t a = 0; a < idx.size();) {
-      starts.push_back(a);
-      size_t b = a;
-      while (b < idx.size() && allm[idx[b]] == allm[idx[a]]) ++b;
-      a = b;
-    }
-    starts.push_back(idx.size());
-    parallel_for((int)starts.size() - 1, [&](int g) {
-      std::sort(idx.begin() + starts[g], idx.begin() + starts[g + 1],
-                [&](int x, int y) { return q[x] > q[y] || (q[x] == q[y] && x < y); });
-    });
-    seg[c].assign(nmol + 1, 0);
-    for (int k : idx) {
-      perm.push_back(k);
-      new_ps.push_back((int)nprim_new);
-      nprim_new += kept[k];
-      pd.q_host.push_back(q[k]);
-      pd.cls_host.push_back(c);
-      pd.mol_host.push_back(allm[k]);
-      seg[c][allm[k] + 1]++;
-    }
-    for (int m = 0; m < nmol; ++m) seg[c][m + 1] += seg[c][m];
-    pd.class_off[c + 1] = (int)perm.size();
-  }
   pd.npair = (int)perm.size();
   pd.nprim = (int)nprim_new;
   tp[4] = wall_ms();
