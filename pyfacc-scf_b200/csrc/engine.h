@@ -258,6 +258,8 @@ void launch_axpby(long long n, double a, const double* x, double b, double* y, c
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
                  cudaStream_t s);                                          // F = H + J - kf K
 void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s);
+// out = sum_k c[k] src[k] (m host-side pointers and coefficients, any m >= 1)
+void launch_lincomb(long long n, int m, const double* const* src, const double* c, double* out, cudaStream_t s);
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb,
                        const double* Fa, const double* Fb, const double* Ea, const double* Eb,
                        const double* Pa_old, const double* Pb_old, double* out, cudaStream_t s);

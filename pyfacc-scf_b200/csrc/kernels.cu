@@ -1490,6 +1490,38 @@ __global__ void dot_many_kernel(long long n, const double* __restrict__ x, const
   acc = block_sum(acc, sh);
   if (threadIdx.x == 0) out[blockIdx.x] = acc;
 }
+struct LinCombArgs {
+  const double* src[8];
+  double c[8];
+  int m, accumulate;
+};
+
+__global__ void lincomb_kernel(long long n, const LinCombArgs a, double* __restrict__ out) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double v = a.accumulate ? out[i] : 0.0;
+    for (int k = 0; k < a.m; ++k) v += a.c[k] * __ldg(a.src[k] + i);
+    out[i] = v;
+  }
+}
+
+void launch_lincomb(long long n, int m, const double* const* src, const double* c, double* out, cudaStream_t s) {
+  if (n <= 0 || m <= 0) return;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 4096);
+  for (int k0 = 0; k0 < m; k0 += 8) {  // eight terms per pass
+    LinCombArgs a{};
+    a.m = std::min(8, m - k0);
+    a.accumulate = k0 > 0;
+    for (int k = 0; k < a.m; ++k) {
+      a.src[k] = src[k0 + k];
+      a.c[k] = c[k0 + k];
+    }
+    lincomb_kernel<<<blocks, 256, 0, s>>>(n, a, out);
+    PF_CUDA(cudaGetLastError());
+    count_launch();
+  }
+}
+
 void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s) {
   if (m <= 0) return;
   dot_many_kernel<<<m, 512, 0, s>>>(n, x, ys, out);

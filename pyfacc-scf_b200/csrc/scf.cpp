@@ -348,6 +348,10 @@ void System::run_scf() {
   PF_CUDA(cudaEventCreate(&t1));
   PF_CUDA(cudaEventCreate(&a0));
   PF_CUDA(cudaEventCreate(&a1));
+  cudaEvent_t d0, d1;
+  PF_CUDA(cudaEventCreate(&d0));
+  PF_CUDA(cudaEventCreate(&d1));
+  bool diag_pending = false;
   PF_CUDA(cudaEventRecord(t0, stream));
   PF_CUDA(cudaEventRecord(a0, stream));
   one_electron();
@@ -383,6 +387,11 @@ void System::run_scf() {
   for (int k = 0; k < ndiis; ++k) {
     launch_zero(diis_F[k], 2 * n2 * sizeof(double), stream);
     launch_zero(diis_E[k], 2 * n2 * sizeof(double), stream);
+  }
+  if (ndiis > 0) {  // the stored error vectors, for the overlaps of each new one
+    std::vector<const double*> ys(ndiis);
+    for (int k = 0; k < ndiis; ++k) ys[k] = diis_E[k];
+    PF_CUDA(cudaMemcpyAsync(ptrs_dev, ys.data(), ndiis * sizeof(double*), cudaMemcpyHostToDevice, stream));
   }
   int nhist = 0, head = 0;
   std::vector<double> Bm;  // DIIS overlap matrix of the stored error vectors
@@ -466,14 +475,15 @@ void System::run_scf() {
         PF_CUDA(cudaMemcpyAsync(diis_F[slot] + s * n2, F[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         PF_CUDA(cudaMemcpyAsync(diis_E[slot] + s * n2, Err[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
       }
-      std::vector<const double*> ys(ndiis);
-      for (int k = 0; k < ndiis; ++k) ys[k] = diis_E[k];
-      PF_CUDA(cudaMemcpyAsync(ptrs_dev, ys.data(), ndiis * sizeof(double*), cudaMemcpyHostToDevice, stream));
       launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, stream);
     }
     double red[8 + 64];
     PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
+    if (diag_pending) {  // the previous iteration's density step, timed now
+      ms_diag += elapsed(d0, d1);
+      diag_pending = false;
+    }
     const float ms_build = elapsed(a0, a1);
     ms_fock += ms_build;
     const double E = 0.5 * red[0];
@@ -533,11 +543,12 @@ void System::run_scf() {
           if (solve_small(m + 1, A, b, x)) {
             // F_diis = sum c_i F_i  (into W3 / Wm as the stacked spins)
             double* Fd = W3;
-            launch_zero(Fd, n2 * sizeof(double), stream);
-            if (uhf) launch_zero(Wm, n2 * sizeof(double), stream);
-            for (int i = 0; i < m; ++i) {
-              launch_axpby((long long)n2, x[i], diis_F[use[i]], 1.0, Fd, stream);
-              if (uhf) launch_axpby((long long)n2, x[i], diis_F[use[i]] + n2, 1.0, Wm, stream);
+            std::vector<const double*> src(m);
+            for (int i = 0; i < m; ++i) src[i] = diis_F[use[i]];
+            launch_lincomb((long long)n2, m, src.data(), x.data(), Fd, stream);
+            if (uhf) {
+              for (int i = 0; i < m; ++i) src[i] = diis_F[use[i]] + n2;
+              launch_lincomb((long long)n2, m, src.data(), x.data(), Wm, stream);
             }
             Fuse[0] = Fd;
             Fuse[1] = Wm;
@@ -551,12 +562,17 @@ void System::run_scf() {
         }
       }
     }
-    // ---- diagonalise and rebuild the density
-    PF_CUDA(cudaEventRecord(a0, stream));
+    // ---- diagonalise and rebuild the density (timed at the next sync, so
+    // the host queues the next Fock build while this one runs)
+    PF_CUDA(cudaEventRecord(d0, stream));
     for (int s = 0; s < nsp; ++s) density_step(Fuse[s], nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
-    PF_CUDA(cudaEventRecord(a1, stream));
-    PF_CUDA(cudaStreamSynchronize(stream));
-    ms_diag += elapsed(a0, a1);
+    PF_CUDA(cudaEventRecord(d1, stream));
+    diag_pending = true;
+  }
+  if (diag_pending) {
+    PF_CUDA(cudaEventSynchronize(d1));
+    ms_diag += elapsed(d0, d1);
+    diag_pending = false;
   }
   if (mixed && st.converged && opt.polish) {
     // FP64 polish: F and E of the converged density from one full FP64 build
@@ -607,6 +623,8 @@ void System::run_scf() {
   cudaEventDestroy(t1);
   cudaEventDestroy(a0);
   cudaEventDestroy(a1);
+  cudaEventDestroy(d0);
+  cudaEventDestroy(d1);
 }
 
 // Analytic gradient of the converged SCF:
