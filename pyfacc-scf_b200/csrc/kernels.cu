@@ -840,6 +840,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
   // per-atom sums of the block in shared memory (one global add per atom
   // and block at the end) when the gradient is small enough
   extern __shared__ double gsh[];
+  constexpr bool kGamSmem = C::L >= 4;
   const int nsm = args.smem_atoms * 3;
   for (int i = threadIdx.x; i < nsm; i += blockDim.x) gsh[i] = 0.0;
   if (nsm) __syncthreads();
@@ -881,7 +882,12 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const size_t mo = (size_t)bi2.x;
       const int ld = bi2.y;
       const int ma = bi0.x, mb = bi0.y, mc = ki0.x, md = ki0.y;
-      R gam[C::NOUT];
+      // the (pp|pp) derivative routines are compiled out of line and read
+      // the density products through a pointer: for that class they live
+      // in shared memory (after the per-atom sums) rather than in local
+      // memory, which spilled to DRAM
+      R gam_reg[kGamSmem ? 1 : C::NOUT];
+      R* gam = kGamSmem ? reinterpret_cast<R*>(gsh + nsm) + (size_t)threadIdx.x * C::NOUT : gam_reg;
 #pragma unroll
       for (int a = 0; a < NA; ++a)
 #pragma unroll
@@ -1015,7 +1021,9 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   // up to 256 atoms (6 KB of per-block sums; above that the end-of-block
   // flush costs more than the contention it saves)
   k.smem_atoms = (a.natoms_total > 0 && a.natoms_total <= 256) ? a.natoms_total : 0;
-  const size_t smem = 3 * (size_t)k.smem_atoms * sizeof(double);
+  // the (pp|pp) kernels keep each thread's density products in shared memory
+  const size_t gam_bytes = k.qclass == NQCLASS - 1 ? 128 * 81 * (fp32 ? sizeof(float) : sizeof(double)) : 0;
+  const size_t smem = 3 * (size_t)k.smem_atoms * sizeof(double) + gam_bytes;
   const int tpw = 32 / tl.width;
   const long long warps = (tl.ntasks + tpw - 1) / tpw;
   k.psplit = primitive_split(warps, num_sms);
