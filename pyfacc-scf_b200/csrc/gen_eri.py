@@ -213,11 +213,59 @@ def gen_class(la, lb, lc, ld):
     src.extend(out_lines)
     src.append("    (void)AB; (void)CD;")
     src.append("  }")
-    # --- gradient (primitive level, contracted with gam), one routine per
-    # centre and direction so that each keeps only its own recursion
-    # intermediates live; grad{A,B,C} call the three directions in turn
+    # --- gradient (primitive level, contracted with gam).  Below L = 4 one
+    # inlined routine per centre and direction (the compiler merges their
+    # common recursion terms); from L = 4 on one out-of-line routine per
+    # centre whose three directions share one recursion to L + 1 (half the
+    # operations of three separate ones; inlined, the (pp|pp) body exhausts
+    # the register file)
     grad_flops = 0
-    for ctr in range(3):
+    for ctr in range(3 if L >= 4 else 0):
+        em = Emitter()
+        v = Vrr(em, L + 1)
+        h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
+        outs = []
+        for x in range(3):
+            up_terms, dn_terms = [], []
+            k = 0
+            for a in comps(la):
+                for b in comps(lb):
+                    for c in comps(lc):
+                        for d in comps(ld):
+                            q = [a, b, c, d]
+                            qu = list(q)
+                            qu[ctr] = up(q[ctr], x)
+                            up_terms.append(f"gam[{k}] * {h.full(*qu)}")
+                            cnt = q[ctr][x]
+                            if cnt > 0:
+                                qd = list(q)
+                                qd[ctr] = down(q[ctr], x)
+                                cc = f"{cnt}.0 * " if cnt > 1 else ""
+                                dn_terms.append(f"{cc}gam[{k}] * {h.full(*qd)}")
+                            k += 1
+            su = em.tmp(" + ".join(up_terms), 2 * len(up_terms) - 1)
+            expr = f"tw * {su}"
+            fl = 2
+            if dn_terms:
+                sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
+                expr += f" - {sd}"
+                fl += 1
+            em.flops += fl
+            outs.append(expr)
+        grad_flops += em.flops
+        c = 'ABC'[ctr]
+        src.append(f"  // centre {c}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
+        src.append(f"  __device__ static __noinline__ void grad{c}(const R* __restrict__ I, const R* __restrict__ PA,")
+        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
+        src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+        src.append("      R tw, const R* __restrict__ gam, R* __restrict__ g) {")
+        src.extend(em.lines)
+        for x in range(3):
+            src.append(f"    g[{x}] += {outs[x]};")
+        src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+        src.append("    (void)AB; (void)CD;")
+        src.append("  }")
+    for ctr in range(0 if L >= 4 else 3):
         for x in range(3):
             em = Emitter()
             v = Vrr(em, L + 1)
@@ -249,10 +297,7 @@ def gen_class(la, lb, lc, ld):
             em.flops += fl
             grad_flops += em.flops
             name = f"grad{'ABC'[ctr]}{'xyz'[x]}"
-            # the (pp|pp) routines are large enough that one inlined body
-            # exhausts the register file; compiled separately they do not
-            inl = "__noinline__" if L >= 4 else "__forceinline__"
-            src.append(f"  __device__ static {inl} R {name}(const R* __restrict__ I, const R* __restrict__ PA,")
+            src.append(f"  __device__ static __forceinline__ R {name}(const R* __restrict__ I, const R* __restrict__ PA,")
             src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
             src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
             src.append("      R tw, const R* __restrict__ gam) {")
