@@ -112,3 +112,22 @@ def test_batch_repeat_is_reproducible(engine):
     for x, y in zip(a, b):
         assert x.energy == pytest.approx(y.energy, abs=1e-9)
         assert x.n_iter == y.n_iter
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_s_only_molecules(engine, precision):
+    """Molecules without p shells (H2, He2) leave the sp and pp classes of
+    their segments empty; in a batch of only such molecules those task lists
+    are empty altogether.  Both batches must match the one-by-one runs."""
+    from pyfacc import geometry as G
+    h2 = (["H", "H"], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 1.40]]))       # bohr
+    he2 = (["He", "He"], np.array([[0.0, 0.0, 0.0], [0.0, 0.0, 5.6]]))
+    h2b = (["H", "H"], np.array([[0.1, 0.0, 0.0], [0.0, 0.2, 1.45]]))
+    for clusters in ([h2, he2, h2b], [h2, G.water(), he2]):
+        mols = _mols(engine, clusters)
+        rb = engine.run_batch(mols, gradient=True, precision=precision)
+        for m, r in zip(mols, rb):
+            rs = engine.run(m, gradient=True, precision=precision)
+            assert r.converged and rs.converged
+            assert r.energy == pytest.approx(rs.energy, abs=1e-7)
+            assert np.abs(r.gradient - rs.gradient).max() < 1e-6
