@@ -94,12 +94,16 @@ GpuContext context_acquire(int dev) {
     throw Error(PYFACC_ERR_CUDA, "cusolverDnSetStream failed");
   PF_CUDA(cudaEventCreate(&c.ev0));
   PF_CUDA(cudaEventCreate(&c.ev1));
+  PF_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+  PF_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
+  PF_CUDA(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
   return c;
 }
 
 void context_release(const GpuContext& c) {
   if (!c.stream) return;
   cudaStreamSynchronize(c.stream);
+  if (c.side) cudaStreamSynchronize(c.side);
   std::lock_guard<std::mutex> lk(g_pool_mu);
   g_free_ctx[c.device].push_back(c);
 }

@@ -23,6 +23,10 @@ struct GpuContext {
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // a second stream for work that may overlap the main stream's (the FP32
+  // half of a mixed Fock build or gradient), forked and joined by events
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
 GpuContext context_acquire(int device);   // the current device must be `device`
 void context_release(const GpuContext& c);
