@@ -74,15 +74,14 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   const double t32 = fp32_thresh >= 0 ? fp32_thresh : opt.fp32_thresh;
   if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? t32 : 0.0, dyn, stream);
   // the FP32 half of a mixed build runs on the side stream, overlapping the
-  // FP64 half (both only add into J and K)
-  cudaStream_t s32 = stream;
-  if (mixed) {
-    PF_CUDA(cudaEventRecord(ctx.fork, stream));
-    PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
-    s32 = ctx.side;
-  }
+  // FP64 half; an FP64 build alternates its classes between the two streams
+  // (every launch only adds into J and K)
+  cudaStream_t s32 = ctx.side;
+  PF_CUDA(cudaEventRecord(ctx.fork, stream));
+  PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
+  int nth = 0;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) {
+    for (int kc = bc; kc >= 0; --kc, ++nth) {
       const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
       if (dynamic) {
         launch_jk(pd, dyn.lists[2 * qc], bc, kc, false, nk, a, num_sms, stream);
@@ -91,13 +90,11 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
         launch_jk(pd, tasks[bc][kc][1], bc, kc, false, nk, a, num_sms, stream);
         launch_jk(pd, tasks[bc][kc][2], bc, kc, true, nk, a, num_sms, s32);
       } else {
-        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, nk, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, nk, a, num_sms, (nth & 1) ? ctx.side : stream);
       }
     }
-  if (mixed) {
-    PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
-    PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
-  }
+  PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
+  PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
   if (reducer) {  // partial J/K of this shard -> sums over all shards
     reduce(Jo, (long long)n2);
     for (int k = 0; k < nk; ++k) reduce(Ko[k], (long long)n2);
@@ -706,13 +703,12 @@ void System::gradient(double* g_host) {
   if (dyn_split)
     launch_dyn_tasks(pd, dmax, ns, opt.schwarz_thresh,
                      opt.gradient_fp32_thresh > 0 ? opt.gradient_fp32_thresh : opt.fp32_thresh, dyn, stream);
-  // the FP32 half runs on the side stream, overlapping the FP64 half
-  cudaStream_t s32 = stream;
-  if (split) {
-    PF_CUDA(cudaEventRecord(ctx.fork, stream));
-    PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
-    s32 = ctx.side;
-  }
+  // the FP32 half runs on the side stream, overlapping the FP64 half (an
+  // FP64 gradient keeps its classes on one stream: its register-heavy
+  // kernels measured slower when two of them share the SMs)
+  cudaStream_t s32 = ctx.side;
+  PF_CUDA(cudaEventRecord(ctx.fork, stream));
+  PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (dyn_split) {
@@ -726,10 +722,8 @@ void System::gradient(double* g_host) {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }
     }
-  if (split) {
-    PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
-    PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
-  }
+  PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
+  PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
   if (reducer) reduce(grad_dev, 3LL * natoms);
   PF_CUDA(cudaEventRecord(a1, stream));
   std::vector<double> g(3 * natoms, 0.0);
