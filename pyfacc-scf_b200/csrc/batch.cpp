@@ -618,7 +618,7 @@ void Batch::alloc() {
   PF_CUDA(cudaStreamSynchronize(stream));
 }
 
-void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32) {
+void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32, bool overlap) {
   launch_batch_dmax(nmol, ns_max, mt_dev, bf_off_dev, nfun_dev, dargs.Db, dmax, stream);
   JkArgs a;
   a.Dj = dargs.Db;
@@ -632,17 +632,28 @@ void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stat
   a.thresh = thresh;
   a.stats = stats;
   a.prim_thresh = thresh * PRIM_QUARTET_REL;
+  const bool fork = overlap && mixed_lists && !all_fp32;
+  cudaStream_t s32 = stream;
+  if (fork) {
+    PF_CUDA(cudaEventRecord(ctx.fork, stream));
+    PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
+    s32 = ctx.side;
+  }
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (all_fp32) {
         launch_jk(pd, tasks[bc][kc][0], bc, kc, true, 1, a, num_sms, stream);
       } else if (mixed_lists) {
         launch_jk(pd, tasks[bc][kc][1], bc, kc, false, 1, a, num_sms, stream);
-        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, s32);
       } else {
         launch_jk(pd, tasks[bc][kc][0], bc, kc, false, 1, a, num_sms, stream);
       }
     }
+  if (fork) {
+    PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
+    PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
+  }
 }
 
 // Task-width autotuner: every quartet class is timed with tasks of 32, 16
@@ -751,7 +762,7 @@ cudaGraphExec_t Batch::capture(int variant, long long* launches) {
     // a full rebuild of an incremental run builds P itself (the previous
     // step left P_new - P in Db); the first full build has Db = P already
     if (variant == G_FULL && dargs.incremental) launch_batch_full_density(nmol, da, stream);
-    fock_build(mixed, thresh, stats_dev, coarse);
+    fock_build(mixed, thresh, stats_dev, coarse, true);
     PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(StepReport), stream));
     launch_batch_step(nmol, da, stream);
   } catch (...) {
@@ -908,15 +919,23 @@ void Batch::gradient_run() {
   const bool split = pd.primf != nullptr &&
                      (opt.gradient_precision == PYFACC_PRECISION_MIXED ||
                       (opt.gradient_precision < 0 && opt.precision == PYFACC_PRECISION_MIXED));
+  if (split) {  // the FP32 half on the side stream, overlapping the FP64 half
+    PF_CUDA(cudaEventRecord(ctx.fork, stream));
+    PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
+  }
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc) {
       if (split) {
         launch_grad2e(pd, tasks[bc][kc][3], bc, kc, false, g2, num_sms, stream);
-        launch_grad2e(pd, tasks[bc][kc][4], bc, kc, true, g2, num_sms, stream);
+        launch_grad2e(pd, tasks[bc][kc][4], bc, kc, true, g2, num_sms, ctx.side);
       } else {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }
     }
+  if (split) {
+    PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
+    PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
+  }
   PF_CUDA(cudaEventRecord(ev[3], stream));
   grad_host.assign(3 * (size_t)natoms_tot, 0.0);
   PF_CUDA(cudaMemcpyAsync(grad_host.data(), grad_dev, grad_host.size() * sizeof(double), cudaMemcpyDeviceToHost,

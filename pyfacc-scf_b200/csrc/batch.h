@@ -206,8 +206,11 @@ class Batch {
   void build_tasks();
   void alloc();
   // J/K of Db into Jd/Kd: FP64 lists, or the FP64 + FP32 halves of mixed mode
-  // (all_fp32: every quartet of the full lists in FP32, the coarse builds)
-  void fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32 = false);
+  // (all_fp32: every quartet of the full lists in FP32, the coarse builds;
+  // overlap: the FP32 half of mixed lists on the side stream, forked and
+  // joined by events, as captured into the iteration graphs)
+  void fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32 = false,
+                  bool overlap = false);
   bool tuned_widths(std::array<int, NQCLASS>* w) const;  // cached tuner result for this batch shape
   std::string tune_key() const;
   void tune();
