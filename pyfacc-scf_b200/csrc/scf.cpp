@@ -73,9 +73,9 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   if (opt.shard_count > 1) dynamic = false;  // shards use their static sub-lists
   const double t32 = fp32_thresh >= 0 ? fp32_thresh : opt.fp32_thresh;
   if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? t32 : 0.0, dyn, stream);
-  // the FP32 half of a mixed build runs on the side stream, overlapping the
-  // FP64 half; an FP64 build alternates its classes between the two streams
-  // (every launch only adds into J and K)
+  // the FP64 and FP32 halves of a mixed build run on different streams,
+  // which swap from class to class; an FP64 build alternates its classes
+  // between the two streams (every launch only adds into J and K)
   cudaStream_t s32 = ctx.side;
   PF_CUDA(cudaEventRecord(ctx.fork, stream));
   PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
@@ -83,9 +83,10 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   for (int bc = NCLASS - 1; bc >= 0; --bc)
     for (int kc = bc; kc >= 0; --kc, ++nth) {
       const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
+      cudaStream_t s64 = (nth & 1) ? s32 : stream, s32c = (nth & 1) ? stream : s32;
       if (dynamic) {
-        launch_jk(pd, dyn.lists[2 * qc], bc, kc, false, nk, a, num_sms, stream);
-        if (mixed) launch_jk(pd, dyn.lists[2 * qc + 1], bc, kc, true, nk, a, num_sms, s32);
+        launch_jk(pd, dyn.lists[2 * qc], bc, kc, false, nk, a, num_sms, mixed ? s64 : stream);
+        if (mixed) launch_jk(pd, dyn.lists[2 * qc + 1], bc, kc, true, nk, a, num_sms, s32c);
       } else if (mixed) {
         launch_jk(pd, tasks[bc][kc][1], bc, kc, false, nk, a, num_sms, stream);
         launch_jk(pd, tasks[bc][kc][2], bc, kc, true, nk, a, num_sms, s32);
