@@ -704,18 +704,19 @@ void System::gradient(double* g_host) {
   if (dyn_split)
     launch_dyn_tasks(pd, dmax, ns, opt.schwarz_thresh,
                      opt.gradient_fp32_thresh > 0 ? opt.gradient_fp32_thresh : opt.fp32_thresh, dyn, stream);
-  // the FP32 half runs on the side stream, overlapping the FP64 half (an
-  // FP64 gradient keeps its classes on one stream: its register-heavy
-  // kernels measured slower when two of them share the SMs)
+  // the FP64 and FP32 halves run on different streams, which swap from
+  // class to class (an FP64 gradient keeps its classes on one stream: its
+  // register-heavy kernels measured slower when two of them share the SMs)
   cudaStream_t s32 = ctx.side;
   PF_CUDA(cudaEventRecord(ctx.fork, stream));
   PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
+  int nth = 0;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) {
+    for (int kc = bc; kc >= 0; --kc, ++nth) {
       if (dyn_split) {
         const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
-        launch_grad2e(pd, dyn.lists[2 * qc], bc, kc, false, g2, num_sms, stream);
-        launch_grad2e(pd, dyn.lists[2 * qc + 1], bc, kc, true, g2, num_sms, s32);
+        launch_grad2e(pd, dyn.lists[2 * qc], bc, kc, false, g2, num_sms, (nth & 1) ? s32 : stream);
+        launch_grad2e(pd, dyn.lists[2 * qc + 1], bc, kc, true, g2, num_sms, (nth & 1) ? stream : s32);
       } else if (split) {
         launch_grad2e(pd, tasks[bc][kc][1], bc, kc, false, g2, num_sms, stream);
         launch_grad2e(pd, tasks[bc][kc][2], bc, kc, true, g2, num_sms, s32);
