@@ -632,22 +632,26 @@ void Batch::fock_build(bool mixed_lists, double thresh, unsigned long long* stat
   a.thresh = thresh;
   a.stats = stats;
   a.prim_thresh = thresh * PRIM_QUARTET_REL;
-  const bool fork = overlap && mixed_lists && !all_fp32;
+  const bool fork = overlap;
   cudaStream_t s32 = stream;
   if (fork) {
     PF_CUDA(cudaEventRecord(ctx.fork, stream));
     PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
     s32 = ctx.side;
   }
+  int nth = 0;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) {
+    for (int kc = bc; kc >= 0; --kc, ++nth) {
+      // the two halves swap streams from class to class
+      // (single-precision lists: the classes alternate between the streams)
+      const bool swap = fork && (nth & 1);
       if (all_fp32) {
-        launch_jk(pd, tasks[bc][kc][0], bc, kc, true, 1, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, true, 1, a, num_sms, swap ? s32 : stream);
       } else if (mixed_lists) {
-        launch_jk(pd, tasks[bc][kc][1], bc, kc, false, 1, a, num_sms, stream);
-        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, s32);
+        launch_jk(pd, tasks[bc][kc][1], bc, kc, false, 1, a, num_sms, swap ? s32 : stream);
+        launch_jk(pd, tasks[bc][kc][2], bc, kc, true, 1, a, num_sms, swap ? stream : s32);
       } else {
-        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, 1, a, num_sms, stream);
+        launch_jk(pd, tasks[bc][kc][0], bc, kc, false, 1, a, num_sms, swap ? s32 : stream);
       }
     }
   if (fork) {
@@ -923,11 +927,12 @@ void Batch::gradient_run() {
     PF_CUDA(cudaEventRecord(ctx.fork, stream));
     PF_CUDA(cudaStreamWaitEvent(ctx.side, ctx.fork, 0));
   }
+  int nth = 0;
   for (int bc = NCLASS - 1; bc >= 0; --bc)
-    for (int kc = bc; kc >= 0; --kc) {
-      if (split) {
-        launch_grad2e(pd, tasks[bc][kc][3], bc, kc, false, g2, num_sms, stream);
-        launch_grad2e(pd, tasks[bc][kc][4], bc, kc, true, g2, num_sms, ctx.side);
+    for (int kc = bc; kc >= 0; --kc, ++nth) {
+      if (split) {  // the two halves swap streams from class to class
+        launch_grad2e(pd, tasks[bc][kc][3], bc, kc, false, g2, num_sms, (nth & 1) ? ctx.side : stream);
+        launch_grad2e(pd, tasks[bc][kc][4], bc, kc, true, g2, num_sms, (nth & 1) ? stream : ctx.side);
       } else {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }

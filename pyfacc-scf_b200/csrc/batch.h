@@ -207,7 +207,8 @@ class Batch {
   void alloc();
   // J/K of Db into Jd/Kd: FP64 lists, or the FP64 + FP32 halves of mixed mode
   // (all_fp32: every quartet of the full lists in FP32, the coarse builds;
-  // overlap: the FP32 half of mixed lists on the side stream, forked and
+  // overlap: the side stream takes every other class (of mixed lists the
+  // FP64 and FP32 halves swap streams from class to class), forked and
   // joined by events, as captured into the iteration graphs)
   void fock_build(bool mixed_lists, double thresh, unsigned long long* stats, bool all_fp32 = false,
                   bool overlap = false);
