@@ -106,9 +106,20 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
   ns = (int)basis.shells.size();
   uhf = (opt.scf_type == PYFACC_SCF_UHF) || (opt.scf_type == PYFACC_SCF_AUTO && nalpha != nbeta);
   e_nuc = nuclear_repulsion();
+  using clk = std::chrono::steady_clock;
+  const auto c0 = clk::now();
   upload_shells();
+  const auto c1 = clk::now();
   build_pairs();
+  const auto c2 = clk::now();
   alloc_matrices();
+  if (opt.verbose) {
+    PF_CUDA(cudaStreamSynchronize(stream));
+    const auto c3 = clk::now();
+    auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    std::fprintf(stderr, "pyfacc setup (ms): shells %.3f  pairs + tasks %.3f  matrices %.3f\n", ms(c0, c1), ms(c1, c2),
+                 ms(c2, c3));
+  }
 }
 
 System::~System() {
@@ -253,6 +264,9 @@ double max_prim_prefactor(const Basis& b) {
 // sorted by Q (descending) inside each class; pairs that cannot reach the
 // threshold against the largest Q are dropped.  Task lists per class pair.
 void System::build_pairs() {
+  using clk = std::chrono::steady_clock;
+  clk::time_point tq[8];
+  tq[0] = clk::now();
   std::vector<int4> pl0[NCLASS];
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
@@ -287,8 +301,10 @@ void System::build_pairs() {
                s_pr = carve((size_t)std::max(nprim_tot, 1) * 3 * sizeof(double4)), s_q = carve(np_all * sizeof(double)),
                s_perm = carve(np_all * sizeof(int)), s_ps = carve(np_all * sizeof(int)),
                s_kept = carve(np_all * sizeof(int));
+  tq[1] = clk::now();
   DeviceBuf scratch;
   scratch.ensure(o);
+  tq[2] = clk::now();
   char* sb = scratch.as<char>();
   int4* d_pl0 = reinterpret_cast<int4*>(sb + s_pl0);
   int4* d_pl1 = reinterpret_cast<int4*>(sb + s_pl1);
@@ -313,6 +329,7 @@ void System::build_pairs() {
   PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaMemcpyAsync(kept.data(), d_kept, np_all * sizeof(int), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
+  tq[3] = clk::now();
   const double qmax = np_all ? *std::max_element(q.begin(), q.end()) : 0.0;
   const double thr = opt.schwarz_thresh;
   std::vector<int> perm, new_ps;
@@ -357,7 +374,15 @@ void System::build_pairs() {
                         pd.info0, pd.info1, pd.info2, pd.geom, pd.prim, pd.primf, stream);
   }
   PF_CUDA(cudaStreamSynchronize(stream));
+  tq[4] = clk::now();
   build_tasks();
+  if (opt.verbose) {
+    PF_CUDA(cudaStreamSynchronize(stream));
+    tq[5] = clk::now();
+    auto ms = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+    std::fprintf(stderr, "pyfacc pairs (ms): host lists %.3f  scratch %.3f  records+Q %.3f  sort+gather %.3f  tasks %.3f\n",
+                 ms(tq[0], tq[1]), ms(tq[1], tq[2]), ms(tq[2], tq[3]), ms(tq[3], tq[4]), ms(tq[4], tq[5]));
+  }
 }
 
 // Contiguous ranges of n items with (as far as the granularity allows)
@@ -393,25 +418,28 @@ void System::build_tasks() {
       const int nk = pd.class_off[kc + 1] - pd.class_off[kc];
       const double* qb = pd.q_host.data() + pd.class_off[bc];
       const double* qk = pd.q_host.data() + pd.class_off[kc];
-      auto prefix = [&](double qbra, double t) {
-        if (t <= 0) return nk;
-        // number of kets with qbra * qk[j] >= t (qk descending)
-        int lo = 0, hi = nk;
-        while (lo < hi) {
-          int mid = (lo + hi) / 2;
-          if (qbra * qk[mid] >= t) lo = mid + 1; else hi = mid;
-        }
-        return lo;
-      };
+      // kets with qb[i] * qk[j] >= t form a prefix of the ket list (qk
+      // descending) that shrinks as i grows (qb descending): one pointer
+      // walk per threshold over all bras
+      std::vector<int> mfull(nb), m64v(nb);
+      int pf = nk, p64 = nk;
+      for (int i = 0; i < nb; ++i) {
+        if (thr > 0)
+          while (pf > 0 && !(qb[i] * qk[pf - 1] >= thr)) --pf;
+        if (t32 > 0)
+          while (p64 > 0 && !(qb[i] * qk[p64 - 1] >= t32)) --p64;
+        int m = pf;
+        if (bc == kc) m = std::min(m, i + 1);
+        mfull[i] = m;
+        m64v[i] = std::min(p64, m);
+      }
       for (int prec = 0; prec < 3; ++prec) {
         Pending p{bc, kc, prec, hostbuf.size(), nb};
         std::vector<int> toff(nb + 1), lo(nb), hi(nb);
         long long quart = 0;
         int ntask = 0;
         for (int i = 0; i < nb; ++i) {
-          int m = prefix(qb[i], thr);
-          if (bc == kc) m = std::min(m, i + 1);
-          int m64 = std::min(prefix(qb[i], t32), m);
+          const int m = mfull[i], m64 = m64v[i];
           int l = 0, h = m;
           if (prec == 1) h = m64;
           if (prec == 2) l = m64;
