@@ -32,6 +32,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -73,7 +74,10 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_gpu{index}.csv")
+        # raw samples go to $PYFACC_CLOCKS_DIR (default: the temp directory);
+        # the JSON line carries their summary
+        out = os.environ.get("PYFACC_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out, f"clocks_gpu{index}.csv")
 
     def __enter__(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)
@@ -212,7 +216,7 @@ def run_ours(args):
         breakdown[name]["scf_iterations"] = rr.n_iter
         breakdown[name]["quartets"] = rr.quartets
 
-    # the north-star molecule, C40H82 / STO-3G (282 bf), on rank 0 only
+    # the larger alkane, C40H82 / STO-3G (282 bf), mixed vs FP64, on rank 0 only
     c40 = None
     if rank == 0 and args.workload == "c20h42" and not args.no_c40:
         m40 = molecule("c40h82", 0)
@@ -327,7 +331,7 @@ def run_ours(args):
         "fock_builds_per_s": 1.0 / fock_s,
         "fock_builds_per_s_by_workload": rates,
         "breakdown_ms": breakdown,
-        "north_star_c40h82": c40,
+        "c40h82": c40,
         "batch_water256": batch,
         "wall_bracket_ms": {"mixed": statistics.mean(ev_mx), "fp64": statistics.mean(ev_64)},
         "e2e": {"value": e2e_step / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
