@@ -1403,7 +1403,9 @@ void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pair
   const size_t smem = use_smem ? need : 0;
   for (int c = 0; c < NCLASS; ++c) {
     if (npair[c] <= 0) continue;
-    const int blocks = std::max(1, std::min((npair[c] + 3) / 4, 2 * num_sms));
+    // one warp per pair; with global atomics up to 16 blocks per SM (a batch's
+    // many pairs), with per-block sums 4 (each block flushes 3 natoms sums)
+    const int blocks = std::max(1, std::min((npair[c] + 3) / 4, (use_smem ? 4 : 16) * num_sms));
     dim3 grid(blocks), block(128);
     if (c == 0) {
       PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
