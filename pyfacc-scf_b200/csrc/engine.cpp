@@ -192,10 +192,36 @@ void System::upload_shells() {
   std::vector<double4> atoms(natoms);
   for (int a = 0; a < natoms; ++a) atoms[a] = make_double4(xyz[3 * a], xyz[3 * a + 1], xyz[3 * a + 2], (double)Z[a]);
   // 1e pair lists: every pair a <= b of the upper triangle of S_overlap
-  // (overlap.f90:292-329), per class, ordered so that l_a >= l_b
+  // (overlap.f90:292-329), per class, ordered so that l_a >= l_b, except
+  // pairs on two atoms whose largest primitive-pair prefactor is below
+  // ONE_E_PAIR_CUT: with mu_min from the two smallest exponents (mu grows
+  // with both) and the largest |c N| of each shell, the test
+  // mu_min R^2 > ln|cN|_a + ln|cN|_b - ln(cut) bounds every primitive pair
+  std::vector<double> lcn(ns), amin(ns);
+  for (int s = 0; s < ns; ++s) {
+    const Shell& sh = basis.shells[s];
+    double mx = 0.0, mn = 1e300;
+    for (size_t k = 0; k < sh.ex.size(); ++k) {
+      const double a = sh.ex[k];
+      double nrm = std::pow(2.0 * a / 3.14159265358979323846, 0.75);
+      if (sh.l) nrm *= 2.0 * std::sqrt(a);
+      mx = std::max(mx, std::fabs(sh.co[k] * nrm));
+      mn = std::min(mn, a);
+    }
+    lcn[s] = std::log(std::max(mx, 1e-300));
+    amin[s] = mn;
+  }
+  const double lcut = std::log(ONE_E_PAIR_CUT);
   std::vector<int2> p1[NCLASS];
   for (int a = 0; a < ns; ++a)
     for (int b = a; b < ns; ++b) {
+      const Shell &sa = basis.shells[a], &sb = basis.shells[b];
+      if (sa.atom != sb.atom) {
+        double r2 = 0.0;
+        for (int x = 0; x < 3; ++x) r2 += (sa.c[x] - sb.c[x]) * (sa.c[x] - sb.c[x]);
+        const double mu = amin[a] * amin[b] / (amin[a] + amin[b]);
+        if (mu * r2 > lcn[a] + lcn[b] - lcut) continue;
+      }
       int x = a, y = b;
       if (basis.shells[x].l < basis.shells[y].l) std::swap(x, y);
       p1[basis.shells[x].l + basis.shells[y].l].push_back(make_int2(x, y));

@@ -60,6 +60,13 @@ constexpr double COARSE_SCREEN = 1e-9;
 // stays above coarse_err (an oscillating start must still reach the
 // mixed builds, on which alone the SCF may converge)
 constexpr int COARSE_MAX_ITER = 20;
+// one-electron pair screen: a shell pair on two atoms is left out of the
+// S/T/V and one-electron-gradient lists when every primitive pair has
+// |c_a N_a c_b N_b| exp(-mu R^2) below this.  The remaining factors (overlap
+// volume, kinetic terms, 2 pi/p sum Z for the nuclei, p-function and
+// derivative polynomials) stay below ~1e9 for STO-nG exponents and
+// molecules of up to ~2000 atoms, so a left-out entry is below 1e-16.
+constexpr double ONE_E_PAIR_CUT = 1e-25;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis

@@ -41,6 +41,10 @@ void System::one_electron() {
   a.T = T;
   a.V = Vm;
   a.nbf = nbf;
+  // pairs left out of the lists (negligible overlap) keep zeros
+  launch_zero(S, (size_t)nbf * nbf * sizeof(double), stream);
+  launch_zero(T, (size_t)nbf * nbf * sizeof(double), stream);
+  launch_zero(Vm, (size_t)nbf * nbf * sizeof(double), stream);
   launch_one_electron(shd, n1e, pairs1e, a, stream);
   launch_axpby((long long)nbf * nbf, 1.0, T, 0.0, H, stream);
   launch_axpby((long long)nbf * nbf, 1.0, Vm, 1.0, H, stream);
