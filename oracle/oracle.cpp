@@ -149,6 +149,14 @@ double norm(int ax, int ay, int az, double a) {
   return n / std::sqrt(fact2(2 * ax - 1) * fact2(2 * ay - 1) * fact2(2 * az - 1));
 }
 
+// norm(ax, ay, az, a) / norm(l, 0, 0, a): the component factor the routines
+// that normalise with the x^l factor of a shell apply afterwards (1 for
+// every s and p component; sqrt(3) for d_xy, d_xz, d_yz)
+double comp_ratio(int ax, int ay, int az) {
+  const int l = ax + ay + az;
+  return std::sqrt(fact2(2 * l - 1) / (fact2(2 * ax - 1) * fact2(2 * ay - 1) * fact2(2 * az - 1)));
+}
+
 // ---------------------------------------------------------------------------
 // Shell container (arrays handed over from Python)
 // ---------------------------------------------------------------------------
@@ -399,9 +407,10 @@ void prim_class(int la, int lb, int lc, int ld, double aa, double bb, double cc,
     }
 }
 
-// Contracted shell quartet with per-primitive normalisation of the s/p shells
-// (for l <= 1 the factor of gaussian.f90:80-98 is the same for every
-// Cartesian component).  VRR per primitive quartet, contraction, then HRR.
+// Contracted shell quartet: the primitives carry the x^l normalisation of
+// gaussian.f90:80-98 (the same for every Cartesian component of an s or p
+// shell), VRR per primitive quartet, contraction, HRR, then the component
+// ratios of d and higher shells.
 void eri_quartet(const Shells& S, int sa, int sb, int sc, int sd, int boys_mode, std::vector<double>& out) {
   const int la = S.l[sa], lb = S.l[sb], lc = S.l[sc], ld = S.l[sd];
   const int na = ncart(la), nb = ncart(lb), nc = ncart(lc), nd = ncart(ld);
@@ -433,12 +442,17 @@ void eri_quartet(const Shells& S, int sa, int sb, int sc, int sd, int boys_mode,
   out.assign((size_t)na * nb * nc * nd, 0.0);
   std::vector<double> Hb(nf);
   const int a0 = CT.first(la), b0 = CT.first(lb), c0 = CT.first(lc), d0 = CT.first(ld);
+  // the primitives above carry the x^l normalisation of their shell; the
+  // other Cartesian components of d and higher shells differ by comp_ratio
+  auto ratio = [](int g) { return comp_ratio(CT.comp[g][0], CT.comp[g][1], CT.comp[g][2]); };
   for (int ia = 0; ia < na; ++ia)
     for (int ib = 0; ib < nb; ++ib) {
       for (int f = 0; f < nf; ++f) Hb[f] = (CT.lval[f] >= lc) ? hrr_bra(H, nf, f, a0 + ia, b0 + ib, AB) : 0.0;
+      const double rab = ratio(a0 + ia) * ratio(b0 + ib);
       for (int ic = 0; ic < nc; ++ic)
         for (int id = 0; id < nd; ++id)
-          out[(((size_t)ia * nb + ib) * nc + ic) * nd + id] = hrr_ket(Hb, c0 + ic, d0 + id, CD);
+          out[(((size_t)ia * nb + ib) * nc + ic) * nd + id] =
+              rab * ratio(c0 + ic) * ratio(d0 + id) * hrr_ket(Hb, c0 + ic, d0 + id, CD);
     }
 }
 
@@ -844,6 +858,11 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
                 double g = Pt[mu * n + nu] * Pt[la * n + si];
                 g -= 0.5 * (Pa[mu * n + la] * Pa[nu * n + si] + Pa[mu * n + si] * Pa[nu * n + la]);
                 g -= 0.5 * (Pb[mu * n + la] * Pb[nu * n + si] + Pb[mu * n + si] * Pb[nu * n + la]);
+                // the derivative integrals below carry the x^l normalisation of
+                // each shell; the component ratios of d and higher shells go here
+                const int* cp[4] = {CT.comp[CT.first(ls[0]) + ia], CT.comp[CT.first(ls[1]) + ib],
+                                    CT.comp[CT.first(ls[2]) + ic], CT.comp[CT.first(ls[3]) + id]};
+                for (int q = 0; q < 4; ++q) g *= comp_ratio(cp[q][0], cp[q][1], cp[q][2]);
                 gam[k] = g;
               }
         const double fac = 4.0 * degeneracy(a, b, c, d);

@@ -192,6 +192,11 @@ def build_basis(basis_file: str, species, coords) -> Shells:
                 groups = [(1, 1)]
             elif kind == 'SP':
                 groups = [(0, 1), (1, 2)]
+            elif kind == 'D':
+                # not read by the reference (basis.f90:76-82 has no D branch);
+                # the oracle takes Cartesian d shells (xx, xy, xz, yy, yz, zz)
+                # so that the d-shell integrals can be checked
+                groups = [(2, 1)]
             else:
                 raise ValueError(f"unsupported shell type {kind!r} for element {label}")
             for lval, col in groups:
