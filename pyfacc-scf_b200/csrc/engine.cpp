@@ -349,7 +349,7 @@ void System::build_pairs() {
   PF_CUDA(cudaMemcpyAsync(d_pl1, all1.data(), np_all * sizeof(int4), cudaMemcpyHostToDevice, stream));
   launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, cut, d_kept,
                      stream);
-  launch_schwarz(tmp, off, d_q, stream);
+  launch_schwarz(tmp, off, d_q, stream, ctx.side, ctx.fork, ctx.join);
   std::vector<double> q(np_all);
   std::vector<int> kept(np_all);
   PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));

@@ -172,7 +172,10 @@ struct ShellDev {  // device copies of the shells (packed over a batch)
 void launch_build_pairs(const ShellDev& sh, int npair, const int4* pl0, const int4* pl1, int4* info0,
                         int4* info1, int4* info2, double4* geom, double4* prim, double cut, int* kept,
                         cudaStream_t s);
-void launch_schwarz(const PairData& pd, int npair_class_begin[NCLASS + 1], double* q, cudaStream_t s);
+// With a side stream and two events the (pp) class runs there, next to the
+// other two classes (the caller's stream waits for it before returning).
+void launch_schwarz(const PairData& pd, int npair_class_begin[NCLASS + 1], double* q, cudaStream_t s,
+                    cudaStream_t side = nullptr, cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
 void launch_gather_pairs(int npair, const int* perm, const int* new_pstart, const int4* i0, const int4* i1,
                          const int4* i2, const double4* g, const double4* pr, const double* q, double cut,
                          int4* o0, int4* o1, int4* o2, double4* og, double4* opr, float4* oprf, cudaStream_t s);

@@ -281,16 +281,27 @@ __global__ void schwarz_kernel(int begin, int end, const int4* __restrict__ info
   q[i] = sqrt(mx);
 }
 
-void launch_schwarz(const PairData& pd, int off[NCLASS + 1], double* q, cudaStream_t s) {
-  for (int c = 0; c < NCLASS; ++c) {
+void launch_schwarz(const PairData& pd, int off[NCLASS + 1], double* q, cudaStream_t s, cudaStream_t side,
+                    cudaEvent_t fork, cudaEvent_t join) {
+  const bool two = side && fork && join;
+  if (two) {
+    PF_CUDA(cudaEventRecord(fork, s));
+    PF_CUDA(cudaStreamWaitEvent(side, fork, 0));
+  }
+  for (int c = NCLASS - 1; c >= 0; --c) {  // the longest class first
     int n = off[c + 1] - off[c];
     if (n <= 0) continue;
     dim3 grid((n + 63) / 64), block(64);
-    if (c == 0) schwarz_kernel<0, 0><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
-    if (c == 1) schwarz_kernel<1, 0><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
-    if (c == 2) schwarz_kernel<1, 1><<<grid, block, 0, s>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    cudaStream_t st = (two && c == NCLASS - 1) ? side : s;
+    if (c == 0) schwarz_kernel<0, 0><<<grid, block, 0, st>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    if (c == 1) schwarz_kernel<1, 0><<<grid, block, 0, st>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
+    if (c == 2) schwarz_kernel<1, 1><<<grid, block, 0, st>>>(off[c], off[c + 1], pd.info0, pd.geom, pd.prim, q);
     PF_CUDA(cudaGetLastError());
-  count_launch();
+    count_launch();
+  }
+  if (two) {
+    PF_CUDA(cudaEventRecord(join, side));
+    PF_CUDA(cudaStreamWaitEvent(s, join, 0));
   }
 }
 
