@@ -1,11 +1,12 @@
 #!/usr/bin/env python3
 """Benchmark: seconds per RHF energy + analytic gradient, mixed precision
 (FP32 quartets below a Schwarz bound of 1e-5, incremental dP Fock builds)
-against the plain FP64 GPU path, on C20H42 / STO-3G (142 basis functions,
+against the plain FP64 GPU path, on C40H82 / STO-3G (282 basis functions,
 all-anti geometry with sigma = 0.02 A seeded jitter); Fock builds per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c20h42|c40h82|h2o] [--no-cpu-baseline]
+                    [--workload c40h82|c20h42|c100h202|c10h22] [--no-cpu-baseline]
+                    [--no-side] [--no-batch]
 
 A step is one energy + gradient from scratch (one-electron integrals, SCF to
 |dE| < 1e-10 and DIIS error < 1e-8, gradient) for one molecule.  With N > 1
@@ -15,14 +16,23 @@ max over ranks of the per-step time.
 
 ``value``  device time of the step on a resident system (shell pairs and
            Schwarz factors already on the GPU), CUDA events on the engine's
-           stream, between steps an L2 flush (256 MiB write).
+           stream, between steps an L2 flush (256 MiB write; the working set
+           is L2-resident, so the flush is what keeps steps cold).
 ``e2e``    the same step through the public C-ABI call ``pyfacc_run`` from
            host coordinates: basis parsing, pair construction, host->device
            copies and the device->host read of energy and gradient included.
-``--impl reference`` times the CPU restatement of the reference's path (the
-           reference itself cannot be built: no Fortran compiler, Libint or
-           LAPACK) on all host cores: a bounded sample of Fock builds, scaled
-           to one energy + gradient.
+``roofline``  the dominant kernels, the J/K digestion classes: algorithmic
+           FP64 flops of a full FP64 Fock build (and FP32 flops of an all-FP32
+           build) on the converged density / the build's CUDA-event time, over
+           the FMA peaks measured in the same run.
+``cpu_baseline`` / ``--impl reference``  the CPU restatement of the
+           reference's path (oracle/; the reference itself cannot be built:
+           no Fortran compiler, Libint or LAPACK) on all host cores, timed on
+           a bounded uniform sample of the same workload: the one-electron
+           matrices in full, every k-th bra shell pair of a Fock build and of
+           the gradient, one dense step (eigh + transforms), scaled to one
+           energy + gradient with the oracle's own SCF iteration count for
+           this molecule (tests/golden/c40h82_sto3g.json).
 """
 from __future__ import annotations
 
@@ -40,17 +50,25 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "pyfacc-scf_b200")
 sys.path.insert(0, PKG)
 
-METRIC = "s per RHF energy+gradient (mixed precision), C20H42/STO-3G"
-# SCF iterations of the oracle (core-Hamiltonian guess + DIIS, the
-# reference's start) for the workloads, measured in this repository
-REF_SCF_ITERS = {"c20h42": 22, "c10h22": 21, "c40h82": 24}
-
 WORKLOADS = {
-    "c20h42": dict(n=20, seed=1, basis="sto-3g", label="C20H42 RHF STO-3G (142 bf)"),
     "c40h82": dict(n=40, seed=40, basis="sto-3g", label="C40H82 RHF STO-3G (282 bf)"),
+    "c20h42": dict(n=20, seed=1, basis="sto-3g", label="C20H42 RHF STO-3G (142 bf)"),
     "c10h22": dict(n=10, seed=1, basis="sto-3g", label="C10H22 RHF STO-3G (72 bf)"),
     "c100h202": dict(n=100, seed=4, basis="sto-3g", label="C100H202 RHF STO-3G (702 bf)"),
 }
+# SCF iterations of the oracle (core-Hamiltonian guess + DIIS, the
+# reference's start, to dE < 1e-10 and DIIS error < 1e-8); read from the
+# oracle fixtures when they hold the count, else these values, measured by
+# running the oracle's SCF on the same molecules
+ORACLE_SCF_ITERS = {"c20h42": 22, "c10h22": 21, "c40h82": 24}
+# DRAM bytes per launch of the dominant J/K class kernel from one ncu capture
+# (profiles/jk_kernel_fp64_c40h82.md): the working set is L2-resident
+JK_TRAFFIC_BYTES = 2.06e6
+JK_TRAFFIC_NOTE = "dram read + write per launch of jk_kernel<double,1,0,0,0> (ncu, profiles/)"
+
+
+def metric_name(wl):
+    return f"s per RHF energy+gradient (mixed precision), {WORKLOADS[wl]['label']}"
 
 
 def dist_env():
@@ -60,12 +78,16 @@ def dist_env():
     return rank, world, local
 
 
-def molecule(wl, rank=0):
-    import pyfacc
+def geometry(wl, rank=0):
     from pyfacc import geometry as G
     w = WORKLOADS[wl]
-    sp, xyz = G.alkane(w["n"], seed=w["seed"] + 1000 * rank)
-    return pyfacc.Molecule(sp, xyz, w["basis"])
+    return G.alkane(w["n"], seed=w["seed"] + 1000 * rank)
+
+
+def molecule(wl, rank=0):
+    import pyfacc
+    sp, xyz = geometry(wl, rank)
+    return pyfacc.Molecule(sp, xyz, WORKLOADS[wl]["basis"])
 
 
 class Clocks:
@@ -116,8 +138,112 @@ class Clocks:
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
 
 
-def flush_l2(buf):
-    buf.zero_()
+def device_step(sys_):
+    """One energy + gradient on a resident system; engine-stream event time (s)."""
+    r = sys_.scf(check=False)
+    g = sys_.gradient()
+    t = (r.timings_ms["total"] + sys_.result().timings_ms["gradient"]) / 1e3
+    return r, g, t
+
+
+def timed_steps(sys_, steps, flush):
+    import torch
+    times, iters, builds = [], [], []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        r, g, t = device_step(sys_)
+        times.append(t)
+        iters.append(r.n_iter)
+        builds.append(r.n_fock_builds)
+    return times, iters, builds
+
+
+def jk_rates(sy, nb=20):
+    """Full J/K builds on the system's converged density: builds per second
+    (engine-stream CUDA events) and the algorithmic flops of each precision,
+    for the FP64 lists, the mixed lists and all quartets in FP32."""
+    import torch
+    from pyfacc import _native as N
+    from pyfacc.distributed import _CudaView
+    n = sy.nbf
+    ptr = ctypes.c_void_p()
+    N.check(N.lib().pyfacc_system_density_dev(sy.handle, ctypes.byref(ptr)), "pyfacc_system_density_dev")
+    P = torch.as_tensor(_CudaView(int(ptr.value), n * n), device="cuda").reshape(n, n).clone()
+    out = {}
+    for name in ("fp64", "mixed", "fp32"):
+        for _ in range(3):
+            sy.jk(P, precision=name)
+        ms, f64, f32 = [], 0.0, 0.0
+        for _ in range(nb):
+            sy.jk(P, precision=name)
+            st = sy.jk_stats()
+            ms.append(st["ms"])
+            f64, f32 = st["flops_fp64"], st["flops_fp32"]
+        t = statistics.mean(ms) * 1e-3
+        out[name] = {"builds_per_s": 1.0 / t, "ms_per_build": t * 1e3, "flops_fp64": f64, "flops_fp32": f32,
+                     "tflops_fp64": f64 / t / 1e12, "tflops_fp32": f32 / t / 1e12}
+    return out, P
+
+
+def oracle_iterations(wl):
+    path = os.path.join(ROOT, "tests", "golden", f"{wl}_sto3g.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        if "scf_iterations" in d:
+            return int(d["scf_iterations"]), f"oracle SCF iterations from {os.path.relpath(path, ROOT)}"
+    except OSError:
+        pass
+    return ORACLE_SCF_ITERS.get(wl, 24), "oracle SCF iterations measured by running oracle.scf on this molecule"
+
+
+def cpu_sample(wl, P=None, jk_stride=32, grad_stride=256):
+    """The oracle (CPU restatement of the reference path, OpenMP on all host
+    cores) on a bounded uniform sample of one energy + gradient of the
+    workload, scaled to the whole: one-electron matrices in full, one dense
+    SCF step (S^-1/2, X^T F X, eigh, density) in full, every jk_stride-th bra
+    pair of a Fock build and every grad_stride-th bra / one-electron pair of
+    the gradient.  P: a density (the engine's converged one, or None for the
+    reference's own core-Hamiltonian guess, rscf.f90:113-114); the oracle's
+    work does not depend on it (Schwarz screening only)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    sp, xyz = geometry(wl, 0)
+    mol = O.molecule(sp, xyz, os.path.join(PKG, "data", "basis_set", WORKLOADS[wl]["basis"] + ".txt"))
+    n = mol.shells.nbf
+    nocc = (mol.nalpha + mol.nbeta + 1) // 2
+    t0 = time.perf_counter()
+    S, T, V = O.one_electron(mol)
+    H = T + V
+    t_1e = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    s, U = np.linalg.eigh(S)
+    X = U / np.sqrt(s)
+    e, Cp = np.linalg.eigh(X.T @ H @ X)
+    C = X @ Cp
+    Pg = 2.0 * C[:, :nocc] @ C[:, :nocc].T
+    t_dense = time.perf_counter() - t0
+    if P is None:
+        P = Pg
+    t0 = time.perf_counter()
+    O.jk_sample(mol, P, jk_stride)
+    t_jk = (time.perf_counter() - t0) * jk_stride
+    t0 = time.perf_counter()
+    O.gradient_sample(mol, P, 0.5 * P, 0.5 * P, P, grad_stride)
+    t_grad = (time.perf_counter() - t0) * grad_stride
+    iters, src = oracle_iterations(wl)
+    value = t_1e + iters * (t_jk + t_dense) + t_grad
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count()))
+    return {"value": value, "unit": "s", "cores": threads, "kind": "port",
+            "sample": (f"oracle on {threads} threads, {WORKLOADS[wl]['label']}: one-electron S/T/V in full "
+                       f"({t_1e:.2f} s), one dense SCF step ({t_dense:.3f} s), every {jk_stride}th bra pair of a "
+                       f"Fock build (x{jk_stride} = {t_jk:.1f} s per build), every {grad_stride}th pair of the "
+                       f"gradient (x{grad_stride} = {t_grad:.1f} s); value = 1e + {iters} x (build + dense) + "
+                       f"gradient, {src}"),
+            "parts_s": {"one_electron": t_1e, "fock_build": t_jk, "dense_step": t_dense, "gradient": t_grad},
+            "scf_iterations": iters}
 
 
 def run_ours(args):
@@ -133,50 +259,26 @@ def run_ours(args):
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
-    mol = molecule(args.workload, rank)
+    wl = args.workload
+    mol = molecule(wl, rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    def device_step(sys_, grad=True):
-        r = sys_.scf(check=False)
-        g = sys_.gradient() if grad else None
-        return r, g
-
-    common = dict(device=local)
-    s_mixed = pyfacc.System(mol, precision="mixed", **common)
-    s_fp64 = pyfacc.System(mol, precision="fp64", **common)
-    # warm-up (also the accuracy comparison)
+    s_mixed = pyfacc.System(mol, precision="mixed", device=local)
+    s_fp64 = pyfacc.System(mol, precision="fp64", device=local)
     for _ in range(max(args.warmup, 1)):
-        rm, gm = device_step(s_mixed)
-        r64, g64 = device_step(s_fp64)
+        rm, gm, _ = device_step(s_mixed)
+        r64, g64, _ = device_step(s_fp64)
     dE = abs(rm.energy - r64.energy)
     dG = float(np.abs(gm - g64).max())
-
-    def timed(sys_, steps):
-        times, fock_ms, fock_flops, iters, ev_ms = [], 0.0, 0.0, [], []
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for _ in range(steps):
-            flush_l2(flush)
-            torch.cuda.synchronize()
-            e0.record()
-            r, g = device_step(sys_)
-            e1.record()
-            torch.cuda.synchronize()
-            # engine-stream events: SCF (1e .. final diagonalisation) + gradient
-            times.append((r.timings_ms["total"] + sys_.result().timings_ms["gradient"]) / 1e3)
-            ev_ms.append(e0.elapsed_time(e1))
-            fock_ms += r.timings_ms["fock"]
-            fock_flops += r.flops["fock"]
-            iters.append(r.n_iter)
-        return times, fock_ms, fock_flops, iters, ev_ms
 
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     l0 = N.lib().pyfacc_launch_count()
     with Clocks(local) as clk:
-        t_mx, fock_ms_mx, fock_fl_mx, it_mx, ev_mx = timed(s_mixed, args.steps)
+        t_mx, it_mx, nb_mx = timed_steps(s_mixed, args.steps, flush)
         launches = (N.lib().pyfacc_launch_count() - l0) // max(args.steps, 1)
-        t_64, fock_ms_64, fock_fl_64, it_64, ev_64 = timed(s_fp64, args.steps)
+        t_64, it_64, nb_64 = timed_steps(s_fp64, args.steps, flush)
     torch.cuda.synchronize()
     step_mx = statistics.mean(t_mx)
     step_64 = statistics.mean(t_64)
@@ -186,69 +288,43 @@ def run_ours(args):
         step_mx, step_64 = t.tolist()
         dist.barrier()
 
-    # Fock builds per second: J/K builds on the converged density (FP64
-    # lists, and the FP64 + FP32 lists of mixed mode), mean of 20
-    def fock_rates(sy):
-        n = sy.nbf
-        Pdev = ctypes.c_void_p()
-        N.lib().pyfacc_system_density_dev(sy.handle, ctypes.byref(Pdev))
-        J = torch.zeros(n, n, dtype=torch.float64, device="cuda")
-        K = torch.zeros(n, n, dtype=torch.float64, device="cuda")
-        out = {}
-        for name, prec in (("fp64", N.PRECISION_FP64), ("mixed", N.PRECISION_MIXED)):
-            for _ in range(3):
-                N.lib().pyfacc_system_jk(sy.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), prec)
-            nb = 20
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for _ in range(nb):
-                N.lib().pyfacc_system_jk(sy.handle, Pdev, 1, Pdev, J.data_ptr(), K.data_ptr(), prec)
-            torch.cuda.synchronize()
-            out[name] = nb / (time.perf_counter() - t0)
-        return out
-
-    rates = {WORKLOADS[args.workload]["label"]: fock_rates(s_fp64)}
-    fock_s = 1.0 / rates[WORKLOADS[args.workload]["label"]]["fp64"]
     breakdown = {}
     for name, sy in (("mixed", s_mixed), ("fp64", s_fp64)):
         rr = sy.result()
         breakdown[name] = {k: round(v, 3) for k, v in rr.timings_ms.items()}
         breakdown[name]["scf_iterations"] = rr.n_iter
+        breakdown[name]["fock_builds"] = rr.n_fock_builds
         breakdown[name]["quartets"] = rr.quartets
 
-    # the larger alkane, C40H82 / STO-3G (282 bf), mixed vs FP64, on rank 0 only
-    c40 = None
-    if rank == 0 and args.workload == "c20h42" and not args.no_c40:
-        m40 = molecule("c40h82", 0)
-        res40 = {}
-        for prec in ("fp64", "mixed"):
-            sy = pyfacc.System(m40, precision=prec, device=local)
-            for _ in range(2):
-                device_step(sy)
-            ts = []
-            for _ in range(2):
-                flush_l2(flush)
-                r, g = device_step(sy)
-                ts.append((r.timings_ms["total"] + sy.result().timings_ms["gradient"]) / 1e3)
-            res40[prec] = (min(ts), r.energy, g)
-            if prec == "fp64":
-                rates[WORKLOADS["c40h82"]["label"]] = fock_rates(sy)
-            sy.close()
-        c40 = {"workload": WORKLOADS["c40h82"]["label"], "fp64_s": res40["fp64"][0], "mixed_s": res40["mixed"][0],
-               "mixed_speedup_vs_fp64": res40["fp64"][0] / res40["mixed"][0],
-               "delta_e": abs(res40["fp64"][1] - res40["mixed"][1]),
-               "max_grad_diff": float(np.abs(res40["fp64"][2] - res40["mixed"][2]).max())}
+    # Fock builds on the converged density: rates and the J/K roofline
+    rates, Pconv = jk_rates(s_fp64)
+    rates_by_wl = {WORKLOADS[wl]["label"]: {k: v["builds_per_s"] for k, v in rates.items()}}
 
-    if rank == 0 and args.workload == "c20h42" and not args.no_c40:
-        sy = pyfacc.System(molecule("c100h202", 0), precision="fp64", device=local)
-        sy.scf(check=False)
-        rates[WORKLOADS["c100h202"]["label"]] = fock_rates(sy)
-        sy.close()
-
-    # batch of 256 water clusters (H2O)n, n uniform in [4, 16], rank 0 only:
-    # one pyfacc_run_batch call = energies and gradients of all 256 molecules
+    # side measurements on rank 0: the other alkanes, and the batch
+    side = {}
+    if rank == 0 and not args.no_side:
+        for swl in ("c20h42", "c100h202"):
+            if swl == wl:
+                continue
+            res = {}
+            for prec in ("fp64", "mixed"):
+                sy = pyfacc.System(molecule(swl, 0), precision=prec, device=local)
+                for _ in range(2):
+                    device_step(sy)
+                ts, _, _ = timed_steps(sy, 3, flush)
+                r, g, _ = device_step(sy)
+                res[prec] = (statistics.mean(ts), r.energy, g)
+                if prec == "fp64":
+                    rr, _ = jk_rates(sy, nb=10)
+                    rates_by_wl[WORKLOADS[swl]["label"]] = {k: v["builds_per_s"] for k, v in rr.items()}
+                sy.close()
+            side[swl] = {"workload": WORKLOADS[swl]["label"], "fp64_s": res["fp64"][0], "mixed_s": res["mixed"][0],
+                         "mixed_speedup_vs_fp64": res["fp64"][0] / res["mixed"][0],
+                         "delta_e": abs(res["fp64"][1] - res["mixed"][1]),
+                         "max_grad_diff": float(np.abs(res["fp64"][2] - res["mixed"][2]).max()),
+                         "timing": "mean of 3 device-timed steps after 2 warm-up steps"}
     batch = None
-    if rank == 0 and args.workload == "c20h42" and not args.no_batch:
+    if rank == 0 and not args.no_batch:
         batch = batch_measurement(pyfacc, local)
 
     # e2e through the C ABI with host buffers
@@ -261,8 +337,9 @@ def run_ours(args):
         res.gradient = grad.ctypes.data_as(N.P_double)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        N.lib().pyfacc_run(ctypes.byref(m), ctypes.byref(opt), ctypes.byref(res))
+        st = N.lib().pyfacc_run(ctypes.byref(m), ctypes.byref(opt), ctypes.byref(res))
         dt = time.perf_counter() - t0
+        N.check(st, "pyfacc_run", allow=(N.OK,))
         if i >= args.warmup:
             e2e.append(dt)
     e2e_step = statistics.mean(e2e)
@@ -279,7 +356,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.workload, 0, n_fock_builds=REF_SCF_ITERS.get(args.workload, 22))
+        cpu = cpu_sample(wl, Pconv.cpu().numpy())
 
     if dist:
         dist.destroy_process_group()
@@ -287,27 +364,32 @@ def run_ours(args):
         return
     h2d = mol.natoms * (3 * 8 + 4 + 2) + len(mol.basis) + 1
     d2h = 8 + mol.natoms * 3 * 8
-    fock_tflops = fock_fl_64 / (fock_ms_64 * 1e-3) / 1e12 if fock_ms_64 > 0 else None
+    a64 = rates["fp64"]["tflops_fp64"]
+    a32 = rates["fp32"]["tflops_fp32"]
     roof = {
-        "kernel": "J/K digestion (jk_kernel<double, class>), FP64 plain path",
+        "kernel": "J/K digestion (jk_kernel<double, class> x 6 classes), full FP64 Fock build on the converged "
+                  "density",
         "bound": "fp64",
-        "achieved": fock_tflops,
+        "achieved": a64,
         "peak": peak64 / 1e3 if peak64 else None,
         "unit": "TFLOP/s",
-        "frac": (fock_tflops / (peak64 / 1e3)) if (fock_tflops and peak64) else None,
-        "peak_source": "measured in this run: FP64 FMA microbenchmark (pyfacc_probe_fp64_gflops)",
-        # DRAM bytes per launch of the dominant class kernel (ps|ss), FP64,
-        # from one ncu capture (profiles/jk_kernel_fp64_c20h42.md): the
-        # working set is L2-resident, so DRAM traffic is a few MB per launch
-        "traffic": 2.06e6,
-        "traffic_unit": "bytes per launch (dram read + write), jk_kernel<double,1,0,0,0> at C20H42",
-        "algorithmic_flops_per_build": fock_fl_64 / max(1, sum(it_64)),
+        "frac": (a64 / (peak64 / 1e3)) if peak64 else None,
+        "traffic": JK_TRAFFIC_BYTES,
+        "traffic_note": JK_TRAFFIC_NOTE,
+        "peak_source": "measured in this run: FP64 FMA microbenchmark (pyfacc_probe_fp64_gflops); "
+                       "MEASURED_PEAKS.json holds no FP64/FP32 CUDA-core figure",
+        "algorithmic_flops_per_build": rates["fp64"]["flops_fp64"],
+        "ms_per_build": rates["fp64"]["ms_per_build"],
+        "fp32": {"kernel": "jk_kernel<float, class> x 6, every quartet in FP32, converged density",
+                 "bound": "fp32", "achieved": a32, "peak": peak32 / 1e3 if peak32 else None, "unit": "TFLOP/s",
+                 "frac": (a32 / (peak32 / 1e3)) if peak32 else None,
+                 "algorithmic_flops_per_build": rates["fp32"]["flops_fp32"],
+                 "ms_per_build": rates["fp32"]["ms_per_build"]},
     }
     clk_s = clk.summary()
     out = {
-        "metric": METRIC if args.workload == "c20h42"
-        else f"s per RHF energy+gradient (mixed precision), {WORKLOADS[args.workload]['label']}",
-        "value": step_mx * 1.0 / world,
+        "metric": metric_name(wl),
+        "value": step_mx / world,
         "unit": "s",
         "n_gpus": world,
         "steps": args.steps,
@@ -318,7 +400,7 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64+f32 (mixed); f64 for the plain path",
         "data": "synthetic, seeded (geometry builder pyfacc.geometry.alkane)",
-        "config": {"workload": WORKLOADS[args.workload]["label"], "precision": "mixed",
+        "config": {"workload": WORKLOADS[wl]["label"], "precision": "mixed",
                    "schwarz_thresh": 1e-12, "fp32_thresh": 1e-5, "scf": "dE<1e-10, DIIS err<1e-8",
                    "coarse_err": 1e-3, "gradient_fp32_thresh": 1e-3,
                    "mixed_energy": "last incremental mixed build (no FP64 polish build)",
@@ -328,21 +410,21 @@ def run_ours(args):
         "delta_e_mixed_vs_fp64": dE,
         "max_grad_diff_mixed_vs_fp64": dG,
         "scf_iterations": {"mixed": it_mx[0], "fp64": it_64[0]},
-        "fock_builds_per_s": 1.0 / fock_s,
-        "fock_builds_per_s_by_workload": rates,
+        "fock_builds_per_step": {"mixed": nb_mx[0], "fp64": nb_64[0]},
+        "step_times_s": {"mixed": t_mx, "fp64": t_64},
+        "fock_builds_per_s": rates["fp64"]["builds_per_s"],
+        "fock_builds_per_s_by_workload": rates_by_wl,
         "breakdown_ms": breakdown,
-        "c40h82": c40,
+        "side": side,
         "batch_water256": batch,
-        "wall_bracket_ms": {"mixed": statistics.mean(ev_mx), "fp64": statistics.mean(ev_64)},
         "e2e": {"value": e2e_step / world, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "api": "pyfacc_run (C ABI, host coordinates)"},
-        "gpu_launches": None,
+                "api": "pyfacc_run (C ABI, host coordinates in, energy + gradient out)"},
+        "gpu_launches": int(launches),
         "roofline": roof,
         "peaks_measured": {"fp64_gflops": peak64, "fp32_gflops": peak32},
         "cpu_baseline": cpu,
         "clocks": clk_s,
     }
-    out["gpu_launches"] = int(launches)
     print(json.dumps(out))
 
 
@@ -350,8 +432,8 @@ def batch_measurement(pyfacc, device):
     """256 water clusters (H2O)n, n ~ U{4..16} (rng seed 3), STO-3G RHF,
     energies + gradients of all molecules in one pyfacc_run_batch call
     (host coordinates in, host energies and gradients out), mixed precision
-    and FP64; a sample of the same molecules one by one through pyfacc_run
-    for comparison."""
+    and FP64, mean of 3 calls after a warm-up call; a sample of the same
+    molecules one by one through pyfacc_run for comparison."""
     import numpy as np
     from pyfacc import geometry as G
     clusters = G.water_clusters(count=256, seed=3)
@@ -362,14 +444,15 @@ def batch_measurement(pyfacc, device):
     for prec in ("mixed", "fp64"):
         pyfacc.run_batch(mols, gradient=True, precision=prec, device=device)  # warm-up (task-width tuning)
         ts = []
-        for _ in range(2):
+        for _ in range(3):
             t0 = time.perf_counter()
             r = pyfacc.run_batch(mols, gradient=True, precision=prec, device=device)
             ts.append(time.perf_counter() - t0)
         st = pyfacc.batch_stats()
         res[prec] = r
-        out[prec] = {"s_per_batch": min(ts), "ms_per_molecule": min(ts) * 1e3 / len(mols),
-                     "molecules_per_s": len(mols) / min(ts),
+        tm = statistics.mean(ts)
+        out[prec] = {"s_per_batch": tm, "s_per_batch_samples": ts, "ms_per_molecule": tm * 1e3 / len(mols),
+                     "molecules_per_s": len(mols) / tm,
                      "converged": int(sum(x.converged for x in r)),
                      "breakdown_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_one_electron", "ms_scf",
                                                                      "ms_polish", "ms_gradient")},
@@ -391,54 +474,37 @@ def batch_measurement(pyfacc, device):
     return out
 
 
-def cpu_baseline(wl, n_iter, n_fock_builds):
-    """The oracle's OpenMP J/K (the CPU restatement of the reference path) on
-    the same molecule: one full Fock build timed, scaled by the number of
-    Fock builds of the GPU run plus 4 build-equivalents for the gradient."""
-    import numpy as np
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    from pyfacc import geometry as G
-    w = WORKLOADS[wl]
-    sp, xyz = G.alkane(w["n"], seed=w["seed"])
-    mol = O.molecule(sp, xyz, os.path.join(PKG, "data", "basis_set", w["basis"] + ".txt"))
-    n = mol.shells.nbf
-    D = np.eye(n) * 0.5
-    t0 = time.perf_counter()
-    O.jk(mol, D, thresh=1e-12)
-    tb = time.perf_counter() - t0
-    builds = n_fock_builds + 4
-    return {"value": tb * builds, "unit": "s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"one FP64 J/K build of {w['label']} on {os.cpu_count()} threads ({tb:.2f} s), "
-                      f"x ({n_fock_builds} SCF builds of the oracle + 4 for the gradient)"}
-
-
 def run_reference(args):
     """The CPU restatement of the reference path (oracle/) on all host
-    cores: per step one full J/K build of the workload (the hot loop of
-    rscf.f90:118-135 done integral-direct), scaled to one energy + gradient
-    by the oracle's own SCF iteration count for this molecule (core guess,
-    DIIS) plus 4 build-equivalents for the gradient."""
+    cores, with the reference's own start (core-Hamiltonian guess density):
+    per step a bounded uniform sample of one energy + gradient of the
+    workload (cpu_sample), scaled to the whole.  Under torchrun only rank 0
+    runs it."""
     rank, world, local = dist_env()
     if rank != 0:
         return
+    wl = args.workload
+    for _ in range(args.warmup):
+        cpu_sample("c10h22", None, jk_stride=64, grad_stride=512)  # warm-up: small, loads the oracle
     samples = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(args.workload, 0, n_fock_builds=REF_SCF_ITERS.get(args.workload, 22))
-        if i >= args.warmup:
-            samples.append(cb["value"])
+    cb = None
+    for _ in range(args.steps):
+        cb = cpu_sample(wl, None)
+        samples.append(cb["value"])
     value = statistics.mean(samples)
     cb["value"] = value
+    cb["samples_s"] = samples
     out = {
         "impl": "reference",
-        "metric": METRIC if args.workload == "c20h42" else f"s per RHF energy+gradient, {WORKLOADS[args.workload]['label']}",
+        "metric": metric_name(wl),
         "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic, seeded", "config": {"workload": WORKLOADS[args.workload]["label"]},
+        "data": "synthetic, seeded", "config": {"workload": WORKLOADS[wl]["label"]},
         "cpu_baseline": cb,
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "CPU restatement of the reference path (oracle/): the reference cannot be built here "
-                "(no gfortran/nvfortran, Libint 2.11.1 or LAPACK) and its ERI path is incomplete",
+                "(no gfortran/nvfortran, Libint 2.11.1 or LAPACK) and its ERI path is incomplete; "
+                "warm-up steps run a small sample (C10H22)",
     }
     print(json.dumps(out))
 
@@ -449,11 +515,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c20h42", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c40h82", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-c40", action="store_true", help="skip the C40H82 side measurement")
+    ap.add_argument("--no-side", action="store_true", help="skip the C20H42 / C100H202 side measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the 256-water-cluster batch measurement")
     args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        print("note: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -24,7 +24,9 @@ extern "C" {
 #define PYFACC_ERR_NOT_CONVERGED   3  /* SCF hit max_iter                   */
 #define PYFACC_ERR_LINDEP          4  /* overlap matrix not positive        */
 #define PYFACC_ERR_CUDA            5  /* CUDA / cuBLAS / cuSOLVER failure   */
-#define PYFACC_ERR_TIMEOUT         6  /* a bounded device wait gave up      */
+#define PYFACC_ERR_TIMEOUT         6  /* a bounded device wait gave up;
+                                           reserved: no kernel of this build
+                                           waits on a flag, so none returns it */
 #define PYFACC_ERR_INVALID         7  /* bad argument                       */
 #define PYFACC_ERR_ELEMENT         8  /* element without basis functions    */
 #define PYFACC_ERR_NO_DEVICE       9  /* no CUDA device                     */
@@ -35,6 +37,9 @@ extern "C" {
 #define PYFACC_BOYS_REFERENCE_TRAPEZOID  1 /* boys.f90:9-43, used for V only */
 #define PYFACC_PRECISION_FP64            0
 #define PYFACC_PRECISION_MIXED           1 /* FP32 quartets below fp32_thresh */
+#define PYFACC_PRECISION_FP32            2 /* pyfacc_system_jk only: every
+                                              quartet in FP32 (the coarse
+                                              builds of a mixed SCF)          */
 #define PYFACC_SCF_AUTO                  0 /* RHF if nalpha == nbeta          */
 #define PYFACC_SCF_RHF                   1
 #define PYFACC_SCF_UHF                   2
@@ -185,6 +190,11 @@ int pyfacc_system_one_electron(pyfacc_system *sys, double *S_dev, double *T_dev,
  * Schwarz screening uses the density: Q_ab Q_cd max|D| < schwarz_thresh. */
 int pyfacc_system_jk(pyfacc_system *sys, const double *Dj_dev, int nk, const double *Dk_dev,
                      double *J_dev, double *K_dev, int precision);
+/* Statistics of the last pyfacc_system_jk call on this system:
+ * out[0..n) = {ms (CUDA events on the engine stream around the build),
+ * algorithmic flops of the FP64 quartets, of the FP32 quartets, contracted
+ * quartets FP64, FP32, primitive quartets FP64, FP32}. */
+int pyfacc_system_jk_stats(const pyfacc_system *sys, double *out, int n);
 /* Full (nbf^4) ERI tensor on the device, small systems only (tests). */
 int pyfacc_system_eri_tensor(pyfacc_system *sys, double *eri_dev);
 /* SCF with the system's options; res as in pyfacc_run. */
@@ -205,6 +215,20 @@ long long pyfacc_launch_count(void);
  * out_dev[i*(mmax+1)+m]).  mode: PYFACC_BOYS_*; fp32 != 0 uses the
  * single-precision path of mixed mode. */
 int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double *x_dev, double *out_dev);
+
+/* Dense FP64 products on the tensor cores (the kernels of the SCF step),
+ * row-major device matrices with leading dimensions m (A: m x k, or k x m
+ * when ta), n (B: k x n, or n x k when tb) and n (C: m x n):
+ * C = op(A) op(B), op = transpose when ta / tb; asym_a != 0 uses
+ * op(A) = A - A^T (square A, ta = 0); sym != 0 computes a result known to be
+ * symmetric from its upper triangle. */
+int pyfacc_dense_gemm_dev(int m, int n, int k, int ta, const double *A_dev, int tb, const double *B_dev,
+                          double *C_dev, int sym, int asym_a);
+/* TC2 purification of a symmetric n x n device matrix F into the projector
+ * onto its nocc lowest eigenvectors (P_dev, n x n, not aliasing F_dev);
+ * *steps receives the
+ * number of TC2 steps.  PYFACC_ERR_NOT_CONVERGED without a gap at nocc. */
+int pyfacc_purify_dev(int n, int nocc, const double *F_dev, double *P_dev, int *steps);
 
 /* Cost-balanced split of n weighted work items into `parts` contiguous
  * ranges: bounds[0..parts] (host only, no GPU needed). */
@@ -235,7 +259,9 @@ const char *pyfacc_version(void);
  * PYFACC_ERR_INVALID (pyfacc_last_message() gives the size).  The first call
  * on a device sets that device up and should precede any stream capture.
  * Calls share the array; calls from one process are serialised and return
- * after their kernels finish. */
+ * after their kernels finish.  The kernels run on the legacy default stream:
+ * a density written on a non-blocking stream must be complete (that stream
+ * synchronised) before the call. */
 int pyfacc_jk_noalloc(const pyfacc_molecule *mol, const char *data_dir, double schwarz_thresh,
                       const double *D_dev, double *J_dev, double *K_dev);
 

@@ -136,6 +136,26 @@ long double boys_ld(int m, long double x) {
   return f;
 }
 
+// F_0..F_L at one argument: the series (or the asymptotic form) for F_L
+// only, then the downward recursion F_m = (2x F_{m+1} + e^-x) / (2m+1), all
+// in long double (stable downwards, no cancellation).  The same values as
+// boys_ld per order to round-off, at one series per argument instead of L+1.
+void boys_all_ld(int L, long double x, long double* F) {
+  F[L] = boys_ld(L, x);
+  if (L == 0) return;
+  const long double ex = expl(-x);
+  for (int m = L - 1; m >= 0; --m) F[m] = (2.0L * x * F[m + 1] + ex) / (2 * m + 1);
+}
+inline void boys_all(int mode, int L, double x, double* F) {
+  if (mode == 1) {
+    for (int m = 0; m <= L; ++m) F[m] = boys_trapezoid(m, x);
+    return;
+  }
+  long double Fl[4 * LMAXC + 2];
+  boys_all_ld(L, (long double)x, Fl);
+  for (int m = 0; m <= L; ++m) F[m] = (double)Fl[m];
+}
+
 inline double boys(int mode, int m, double x) {
   return mode == 1 ? boys_trapezoid(m, x) : (double)boys_ld(m, (long double)x);
 }
@@ -287,7 +307,7 @@ double nuclear_prim(const int a[3], const int b[3], double aa, double bb, const 
   double eps = 1.0 / (4.0 * g);
   int L = a[0] + a[1] + a[2] + b[0] + b[1] + b[2];
   double F[2 * LMAXC + 1];
-  for (int m = 0; m <= L; ++m) F[m] = boys(boys_mode, m, g * pc2);
+  boys_all(boys_mode, L, g * pc2, F);
   double v = 0.0;
   for (int l = 0; l <= a[0] + b[0]; ++l)
     for (int r = 0; r <= l / 2; ++r)
@@ -329,7 +349,11 @@ void vrr(int Le, int Lf, double p, const double* P, const double* A, double q, c
     pq2 += (P[i] - Q[i]) * (P[i] - Q[i]);
   }
   const double T = rho * pq2;
-  for (int m = 0; m <= L; ++m) X[m] = pref * boys(boys_mode, m, T);
+  {
+    double F[4 * LMAXC + 2];
+    boys_all(boys_mode, L, T, F);
+    for (int m = 0; m <= L; ++m) X[m] = pref * F[m];
+  }
   auto at = [&](int e, int f, int m) -> double& { return X[((size_t)e * nf + f) * M + m]; };
   for (int e = 1; e < ne; ++e) {
     int i = CT.first_axis(e), par = CT.down(e, i);
@@ -487,7 +511,7 @@ double cook_eri_prim(const int* a, const int* b, const int* c, const int* d, dou
   double T = pq2 / (4.0 * delta);  // D1: rho*|PQ|^2
   double F[4 * LMAXC + 1];
   int L = a[0] + a[1] + a[2] + b[0] + b[1] + b[2] + c[0] + c[1] + c[2] + d[0] + d[1] + d[2];
-  for (int m = 0; m <= L; ++m) F[m] = boys(boys_mode, m, T);
+  boys_all(boys_mode, L, T, F);
   double G = 0.0;
   for (int l = 0; l <= a[0] + b[0]; ++l)
     for (int r = 0; r <= l / 2; ++r)
@@ -678,11 +702,15 @@ long orc_jk(int ns, const int* l, const int* atom, const double* cen, const int*
   return orc_jk_range(ns, l, atom, cen, poff, ex, co, boys_mode, nd, D, thresh, 0, ns * (ns + 1) / 2, J, K);
 }
 
-// J/K from the canonical quartets whose bra pair index (a(a+1)/2 + b) lies
-// in [ij_begin, ij_end): the share of one rank of a sharded Fock build.
-long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
-                  const double* co, int boys_mode, int nd, const double* D, double thresh, int ij_begin, int ij_end,
-                  double* J, double* K) {
+}  // extern "C"
+
+namespace {
+// J/K over the bra pairs ij in [ij_begin, ij_end) with ij % stride == phase
+// (every ket of each of them): stride 1 is the whole range, a larger stride
+// a uniform sample of the bra pairs whose cost is ~1/stride of the whole.
+long jk_impl(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+             const double* co, int boys_mode, int nd, const double* D, double thresh, int ij_begin, int ij_end,
+             int stride, int phase, double* J, double* K) {
   Shells S(ns, l, atom, cen, poff, ex, co);
   const int n = S.nbf;
   const size_t nn = (size_t)n * n;
@@ -700,6 +728,7 @@ long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, cons
     std::vector<double> Jl(nd * nn, 0.0), Kl(nd * nn, 0.0), o;
 #pragma omp for schedule(dynamic, 1)
     for (int ij = std::min(ij_end, npair) - 1; ij >= std::max(ij_begin, 0); --ij) {
+      if (ij % stride != phase) continue;
       const int a = pa[ij], b = pb[ij];
       for (int kl = 0; kl <= ij; ++kl) {
         const int c = pa[kl], d = pb[kl];
@@ -748,6 +777,27 @@ long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, cons
   }
   return count;
 }
+}  // namespace
+
+extern "C" {
+
+// J/K from the canonical quartets whose bra pair index (a(a+1)/2 + b) lies
+// in [ij_begin, ij_end): the share of one rank of a sharded Fock build.
+long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                  const double* co, int boys_mode, int nd, const double* D, double thresh, int ij_begin, int ij_end,
+                  double* J, double* K) {
+  return jk_impl(ns, l, atom, cen, poff, ex, co, boys_mode, nd, D, thresh, ij_begin, ij_end, 1, 0, J, K);
+}
+
+// The partial J/K of every stride-th bra pair (ij % stride == phase): a
+// bounded, uniform sample of a Fock build for timing the CPU path.
+long orc_jk_sample(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                   const double* co, int boys_mode, int nd, const double* D, double thresh, int stride, int phase,
+                   double* J, double* K) {
+  if (stride < 1) stride = 1;
+  return jk_impl(ns, l, atom, cen, poff, ex, co, boys_mode, nd, D, thresh, 0, ns * (ns + 1) / 2, stride,
+                 ((phase % stride) + stride) % stride, J, K);
+}
 
 // Analytic nuclear gradient pieces (natoms x 3 each, accumulated):
 //   g1[]  = sum P dH          (kinetic + nuclear attraction incl. Hellmann-Feynman)
@@ -757,10 +807,16 @@ long orc_jk_range(int ns, const int* l, const int* atom, const double* cen, cons
 // Pt = total density, Pa/Pb = spin densities (RHF: Pa = Pb = Pt/2).
 // Derivatives of the normalised contracted functions are taken at the
 // primitive level: d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}.
-void orc_gradient(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
-                  const double* co, int natoms, const double* axyz, const int* Z, int boys_mode,
-                  const double* Pt, const double* Pa, const double* Pb, const double* W, double thresh,
-                  double* g1, double* gS, double* g2, double* gN) {
+}  // extern "C"
+
+namespace {
+// The gradient pieces from the ordered one-electron shell pairs with
+// (sa ns + sb) % stride == phase and the two-electron bra pairs with
+// ij % stride == phase (stride 1: everything).
+void gradient_impl(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                   const double* co, int natoms, const double* axyz, const int* Z, int boys_mode,
+                   const double* Pt, const double* Pa, const double* Pb, const double* W, double thresh,
+                   int stride, int phase, double* g1, double* gS, double* g2, double* gN) {
   Shells S(ns, l, atom, cen, poff, ex, co);
   const int n = S.nbf;
   for (int i = 0; i < 3 * natoms; ++i) g1[i] = gS[i] = g2[i] = gN[i] = 0.0;
@@ -774,9 +830,15 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
       if (r <= 1e-10) continue;
       for (int x = 0; x < 3; ++x) gN[3 * i + x] -= (double)Z[i] * Z[j] * d[x] / (r2 * r);
     }
-  // one-electron terms over all ordered shell pairs
-  for (int sa = 0; sa < ns; ++sa)
+  // one-electron terms over all ordered shell pairs (threads over sa, each
+  // with its own accumulators, summed at the end)
+#pragma omp parallel
+  {
+  std::vector<double> g1l(3 * natoms, 0.0), gSl(3 * natoms, 0.0);
+#pragma omp for schedule(dynamic, 1)
+  for (int sa = 0; sa < ns; ++sa) {
     for (int sb = 0; sb < ns; ++sb) {
+      if ((sa * ns + sb) % stride != phase) continue;
       const double *A = cen + 3 * sa, *B = cen + 3 * sb;
       const int at_a = atom[sa], at_b = atom[sb];
       for (int ia = 0; ia < ncart(l[sa]); ++ia)
@@ -815,18 +877,24 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
                 }
               }
             // two-centre S, T: d/dB = -d/dA
-            gS[3 * at_a + x] -= wmn * dS;
-            gS[3 * at_b + x] += wmn * dS;
-            g1[3 * at_a + x] += pmn * dT;
-            g1[3 * at_b + x] -= pmn * dT;
+            gSl[3 * at_a + x] -= wmn * dS;
+            gSl[3 * at_b + x] += wmn * dS;
+            g1l[3 * at_a + x] += pmn * dT;
+            g1l[3 * at_b + x] -= pmn * dT;
             for (int c = 0; c < natoms; ++c) {
-              g1[3 * at_a + x] += pmn * dVa[c];
-              g1[3 * at_b + x] += pmn * dVb[c];
-              g1[3 * c + x] -= pmn * (dVa[c] + dVb[c]);
+              g1l[3 * at_a + x] += pmn * dVa[c];
+              g1l[3 * at_b + x] += pmn * dVb[c];
+              g1l[3 * c + x] -= pmn * (dVa[c] + dVb[c]);
             }
           }
         }
     }
+  }
+#pragma omp critical
+  {
+    for (int i = 0; i < 3 * natoms; ++i) { g1[i] += g1l[i]; gS[i] += gSl[i]; }
+  }
+  }
   // two-electron term over canonical shell quartets
   std::vector<double> Q((size_t)ns * (ns + 1) / 2);
   orc_schwarz(ns, l, atom, cen, poff, ex, co, 0, Q.data());
@@ -840,6 +908,7 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
     std::vector<double> gam;
 #pragma omp for schedule(dynamic, 1)
     for (int ij = npair - 1; ij >= 0; --ij) {
+      if (ij % stride != phase) continue;
       const int a = pa[ij], b = pb[ij];
       for (int kl = 0; kl <= ij; ++kl) {
         const int c = pa[kl], d = pb[kl];
@@ -923,6 +992,28 @@ void orc_gradient(int ns, const int* l, const int* atom, const double* cen, cons
       for (int i = 0; i < 3 * natoms; ++i) g2[i] += gl[i];
     }
   }
+}
+}  // namespace
+
+extern "C" {
+
+void orc_gradient(int ns, const int* l, const int* atom, const double* cen, const int* poff, const double* ex,
+                  const double* co, int natoms, const double* axyz, const int* Z, int boys_mode,
+                  const double* Pt, const double* Pa, const double* Pb, const double* W, double thresh,
+                  double* g1, double* gS, double* g2, double* gN) {
+  gradient_impl(ns, l, atom, cen, poff, ex, co, natoms, axyz, Z, boys_mode, Pt, Pa, Pb, W, thresh, 1, 0, g1, gS, g2,
+                gN);
+}
+
+// The gradient pieces of every stride-th one-electron shell and two-electron
+// bra pair: a bounded, uniform sample of the gradient for timing the CPU path.
+void orc_gradient_sample(int ns, const int* l, const int* atom, const double* cen, const int* poff,
+                         const double* ex, const double* co, int natoms, const double* axyz, const int* Z,
+                         int boys_mode, const double* Pt, const double* Pa, const double* Pb, const double* W,
+                         double thresh, int stride, int phase, double* g1, double* gS, double* g2, double* gN) {
+  if (stride < 1) stride = 1;
+  gradient_impl(ns, l, atom, cen, poff, ex, co, natoms, axyz, Z, boys_mode, Pt, Pa, Pb, W, thresh, stride,
+                ((phase % stride) + stride) % stride, g1, gS, g2, gN);
 }
 
 }  // extern "C"

@@ -83,6 +83,9 @@ def lib():
         _LIB.orc_jk_range.restype = ctypes.c_long
         _LIB.orc_jk_range.argtypes = sh + [i, i, p, d, i, i, p, p]
         _LIB.orc_gradient.argtypes = sh + [i, p, p, i, p, p, p, p, d, p, p, p, p]
+        _LIB.orc_jk_sample.restype = ctypes.c_long
+        _LIB.orc_jk_sample.argtypes = sh + [i, i, p, d, i, i, p, p]
+        _LIB.orc_gradient_sample.argtypes = sh + [i, p, p, i, p, p, p, p, d, i, i, p, p, p, p]
     return _LIB
 
 
@@ -307,6 +310,29 @@ def jk(mol: Molecule, dens, thresh=1e-12, boys_mode=0):
     K = np.zeros_like(D)
     lib().orc_jk(*mol.shells.args(), boys_mode, nd, _ptr(D), thresh, _ptr(J), _ptr(K))
     return (J[0], K[0]) if single else (J, K)
+
+
+def jk_sample(mol: Molecule, dens, stride, phase=0, thresh=1e-12):
+    """Partial J/K of the bra pairs ij with ij % stride == phase (a uniform
+    sample of one Fock build, ~1/stride of its work; for timing)."""
+    D = np.ascontiguousarray(np.asarray(dens, dtype=np.float64))
+    if D.ndim == 2:
+        D = D[None]
+    J = np.zeros_like(D)
+    K = np.zeros_like(D)
+    lib().orc_jk_sample(*mol.shells.args(), 0, D.shape[0], _ptr(D), thresh, stride, phase, _ptr(J), _ptr(K))
+    return J, K
+
+
+def gradient_sample(mol: Molecule, Pt, Pa, Pb, W, stride, phase=0, thresh=1e-12):
+    """Gradient pieces of every stride-th one-electron shell and two-electron
+    bra pair (a uniform sample of the analytic gradient; for timing)."""
+    na = mol.natoms
+    g = [np.zeros((na, 3)) for _ in range(4)]
+    c = np.ascontiguousarray
+    lib().orc_gradient_sample(*mol.shells.args(), na, _ptr(mol.xyz), _ptr(mol.Z), 0, _ptr(c(Pt)), _ptr(c(Pa)),
+                              _ptr(c(Pb)), _ptr(c(W)), thresh, stride, phase, *[_ptr(x) for x in g])
+    return g
 
 
 # ---------------------------------------------------------------------------

@@ -48,7 +48,7 @@ static int qclass_index(int bc, int kc) { return (bc == 0) ? 0 : (bc == 1 ? 1 + 
 static const int kWidths[3] = {32, 16, 8};
 
 BatchMolHost batch_parse(const pyfacc_molecule& m, const pyfacc_options& o, bool* uhf) {
-  if (m.natoms <= 0 || !m.z || !m.coords || !m.basis) throw Error(PYFACC_ERR_INVALID, "empty molecule");
+  validate_molecule(m);
   BatchMolHost h;
   h.natoms = m.natoms;
   h.Z.assign(m.z, m.z + m.natoms);

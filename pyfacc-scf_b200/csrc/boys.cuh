@@ -22,6 +22,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "f2.cuh"
+
 #define PF_BOYS_NGRID 361
 #define PF_BOYS_STEP 0.1
 #define PF_BOYS_INV_STEP 10.0
@@ -119,6 +121,45 @@ __device__ __forceinline__ void boys_fp32(float T, float* __restrict__ F) {
   const float t2 = 2.0f * T;
 #pragma unroll
   for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + e) * (1.0f / (2 * m + 1));
+}
+
+// Two arguments at once in packed float pairs (F2, f2.cuh): the grid rows
+// are gathered per argument, the Taylor sum and the recursions run on both
+// in FFMA2/FMUL2; the per-argument selections (Taylor or asymptotic, grid
+// index) stay scalar.  The same arithmetic as boys_fp32, argument by
+// argument.
+template <int L>
+__device__ __forceinline__ void boys_fp32x2(F2 T, F2* __restrict__ F) {
+  const float Tx = T.v.x, Ty = T.v.y;
+  const bool tabx = Tx < (float)PF_BOYS_TMAX, taby = Ty < (float)PF_BOYS_TMAX;
+  const F2 biased = pf_fma(F2(fminf(Tx, (float)PF_BOYS_TMAX), fminf(Ty, (float)PF_BOYS_TMAX)),
+                           F2((float)PF_BOYS_INV_STEP), F2(12582912.0f));
+  const int kx = tabx ? (__float_as_int(biased.v.x) & 0x7fffff) - 0x400000 : 0;
+  const int ky = taby ? (__float_as_int(biased.v.y) & 0x7fffff) - 0x400000 : 0;
+  const F2 kd = biased + F2(-12582912.0f);
+  const F2 x = pf_fma(kd, F2((float)PF_BOYS_STEP), T * F2(-1.0f));
+  const float4* rx = reinterpret_cast<const float4*>(g_boys_tlf + ((size_t)L * PF_BOYS_NGRID + kx) * PF_BOYS_NT);
+  const float4* ry = reinterpret_cast<const float4*>(g_boys_tlf + ((size_t)L * PF_BOYS_NGRID + ky) * PF_BOYS_NT);
+  const float4 x0 = __ldg(rx), x1 = __ldg(rx + 1), y0 = __ldg(ry), y1 = __ldg(ry + 1);
+  F2 f = pf_fma(F2(x1.x, y1.x), x, F2(x0.w, y0.w));
+  f = pf_fma(f, x, F2(x0.z, y0.z));
+  f = pf_fma(f, x, F2(x0.y, y0.y));
+  f = pf_fma(f, x, F2(x0.x, y0.x));
+  const F2 rt(rsqrtf(fmaxf(Tx, (float)PF_BOYS_TMAX)), rsqrtf(fmaxf(Ty, (float)PF_BOYS_TMAX)));
+  F2 fa = F2(0.88622692545275801365f) * rt;
+  if (L == 0) {
+    F[0] = F2(tabx ? f.v.x : fa.v.x, taby ? f.v.y : fa.v.y);
+    return;
+  }
+  const F2 e(expf(-Tx), expf(-Ty));
+  const F2 ne = e * F2(-1.0f);
+  const F2 o2t = F2(0.5f) * rt * rt;
+#pragma unroll
+  for (int m = 0; m < L; ++m) fa = pf_fma(F2((float)(2 * m + 1)), fa, ne) * o2t;
+  F[L] = F2(tabx ? f.v.x : fa.v.x, taby ? f.v.y : fa.v.y);
+  const F2 t2 = T + T;
+#pragma unroll
+  for (int m = L - 1; m >= 0; --m) F[m] = pf_fma(t2, F[m + 1], e) * F2(1.0f / (2 * m + 1));
 }
 
 template <int L, typename R> struct Boys;

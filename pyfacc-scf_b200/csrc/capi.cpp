@@ -321,9 +321,27 @@ int pyfacc_system_jk(pyfacc_system* sys, const double* Dj_dev, int nk, const dou
     const size_t n2 = (size_t)s.nbf * s.nbf;
     const double* Dk[2] = {Dk_dev, Dk_dev + n2};
     double* Ko[2] = {K_dev, K_dev + n2};
-    s.jk(Dj_dev, nk, Dk, J_dev, Ko, precision);
+    if (precision < PYFACC_PRECISION_FP64 || precision > PYFACC_PRECISION_FP32)
+      throw Error(PYFACC_ERR_INVALID, "precision must be PYFACC_PRECISION_FP64, _MIXED or _FP32");
+    PF_CUDA(cudaMemsetAsync(s.stats_dev, 0, sizeof(pyfacc::JkStats), s.stream));
+    PF_CUDA(cudaEventRecord(s.ev0, s.stream));
+    if (precision == PYFACC_PRECISION_FP32)  // every quartet in FP32, lists built on the device
+      s.jk(Dj_dev, nk, Dk, J_dev, Ko, PYFACC_PRECISION_MIXED, true, -1.0, 1e300);
+    else
+      s.jk(Dj_dev, nk, Dk, J_dev, Ko, precision);
+    PF_CUDA(cudaEventRecord(s.ev1, s.stream));
     PF_CUDA(cudaStreamSynchronize(s.stream));
+    double c[6];
+    s.jk_counters(nk, c);
+    s.last_jk[0] = s.elapsed(s.ev0, s.ev1);
+    for (int k = 0; k < 6; ++k) s.last_jk[1 + k] = c[k];
   });
+}
+
+int pyfacc_system_jk_stats(const pyfacc_system* sys, double* out, int n) {
+  if (!sys || !out || n <= 0) return PYFACC_ERR_INVALID;
+  for (int k = 0; k < n; ++k) out[k] = k < 7 ? sys->impl->last_jk[k] : 0.0;
+  return PYFACC_OK;
 }
 
 int pyfacc_system_eri_tensor(pyfacc_system* sys, double* eri_dev) {
@@ -387,6 +405,39 @@ int pyfacc_boys_dev(int mode, int fp32, int mmax, int n, const double* x_dev, do
     pyfacc::launch_boys_test(mode, fp32, mmax, n, x_dev, out_dev, 0);
     PF_CUDA(cudaDeviceSynchronize());
   });
+}
+
+int pyfacc_dense_gemm_dev(int m, int n, int k, int ta, const double* A_dev, int tb, const double* B_dev,
+                          double* C_dev, int sym, int asym_a) {
+  if (m < 0 || n < 0 || k < 0 || (m * n > 0 && (!A_dev || !B_dev || !C_dev))) return PYFACC_ERR_INVALID;
+  return guarded([&] {
+    const int lda = ta ? m : k, ldb = tb ? k : n;
+    pyfacc::launch_dgemm(m, n, k, ta != 0, A_dev, lda, tb != 0, B_dev, ldb, C_dev, n, 1.0, nullptr, n, 0.0, sym != 0,
+                         asym_a != 0, 0);
+    PF_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+int pyfacc_purify_dev(int n, int nocc, const double* F_dev, double* P_dev, int* steps) {
+  if (n <= 0 || nocc < 0 || nocc > n || !F_dev || !P_dev || F_dev == P_dev) return PYFACC_ERR_INVALID;
+  int status = PYFACC_OK;
+  const int st = guarded([&] {
+    const size_t n2 = (size_t)n * n;
+    pyfacc::DeviceBuf work;
+    work.ensure(2 * n2 * sizeof(double) + 64 * sizeof(double));
+    double* Xb = work.as<double>();
+    double* state = Xb + n2 + n2;
+    // the projector is built in P_dev itself (the graph's X_a)
+    cudaGraphExec_t g = pyfacc::build_tc2_graph(n, nocc, F_dev, P_dev, Xb, state, pyfacc::TC2_KMAX);
+    const cudaError_t e = cudaGraphLaunch(g, 0);
+    double ctl[8];
+    cudaError_t e2 = e == cudaSuccess ? cudaMemcpy(ctl, state + 8, sizeof(ctl), cudaMemcpyDeviceToHost) : e;
+    cudaGraphExecDestroy(g);
+    PF_CUDA(e2);
+    if (steps) *steps = (int)ctl[2];
+    if (ctl[1] == 0.0 || ctl[4] != 0.0) status = PYFACC_ERR_NOT_CONVERGED;
+  });
+  return st != PYFACC_OK ? st : status;
 }
 
 int pyfacc_partition(int n, const double* cost, int parts, int* bounds) {

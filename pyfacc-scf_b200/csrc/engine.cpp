@@ -55,28 +55,26 @@ void DeviceBuf::release() {
   } while (0)
 
 // ------------------------------------------------------------------ setup
-System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
+// Argument checks shared by the single-molecule and batched engines, made
+// before any device work so that bad input is reported the same way with
+// or without a GPU.  The reference reads whatever the XYZ file holds
+// (helper_functions.py:25-54); a NaN or infinite coordinate would reach the
+// integrals there, here it is PYFACC_ERR_INVALID.
+void validate_molecule(const pyfacc_molecule& m) {
   if (m.natoms <= 0 || !m.z || !m.coords || !m.basis) throw Error(PYFACC_ERR_INVALID, "empty molecule");
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(PYFACC_ERR_NO_DEVICE, "no CUDA device");
-  if (opt.device >= 0) {
-    device = opt.device;
-    PF_CUDA(cudaSetDevice(device));
-  } else {
-    PF_CUDA(cudaGetDevice(&device));
-  }
-  PF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  for (int i = 0; i < 3 * m.natoms; ++i)
+    if (!std::isfinite(m.coords[i]))
+      throw Error(PYFACC_ERR_INVALID, "coordinate " + std::to_string(i % 3) + " of atom " + std::to_string(i / 3) +
+                                          " is not finite");
+}
+
+System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
+  validate_molecule(m);
   if (opt.task_width != 0 && opt.task_width != 8 && opt.task_width != 16 && opt.task_width != 32)
     throw Error(PYFACC_ERR_INVALID, "task_width must be 0, 8, 16 or 32");
   if (opt.task_width) task_width = opt.task_width;
-  ensure_boys_tables(device);
-  ctx = context_acquire(device);
-  stream = ctx.stream;
-  cublas = ctx.cublas;
-  cusolver = ctx.cusolver;
-  ev0 = ctx.ev0;
-  ev1 = ctx.ev1;
-
+  // host-side parsing first: argument, element and basis errors are
+  // reported before (and without) any device work
   natoms = m.natoms;
   Z.assign(m.z, m.z + natoms);
   xyz.assign(m.coords, m.coords + 3 * natoms);
@@ -106,6 +104,23 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
   ns = (int)basis.shells.size();
   uhf = (opt.scf_type == PYFACC_SCF_UHF) || (opt.scf_type == PYFACC_SCF_AUTO && nalpha != nbeta);
   e_nuc = nuclear_repulsion();
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw Error(PYFACC_ERR_NO_DEVICE, "no CUDA device");
+  if (opt.device >= 0) {
+    device = opt.device;
+    PF_CUDA(cudaSetDevice(device));
+  } else {
+    PF_CUDA(cudaGetDevice(&device));
+  }
+  PF_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+  ensure_boys_tables(device);
+  ctx = context_acquire(device);
+  stream = ctx.stream;
+  cublas = ctx.cublas;
+  cusolver = ctx.cusolver;
+  ev0 = ctx.ev0;
+  ev1 = ctx.ev1;
+
   using clk = std::chrono::steady_clock;
   const auto c0 = clk::now();
   upload_shells();
@@ -139,6 +154,7 @@ void System::spin_electrons(const std::vector<std::string>& sp, int chg, int* na
   if (all_same && sp.size() == 2 && sp[0] == "O") mult = 3;
   if (all_same && sp.size() == 2 && sp[0] == "N") mult = 4;
   const int twoS = mult - 1;
+  if (total < 0) throw Error(PYFACC_ERR_INVALID, "charge exceeds the nuclear charge (negative electron count)");
   if ((total + twoS) % 2 != 0) throw Error(PYFACC_ERR_INVALID, "Inconsistent electron count and spin state.");
   *na = (total + twoS) / 2;
   *nb = total - *na;
@@ -550,7 +566,7 @@ void System::build_tasks() {
 void System::alloc_matrices() {
   const size_t n2 = (size_t)nbf * nbf;
   const int nmat = 28 + 4 * std::max(opt.diis_size, 1);
-  mats.ensure(nmat * n2 * sizeof(double) + 64 * sizeof(double) + ns * ns * sizeof(float) + 1024);
+  mats.ensure(nmat * n2 * sizeof(double) + 96 * sizeof(double) + ns * ns * sizeof(float) + 1024);
   double* m = mats.as<double>();
   auto take = [&]() { double* r = m; m += n2; return r; };
   S = take(); T = take(); Vm = take(); H = take(); X = take();
@@ -565,7 +581,7 @@ void System::alloc_matrices() {
     diis_E.push_back(m); m += 2 * n2;
   }
   small = m; m += 48;
-  pstate = m; m += 16;
+  pstate = m; m += 48;  // purification graph state (24 doubles used)
   dmax = reinterpret_cast<float*>(m);
   small_buf.ensure(2 * nbf * sizeof(double) + 256 + sizeof(JkStats) + 256 + 64 * sizeof(double*) + 256 +
                    3 * natoms * sizeof(double) + 256 + 256);

@@ -67,6 +67,9 @@ constexpr int COARSE_MAX_ITER = 20;
 // derivative polynomials) stay below ~1e9 for STO-nG exponents and
 // molecules of up to ~2000 atoms, so a left-out entry is below 1e-16.
 constexpr double ONE_E_PAIR_CUT = 1e-25;
+// smallest Cholesky pivot L_ii^2 of the overlap matrix (unit diagonal) below
+// which it counts as linearly dependent (PYFACC_ERR_LINDEP)
+constexpr double LINDEP_PIVOT = 1e-10;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
 
 // ---------------------------------------------------------------- host basis
@@ -81,6 +84,10 @@ struct Basis {
   std::vector<int> bf_off;  // nshell + 1
   int nbf = 0;
 };
+
+// Argument checks of a molecule (engine.cpp): pointers and finite
+// coordinates; throws PYFACC_ERR_INVALID.
+void validate_molecule(const pyfacc_molecule& m);
 
 // Diagonal atomic-occupation guess of a minimal basis (scf.cpp).
 std::vector<double> atomic_occupations(const Basis& basis, const std::vector<int>& Z, int nelec);
@@ -282,6 +289,20 @@ void launch_gersh(int n, const double* F, double* state, cudaStream_t s);
 void launch_tc2_init(int n, const double* F, const double* state, double* X, cudaStream_t s);
 void launch_tc2_step(int n, double nocc, const double* Xin, const double* X2, double* Xout, const double* sin,
                      double* sout, cudaStream_t s);
+
+// FP64 tensor-core products of row-major matrices (dense.cu):
+// C = alpha op(A) op(B) + beta Y (Y may be null), op = transpose when ta/tb;
+// sym: the result is symmetric, only its upper-triangle tiles are computed
+// and mirrored; asym_a: op(A) = A - A^T (not with ta).
+void launch_dgemm(int m, int n, int k, bool ta, const double* A, int lda, bool tb, const double* B, int ldb,
+                  double* C, int ldc, double alpha, const double* Y, int ldy, double beta, bool sym, bool asym_a,
+                  cudaStream_t s);
+// TC2 purification of the n x n matrix Fp into the projector on its nocc
+// lowest eigenvectors as one graph (bounds, X_0 into Xa, a conditional WHILE
+// loop of fused steps Xa -> Xb -> Xa); st holds >= 24 doubles of state, of
+// which st[9] (done), st[10] (steps) and st[12] (failed) give the outcome.
+cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, double* Xb, double* st, int kmax);
+constexpr int TC2_KMAX = 200;
 
 double probe_fp64(int device, double* fp32);
 

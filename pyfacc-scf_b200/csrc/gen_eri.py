@@ -66,6 +66,26 @@ def cname(c):
     return f"{c[0]}{c[1]}{c[2]}"
 
 
+def scaled(c, name):
+    """c * name for a small positive integer c, in the kernel's type R."""
+    return name if c == 1 else f"(R({c}.0f) * {name})"
+
+
+def fma_chain(terms, tail=None):
+    """sum of the products a * b of terms (+ tail) as nested pf_fma calls,
+    so that the code maps onto FMA instructions for every R (double, float
+    and the packed float pair, whose pf_fma is one FFMA2)."""
+    if tail is None:
+        a, b = terms[-1]
+        expr = f"{a} * {b}"
+        terms = terms[:-1]
+    else:
+        expr = tail
+    for a, b in reversed(terms):
+        expr = f"pf_fma({a}, {b}, {expr})"
+    return expr
+
+
 class Emitter:
     def __init__(self):
         self.lines = []
@@ -98,27 +118,24 @@ class Vrr:
         elif lsum(f) == 0:
             i = first_axis(e)
             e1 = down(e, i)
-            terms, fl = [f"PA[{i}] * {self.V(e1, f, m)}", f"WP[{i}] * {self.V(e1, f, m + 1)}"], 3
+            terms, fl = [(f"PA[{i}]", self.V(e1, f, m)), (f"WP[{i}]", self.V(e1, f, m + 1))], 3
             if e1[i] > 0:
                 e2 = down(e1, i)
-                c = f"{e1[i]}.0 * " if e1[i] > 1 else ""
-                terms.append(f"{c}o2p * ({self.V(e2, f, m)} - rp * {self.V(e2, f, m + 1)})")
+                terms.append((scaled(e1[i], "o2p"), f"pf_fma(nrp, {self.V(e2, f, m + 1)}, {self.V(e2, f, m)})"))
                 fl += 4 + (1 if e1[i] > 1 else 0)
-            r = em.tmp(" + ".join(terms), fl)
+            r = em.tmp(fma_chain(terms), fl)
         else:
             i = first_axis(f)
             f1 = down(f, i)
-            terms, fl = [f"QC[{i}] * {self.V(e, f1, m)}", f"WQ[{i}] * {self.V(e, f1, m + 1)}"], 3
+            terms, fl = [(f"QC[{i}]", self.V(e, f1, m)), (f"WQ[{i}]", self.V(e, f1, m + 1))], 3
             if f1[i] > 0:
                 f2 = down(f1, i)
-                c = f"{f1[i]}.0 * " if f1[i] > 1 else ""
-                terms.append(f"{c}o2q * ({self.V(e, f2, m)} - rq * {self.V(e, f2, m + 1)})")
+                terms.append((scaled(f1[i], "o2q"), f"pf_fma(nrq, {self.V(e, f2, m + 1)}, {self.V(e, f2, m)})"))
                 fl += 4 + (1 if f1[i] > 1 else 0)
             if e[i] > 0:
-                c = f"{e[i]}.0 * " if e[i] > 1 else ""
-                terms.append(f"{c}o2pq * {self.V(down(e, i), f1, m + 1)}")
+                terms.append((scaled(e[i], "o2pq"), self.V(down(e, i), f1, m + 1)))
                 fl += 2 + (1 if e[i] > 1 else 0)
-            r = em.tmp(" + ".join(terms), fl)
+            r = em.tmp(fma_chain(terms), fl)
         self.memo[key] = r
         return r
 
@@ -140,7 +157,7 @@ class Hrr:
             r = self.base(a, f)
         else:
             i = first_axis(b)
-            r = self.em.tmp(f"{self.bra(up(a, i), down(b, i), f)} + AB[{i}] * {self.bra(a, down(b, i), f)}", 2)
+            r = self.em.tmp(f"pf_fma(AB[{i}], {self.bra(a, down(b, i), f)}, {self.bra(up(a, i), down(b, i), f)})", 2)
         self.mb[key] = r
         return r
 
@@ -152,7 +169,8 @@ class Hrr:
             r = self.bra(a, b, c)
         else:
             i = first_axis(d)
-            r = self.em.tmp(f"{self.full(a, b, up(c, i), down(d, i))} + CD[{i}] * {self.full(a, b, c, down(d, i))}", 2)
+            r = self.em.tmp(f"pf_fma(CD[{i}], {self.full(a, b, c, down(d, i))}, {self.full(a, b, up(c, i), down(d, i))})",
+                            2)
         self.mk[key] = r
         return r
 
@@ -189,11 +207,11 @@ def gen_class(la, lb, lc, ld):
         em.flops += 1
     vrr_flops = em.flops
     src.append("  __device__ static __forceinline__ void vrr(const R* __restrict__ I, const R* __restrict__ PA,")
-    src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
-    src.append("      R o2q, R rq, R o2pq, R* __restrict__ acc) {")
+    src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R nrp,")
+    src.append("      R o2q, R nrq, R o2pq, R* __restrict__ acc) {")
     src.extend(em.lines)
     src.extend(acc_lines)
-    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)nrp; (void)o2q; (void)nrq; (void)o2pq;")
     src.append("  }")
     # --- hrr
     em = Emitter()
@@ -235,20 +253,19 @@ def gen_class(la, lb, lc, ld):
                             q = [a, b, c, d]
                             qu = list(q)
                             qu[ctr] = up(q[ctr], x)
-                            up_terms.append(f"gam[{k}] * {h.full(*qu)}")
+                            up_terms.append((f"gam[{k}]", h.full(*qu)))
                             cnt = q[ctr][x]
                             if cnt > 0:
                                 qd = list(q)
                                 qd[ctr] = down(q[ctr], x)
-                                cc = f"{cnt}.0 * " if cnt > 1 else ""
-                                dn_terms.append(f"{cc}gam[{k}] * {h.full(*qd)}")
+                                dn_terms.append((scaled(cnt, f"gam[{k}]"), h.full(*qd)))
                             k += 1
-            su = em.tmp(" + ".join(up_terms), 2 * len(up_terms) - 1)
+            su = em.tmp(fma_chain(up_terms), 2 * len(up_terms) - 1)
             expr = f"tw * {su}"
             fl = 2
             if dn_terms:
-                sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
-                expr += f" - {sd}"
+                sd = em.tmp(fma_chain(dn_terms), 2 * len(dn_terms) - 1)
+                expr = f"pf_fma(tw, {su}, R(-1.0f) * {sd})"
                 fl += 1
             em.flops += fl
             outs.append(expr)
@@ -256,13 +273,13 @@ def gen_class(la, lb, lc, ld):
         c = 'ABC'[ctr]
         src.append(f"  // centre {c}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
         src.append(f"  __device__ static __noinline__ void grad{c}(const R* __restrict__ I, const R* __restrict__ PA,")
-        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
-        src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R nrp,")
+        src.append("      R o2q, R nrq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
         src.append("      R tw, const R* __restrict__ gam, R* __restrict__ g) {")
         src.extend(em.lines)
         for x in range(3):
             src.append(f"    g[{x}] += {outs[x]};")
-        src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+        src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)nrp; (void)o2q; (void)nrq; (void)o2pq;")
         src.append("    (void)AB; (void)CD;")
         src.append("  }")
     for ctr in range(0 if L >= 4 else 3):
@@ -279,41 +296,40 @@ def gen_class(la, lb, lc, ld):
                             q = [a, b, c, d]
                             qu = list(q)
                             qu[ctr] = up(q[ctr], x)
-                            up_terms.append(f"gam[{k}] * {h.full(*qu)}")
+                            up_terms.append((f"gam[{k}]", h.full(*qu)))
                             cnt = q[ctr][x]
                             if cnt > 0:
                                 qd = list(q)
                                 qd[ctr] = down(q[ctr], x)
-                                cc = f"{cnt}.0 * " if cnt > 1 else ""
-                                dn_terms.append(f"{cc}gam[{k}] * {h.full(*qd)}")
+                                dn_terms.append((scaled(cnt, f"gam[{k}]"), h.full(*qd)))
                             k += 1
-            su = em.tmp(" + ".join(up_terms), 2 * len(up_terms) - 1)
+            su = em.tmp(fma_chain(up_terms), 2 * len(up_terms) - 1)
             expr = f"tw * {su}"
             fl = 2
             if dn_terms:
-                sd = em.tmp(" + ".join(dn_terms), 2 * len(dn_terms) - 1)
-                expr += f" - {sd}"
+                sd = em.tmp(fma_chain(dn_terms), 2 * len(dn_terms) - 1)
+                expr = f"pf_fma(tw, {su}, R(-1.0f) * {sd})"
                 fl += 1
             em.flops += fl
             grad_flops += em.flops
             name = f"grad{'ABC'[ctr]}{'xyz'[x]}"
             src.append(f"  __device__ static __forceinline__ R {name}(const R* __restrict__ I, const R* __restrict__ PA,")
-            src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
-            src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+            src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R nrp,")
+            src.append("      R o2q, R nrq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
             src.append("      R tw, const R* __restrict__ gam) {")
             src.extend(em.lines)
             src.append(f"    return {expr};")
-            src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)rp; (void)o2q; (void)rq; (void)o2pq;")
+            src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)nrp; (void)o2q; (void)nrq; (void)o2pq;")
             src.append("    (void)AB; (void)CD;")
             src.append("  }")
         c = 'ABC'[ctr]
         src.append(f"  // centre {c}: g[x] += tw * sum gam (..+1x..) - sum gam n_x (..-1x..), tw = 2 exponent")
         src.append(f"  __device__ static __forceinline__ void grad{c}(const R* __restrict__ I, const R* __restrict__ PA,")
-        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R rp,")
-        src.append("      R o2q, R rq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
+        src.append("      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R nrp,")
+        src.append("      R o2q, R nrq, R o2pq, const R* __restrict__ AB, const R* __restrict__ CD,")
         src.append("      R tw, const R* __restrict__ gam, R* __restrict__ g) {")
         for x in range(3):
-            src.append(f"    g[{x}] += grad{c}{'xyz'[x]}(I, PA, WP, QC, WQ, o2p, rp, o2q, rq, o2pq, AB, CD, tw, gam);")
+            src.append(f"    g[{x}] += grad{c}{'xyz'[x]}(I, PA, WP, QC, WQ, o2p, nrp, o2q, nrq, o2pq, AB, CD, tw, gam);")
         src.append("  }")
     src.append(f"  static constexpr int VRR_FLOPS = {vrr_flops};")
     src.append(f"  static constexpr int HRR_FLOPS = {hrr_flops};")
@@ -446,6 +462,11 @@ def generate() -> str:
     parts = ["// Generated by gen_eri.py -- do not edit by hand.",
              "// Obara-Saika VRR / Head-Gordon-Pople HRR for s/p shell quartets.",
              "#pragma once", "",
+             "// Multiply-add of the class routines: the scalar FMA for double and float;",
+             "// a packed type supplies its own pf_fma (found by argument lookup).",
+             "__device__ __forceinline__ double pf_fma(double a, double b, double c) { return __fma_rn(a, b, c); }",
+             "__device__ __forceinline__ float pf_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }",
+             "",
              "template <typename R, int LA, int LB, int LC, int LD> struct EriClass;",
              "template <typename R, int LA, int LB> struct NucClass;", ""]
     table = []

@@ -177,7 +177,7 @@ template <typename R>
 struct PrimGeo {
   R I[PF_BOYS_MMAX + 1];
   R WP[3], WQ[3];
-  R o2p, rp, o2q, rq, o2pq;
+  R o2p, nrp, o2q, nrq, o2pq;  // nrp = -rho/p, nrq = -rho/q
 };
 
 template <typename R> struct Rec;  // primitive-pair record vector of a precision
@@ -209,8 +209,8 @@ __device__ __forceinline__ void prim_setup(const V& b0, const V& b1, const V& k0
   g.WQ[0] = pz * PQx;  g.WQ[1] = pz * PQy;  g.WQ[2] = pz * PQz;
   g.o2p = (R)b0.y;
   g.o2q = (R)k0.y;
-  g.rp = qz;  // rho / p
-  g.rq = pz;  // rho / q
+  g.nrp = -qz;  // -rho / p
+  g.nrq = -pz;  // -rho / q
   g.o2pq = (R)0.5 * oz;
 }
 
@@ -251,13 +251,101 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
       const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
       PrimGeo<R> g;
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
-      C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.rp, g.o2q, g.rq, g.o2pq, acc);
+      C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.nrp, g.o2q, g.nrq, g.o2pq, acc);
       ++nprim;
     }
   }
   const R AB[3] = {(R)bgeo.x, (R)bgeo.y, (R)bgeo.z};
   const R CD[3] = {(R)kgeo.x, (R)kgeo.y, (R)kgeo.z};
   C::hrr(acc, AB, CD, out);
+  return nprim;
+}
+
+// The FP32 contracted quartet with two bra primitives per step in packed
+// float pairs (FFMA2, f2.cuh): the same primitive quartets, cuts and sums as
+// contracted_quartet<float>, but each Obara-Saika step of the generated
+// recursion does the work of both primitives in one instruction.  An odd
+// bra primitive count, or a second primitive below the cut, fills the upper
+// half with the lower primitive at zero weight.
+template <int L>
+__device__ __forceinline__ void prim_setup_f2(const float4& blo0, const float4& blo1, const float4& bhi0,
+                                              const float4& bhi1, float khi_weight, const float4& k0,
+                                              const float4& k1, PrimGeo<F2>& g) {
+  const F2 p(blo0.x, bhi0.x), q(k0.x);
+  const F2 PQx = F2(blo1.x, bhi1.x) + F2(-k1.x), PQy = F2(blo1.y, bhi1.y) + F2(-k1.y),
+           PQz = F2(blo1.z, bhi1.z) + F2(-k1.z);
+  const F2 zeta = p + q;
+  const F2 rs(rsqrtf(zeta.v.x), rsqrtf(zeta.v.y));
+  const F2 oz = rs * rs;
+  const F2 rho = p * q * oz;
+  const F2 T = rho * pf_fma(PQx, PQx, pf_fma(PQy, PQy, PQz * PQz));
+  const F2 pref = F2(blo0.z, bhi0.z * khi_weight) * F2(k0.z) * rs;
+  F2 F[L + 1];
+  boys_fp32x2<L>(T, F);
+#pragma unroll
+  for (int m = 0; m <= L; ++m) g.I[m] = pref * F[m];
+  const F2 qz = q * oz, pz = p * oz;
+  const F2 nqz = qz * F2(-1.0f);
+  g.WP[0] = nqz * PQx; g.WP[1] = nqz * PQy; g.WP[2] = nqz * PQz;
+  g.WQ[0] = pz * PQx;  g.WQ[1] = pz * PQy;  g.WQ[2] = pz * PQz;
+  g.o2p = F2(blo0.y, bhi0.y);
+  g.o2q = F2(k0.y);
+  g.nrp = nqz;               // -rho / p
+  g.nrq = pz * F2(-1.0f);    // -rho / q
+  g.o2pq = F2(0.5f) * oz;
+}
+
+template <int LA, int LB, int LC, int LD>
+__device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ prim, int4 bi0, int4 ki0,
+                                                     const double4& bgeo, const double4& kgeo,
+                                                     float out[EriClass<float, LA, LB, LC, LD>::NOUT],
+                                                     double kcut = 0.0, int kq0 = 0, int kq_step = 1) {
+  using C2 = EriClass<F2, LA, LB, LC, LD>;
+  using C1 = EriClass<float, LA, LB, LC, LD>;
+  F2 acc[C2::NACC];
+#pragma unroll
+  for (int i = 0; i < C2::NACC; ++i) acc[i] = F2(0.0f);
+  const float cut = (float)kcut;
+  const float kab_max = fabsf(prim[3 * (size_t)bi0.z].z);
+  int nprim = 0;
+  for (int kq = kq0; kq < ki0.w; kq += kq_step) {
+    const float4* kr = prim + 3 * (size_t)(ki0.z + kq);
+    const float4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const float kcd = fabsf(k0.z);
+    if (kab_max * kcd < cut) break;
+    const F2 QC[3] = {F2(k2.x), F2(k2.y), F2(k2.z)};
+#pragma unroll 1
+    for (int kp = 0; kp < bi0.w; kp += 2) {
+      const float4* br = prim + 3 * (size_t)(bi0.z + kp);
+      const float4 b0 = br[0], b1 = br[1], b2 = br[2];
+      if (fabsf(b0.z) * kcd < cut) break;
+      // the second primitive, or the first again at zero weight
+      bool two = kp + 1 < bi0.w;
+      float4 c0 = b0, c1 = b1, c2 = b2;
+      if (two) {
+        c0 = br[3];
+        two = fabsf(c0.z) * kcd >= cut;
+        if (two) {
+          c1 = br[4];
+          c2 = br[5];
+        } else {
+          c0 = b0;
+        }
+      }
+      const F2 PA[3] = {F2(b2.x, c2.x), F2(b2.y, c2.y), F2(b2.z, c2.z)};
+      PrimGeo<F2> g;
+      prim_setup_f2<C2::L>(b0, b1, c0, c1, two ? 1.0f : 0.0f, k0, k1, g);
+      C2::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.nrp, g.o2q, g.nrq, g.o2pq, acc);
+      nprim += two ? 2 : 1;
+      if (!two) break;
+    }
+  }
+  float accs[C1::NACC];
+#pragma unroll
+  for (int i = 0; i < C1::NACC; ++i) accs[i] = acc[i].v.x + acc[i].v.y;
+  const float AB[3] = {(float)bgeo.x, (float)bgeo.y, (float)bgeo.z};
+  const float CD[3] = {(float)kgeo.x, (float)kgeo.y, (float)kgeo.z};
+  C1::hrr(accs, AB, CD, out);
   return nprim;
 }
 
@@ -495,7 +583,12 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     R out[C::NOUT];
     int nprim = 0;
     if (active) {
-      nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut, slice, ps);
+      // FP32 quartets: two primitives per step in packed pairs, except
+      // (pp|pp), whose 81 packed accumulators would not fit the registers
+      if constexpr (sizeof(R) == 4 && C::L < 4)
+        nprim = contracted_quartet_f2<LA, LB, LC, LD>(args.primf, bi0, ki0, bg, kg, out, kcut, slice, ps);
+      else
+        nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut, slice, ps);
     } else {
 #pragma unroll
       for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
@@ -945,11 +1038,11 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
           const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
           PrimGeo<R> pg;
           prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
-          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, (R)(2 * b0.w), gam,
+          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * b0.w), gam,
                    gr);
-          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD,
+          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD,
                    (R)(2 * (b0.x - b0.w)), gam, gr + 3);
-          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.rp, pg.o2q, pg.rq, pg.o2pq, AB, CD, (R)(2 * k0.w), gam,
+          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * k0.w), gam,
                    gr + 6);
         }
       }

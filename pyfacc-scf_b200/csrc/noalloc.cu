@@ -24,6 +24,12 @@
 // uploads the Boys tables.  That first call should come before any stream
 // capture on the device.
 //
+// Stream: the work runs on the legacy default stream, which waits for the
+// caller's blocking streams but not for streams created non-blocking (torch's
+// side streams, for instance).  Whatever writes D_dev on such a stream must
+// have finished (stream or event synchronised) before the call; J_dev and
+// K_dev are complete when it returns.
+//
 // Sharing: every call uses the same array and leaves the last call's data in
 // it.  Two calls whose work overlapped on the GPU would race on it, so calls
 // from this process take a lock and return only after their kernels have
@@ -84,9 +90,7 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
     using namespace pyfacc;
     int dev = 0;
     PF_CUDA(cudaGetDevice(&dev));
-    unsigned char* base = scratch_on(dev);
-    ensure_boys_tables(dev);
-    cudaStream_t s = 0;
+    cudaStream_t s = 0;  // the legacy default stream (see the header comment)
 
     // ---- basis (host)
     const int natoms = mol->natoms;
@@ -160,7 +164,9 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
                                           " bytes of scratch, the static array holds " +
                                           std::to_string((size_t)PYFACC_NOALLOC_SCRATCH_BYTES));
 
-    // ---- carve the array
+    // ---- device set-up (first call on this device) and carving of the array
+    unsigned char* base = scratch_on(dev);
+    ensure_boys_tables(dev);
     Carver cv{base};
     ShellDev shd;
     shd.ns = ns;

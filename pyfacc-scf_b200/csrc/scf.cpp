@@ -109,6 +109,20 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   st.n_fock++;
 }
 
+void System::jk_counters(int nk, double out[6]) {
+  JkStats js;
+  PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < 6; ++k) out[k] = 0.0;
+  for (int p = 0; p < 2; ++p)
+    for (int q = 0; q < NQCLASS; ++q) {
+      const ClassFlops& cf = class_flops(q);
+      out[p] += (double)js.prims[p][q] * (cf.vrr + prim_overhead_flops(q, p == 1)) +
+                (double)js.quartets[p][q] * (cf.hrr + digest_flops(q, nk));
+      out[2 + p] += (double)js.quartets[p][q];
+      out[4 + p] += (double)js.prims[p][q];
+    }
+}
+
 void System::reduce(double* data, long long count) {
   PF_CUDA(cudaStreamSynchronize(stream));
   const int rc = reducer(reducer_ctx, data, count);
@@ -140,10 +154,22 @@ void System::orthogonalizer() {
   PF_CUSOLVER(cusolverDnDpotrf(cusolver, CUBLAS_FILL_MODE_LOWER, nbf, L, nbf, syev_work.as<double>(), lwork,
                                info_dev));
   int info = 0;
+  std::vector<double> piv(nbf);
   PF_CUDA(cudaMemcpyAsync(&info, info_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaMemcpy2DAsync(piv.data(), sizeof(double), L, (size_t)(nbf + 1) * sizeof(double), sizeof(double), nbf,
+                            cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   if (info > 0) throw Error(PYFACC_ERR_LINDEP, "overlap matrix is not positive definite");
   if (info < 0) throw Error(PYFACC_ERR_CUDA, "overlap factorisation failed");
+  // Cholesky pivots L_ii^2 bound the smallest eigenvalue of S from above;
+  // coincident atoms give a pivot at round-off level without a negative
+  // one.  la.f90:40-44 warns below an eigenvalue of 1e-8 and goes on into
+  // 1/sqrt of it; here a pivot below 1e-10 (S_ii = 1) is reported.
+  double pmin = 1e300;
+  for (double d : piv) pmin = std::min(pmin, d * d);
+  if (!(pmin >= LINDEP_PIVOT))
+    throw Error(PYFACC_ERR_LINDEP, "overlap matrix is numerically singular (smallest Cholesky pivot " +
+                                       std::to_string(pmin) + "; coincident atoms?)");
   launch_identity(nbf, X, stream);
   const double one = 1.0;
   PF_CUBLAS(cublasDtrsm(cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nbf, nbf,
@@ -204,96 +230,46 @@ std::vector<double> System::atomic_occupations() const {
   return pyfacc::atomic_occupations(basis, Z, nalpha + nbeta);
 }
 
+// The buffer X holds, read row-major, R = L^{-1} (cuBLAS wrote X = L^{-T}
+// column-major), so X^T F X = R F R^T and X P' X^T = R^T P' R in the
+// row-major products of dense.cu.
 bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
-  const double one = 1.0, zero = 0.0;
+  const int n = nbf;
   if (nocc <= 0) {
-    launch_zero(Pm, (size_t)nbf * nbf * sizeof(double), stream);
+    launch_zero(Pm, (size_t)n * n * sizeof(double), stream);
     return true;
   }
-  if (nocc >= nbf) {  // every orbital occupied: P = scale * X X^T = scale * S^-1
-    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, X, nbf, X, nbf, &zero, Pm, nbf));
+  if (nocc >= n) {  // every orbital occupied: P = scale * X X^T = scale * S^-1
+    launch_dgemm(n, n, n, true, X, n, false, X, n, Pm, n, scale, nullptr, n, 0.0, true, false, stream);
     return true;
   }
   double* Fp = Pu[0];
   double* Xa = Pu[1];
-  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, Fm, nbf, X, nbf, &zero, W1, nbf));
-  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W1, nbf, &zero, Fp, nbf));
-  // one cuBLAS DGEMM + one update kernel per step, the state double-buffered
-  // on the device, four steps per graph replay; the host checks first after
-  // as many steps as the last purification of this occupation took (16 the
-  // first time), then every 4 (converged steps only copy X).  Successive SCF
-  // iterations need about the same number of steps, so most purifications
-  // cost one host round trip instead of four.
-  double* S0 = pstate;
-  launch_gersh(nbf, Fp, S0, stream);
-  launch_tc2_init(nbf, Fp, S0, Xa, stream);
-  cudaGraphExec_t g4 = tc2_graph(nocc);
-  const int kmax = 200;
-  double st_h[8] = {0};
-  bool ok = false;
-  int k = 0;
-  int* last = nullptr;
-  for (auto& e : tc2_last)
-    if (e.first == nocc) last = &e.second;
-  if (!last) {
-    tc2_last.emplace_back(nocc, 16);
-    last = &tc2_last.back().second;
-  }
-  const int first = std::min(std::max((*last + 3) / 4 * 4, 4), 64);
-  while (k < kmax) {
-    const int chunk = (k == 0) ? first : 4;
-    for (int j = 0; j < chunk; j += 4, k += 4) {
-      PF_CUDA(cudaGraphLaunch(g4, stream));
-      count_launches(4);
-    }
-    PF_CUDA(cudaMemcpyAsync(st_h, S0, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PF_CUDA(cudaStreamSynchronize(stream));
-    if (st_h[4] != 0.0) {
-      ok = true;
-      break;
-    }
-  }
-  purify_steps += (int)st_h[5];
-  if (!ok) return false;
-  *last = (int)st_h[5];
-  const double* Xp = Xa;  // after a multiple of four steps the iterate is back in Xa
-  // P = scale * X Xp X^T
-  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, Xp, nbf, &zero, W1, nbf));
-  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, nbf, &scale, W1, nbf, X, nbf, &zero, Pm, nbf));
+  // F' = R F R^T
+  launch_dgemm(n, n, n, false, Fm, n, true, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
+  launch_dgemm(n, n, n, false, X, n, false, W1, n, Fp, n, 1.0, nullptr, n, 0.0, true, false, stream);
+  // the whole TC2 iteration is one graph launch (conditional WHILE loop on
+  // the device); the host reads the outcome once
+  PF_CUDA(cudaGraphLaunch(tc2_graph(nocc), stream));
+  double ctl[8];
+  PF_CUDA(cudaMemcpyAsync(ctl, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaStreamSynchronize(stream));
+  const int steps = (int)ctl[2];
+  count_launches(2 + steps + (steps & 1));
+  purify_steps += steps;
+  if (ctl[1] == 0.0 || ctl[4] != 0.0) return false;
+  // P = scale R^T Xp R
+  launch_dgemm(n, n, n, false, Xa, n, false, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
+  launch_dgemm(n, n, n, true, X, n, false, W1, n, Pm, n, scale, nullptr, n, 0.0, true, false, stream);
   return true;
 }
 
-// Four TC2 steps X_a -> X_b -> X_a -> X_b -> X_a (state S0 -> S1 -> S0 ...),
-// captured once per occupation number: after four steps the iterate and the
-// state are back in X_a and S0, so the graph can be replayed.  (A single
-// cooperative launch for the whole iteration, grid barriers between steps,
-// measured slower than these replays at every size tried on B200.)
+// The purification graph of one occupation number (dense.cu): built once
+// per system and occupation, replayed by every purify() of that occupation.
 cudaGraphExec_t System::tc2_graph(int nocc) {
   for (auto& g : tc2_graphs)
     if (g.first == nocc) return g.second;
-  const double one = 1.0, zero = 0.0;
-  double* bufs[2] = {Pu[1], Pu[3]};
-  double* st[2] = {pstate, pstate + 8};
-  cudaGraph_t graph = nullptr;
-  PF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-  try {
-    for (int k = 0; k < 4; ++k) {
-      double* cur = bufs[k % 2];
-      double* nxt = bufs[(k + 1) % 2];
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, cur, nbf, cur, nbf, &zero, Pu[2],
-                            nbf));
-      launch_tc2_step(nbf, (double)nocc, cur, Pu[2], nxt, st[k % 2], st[(k + 1) % 2], stream);
-    }
-  } catch (...) {
-    cudaStreamEndCapture(stream, &graph);
-    if (graph) cudaGraphDestroy(graph);
-    throw;
-  }
-  PF_CUDA(cudaStreamEndCapture(stream, &graph));
-  cudaGraphExec_t exec = nullptr;
-  const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (rc != cudaSuccess) throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
+  cudaGraphExec_t exec = build_tc2_graph(nbf, nocc, Pu[0], Pu[1], Pu[3], pstate, TC2_KMAX);
   tc2_graphs.emplace_back(nocc, exec);
   return exec;
 }
@@ -470,13 +446,18 @@ void System::run_scf() {
     for (int s = 0; s < nsp; ++s) launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
     PF_CUDA(cudaEventRecord(a1, stream));
     // ---- DIIS error X^T (F P S - S P F) X and energy
-    const double one = 1.0, zero = 0.0, mone = -1.0;
+    // R (F P S - S P F) R^T with R = L^{-1} the row-major view of X (the
+    // error's sign and transpose do not matter: only max |E| and <E_i, E_j>
+    // are used); FPS - SPF = A - A^T with A = F P S
     for (int s = 0; s < nsp; ++s) {
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, F[s], nbf, P[s], nbf, &zero, W1, nbf));
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, W1, nbf, S, nbf, &zero, W2, nbf));
-      PF_CUBLAS(cublasDgeam(cublas, CUBLAS_OP_N, CUBLAS_OP_T, nbf, nbf, &one, W2, nbf, &mone, W2, nbf, W1, nbf));
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, W1, nbf, X, nbf, &zero, W2, nbf));
-      PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W2, nbf, &zero, Err[s], nbf));
+      launch_dgemm(nbf, nbf, nbf, false, F[s], nbf, false, P[s], nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, false,
+                   stream);
+      launch_dgemm(nbf, nbf, nbf, false, W1, nbf, false, S, nbf, W2, nbf, 1.0, nullptr, nbf, 0.0, false, false,
+                   stream);
+      launch_dgemm(nbf, nbf, nbf, false, W2, nbf, true, X, nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, true,
+                   stream);
+      launch_dgemm(nbf, nbf, nbf, false, X, nbf, false, W1, nbf, Err[s], nbf, 1.0, nullptr, nbf, 0.0, false, false,
+                   stream);
     }
     launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Err[0],
                       uhf ? Err[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, stream);
@@ -646,7 +627,6 @@ void System::run_scf() {
 void System::gradient(double* g_host) {
   if (!st.done) throw Error(PYFACC_ERR_NOT_READY, "gradient requested before the SCF");
   const size_t n2 = (size_t)nbf * nbf;
-  const double one = 1.0, zero = 0.0;
   cudaEvent_t a0, a1;
   PF_CUDA(cudaEventCreate(&a0));
   PF_CUDA(cudaEventCreate(&a1));
@@ -655,11 +635,12 @@ void System::gradient(double* g_host) {
   // sum_occ eps_i c_i c_i^T = P_s F_s P_s (UHF), = P F P / 4 for the RHF
   // total density P = 2 C_occ C_occ^T, and W = 2 x that for RHF.
   const int nsp = uhf ? 2 : 1;
-  launch_zero(Wm, n2 * sizeof(double), stream);
   for (int s = 0; s < nsp; ++s) {
     const double f = uhf ? 1.0 : 0.5;
-    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, F[s], nbf, P[s], nbf, &zero, W1, nbf));
-    PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &f, P[s], nbf, W1, nbf, &one, Wm, nbf));
+    launch_dgemm(nbf, nbf, nbf, false, F[s], nbf, false, P[s], nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, false,
+                 stream);
+    launch_dgemm(nbf, nbf, nbf, false, P[s], nbf, false, W1, nbf, Wm, nbf, f, s == 0 ? nullptr : Wm, nbf, 1.0, true,
+                 false, stream);
   }
   // total density and spin densities of the converged SCF
   double* Pt = W2;

@@ -89,6 +89,9 @@ struct System {
   int syev_lwork = 0;
 
   ScfState st;
+  double last_jk[7] = {0, 0, 0, 0, 0, 0, 0};  // pyfacc_system_jk_stats
+  // flops and counts of the J/K counters (stats_dev) for nk exchange densities
+  void jk_counters(int nk, double out[6]);
   pyfacc_reduce_fn reducer = nullptr;   // sums shard results across processes
   void* reducer_ctx = nullptr;
   void reduce(double* data, long long count);

@@ -300,11 +300,20 @@ class System:
         nk = 1 if Dk.dim() == 2 else Dk.shape[0]
         J = self._empty(self.nbf, self.nbf)
         K = self._empty(nk, self.nbf, self.nbf)
-        prec = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED}.get(precision, precision)
+        prec = {"fp64": N.PRECISION_FP64, "mixed": N.PRECISION_MIXED, "fp32": N.PRECISION_FP32}.get(precision,
+                                                                                                   precision)
         self._sync()
         N.check(lib().pyfacc_system_jk(self.handle, Dj.data_ptr(), nk, Dk.data_ptr(), J.data_ptr(), K.data_ptr(),
                                        prec), "pyfacc_system_jk")
         return J, (K[0] if Dk.dim() == 2 else K)
+
+    def jk_stats(self) -> dict:
+        """Timing (CUDA events on the engine stream) and algorithmic flops of
+        the last :meth:`jk` build, split by precision."""
+        buf = (ctypes.c_double * 7)()
+        N.check(lib().pyfacc_system_jk_stats(self.handle, buf, 7), "pyfacc_system_jk_stats")
+        keys = ("ms", "flops_fp64", "flops_fp32", "quartets_fp64", "quartets_fp32", "prims_fp64", "prims_fp32")
+        return dict(zip(keys, list(buf)))
 
     def eri_tensor(self):
         eri = self._empty(self.nbf, self.nbf, self.nbf, self.nbf)

@@ -34,6 +34,7 @@ BOYS_ACCURATE = 0
 BOYS_REFERENCE_TRAPEZOID = 1
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_FP32 = 2
 SCF_AUTO, SCF_RHF, SCF_UHF = 0, 1, 2
 GUESS_CORE, GUESS_ATOMIC = 0, 1
 
@@ -96,6 +97,7 @@ SIGNATURES = {
     "pyfacc_system_one_electron": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "pyfacc_system_jk": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_int]),
     "pyfacc_system_eri_tensor": (c_int, [c_void_p, c_void_p]),
+    "pyfacc_system_jk_stats": (c_int, [c_void_p, P_double, c_int]),
     "pyfacc_system_scf": (c_int, [c_void_p, ctypes.POINTER(Result)]),
     "pyfacc_system_gradient": (c_int, [c_void_p, P_double]),
     "pyfacc_system_density_dev": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
@@ -103,6 +105,8 @@ SIGNATURES = {
     "pyfacc_launch_count": (ctypes.c_longlong, []),
     "pyfacc_boys_dev": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
     "pyfacc_partition": (c_int, [c_int, P_double, c_int, ctypes.POINTER(c_int)]),
+    "pyfacc_dense_gemm_dev": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_int, c_void_p, c_void_p, c_int, c_int]),
+    "pyfacc_purify_dev": (c_int, [c_int, c_int, c_void_p, c_void_p, ctypes.POINTER(c_int)]),
     "pyfacc_system_set_reducer": (c_int, [c_void_p, REDUCE_FN, c_void_p]),
     "pyfacc_probe_fp64_gflops": (c_double, [c_int, P_double]),
     "pyfacc_version": (c_char_p, []),

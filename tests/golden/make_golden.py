@@ -7,8 +7,11 @@
 * c20h42_sto3g.json -- the oracle's converged energy and analytic gradient of
   the C20H42/STO-3G benchmark molecule (pyfacc.geometry.alkane(20, seed=1),
   142 basis functions); several minutes of CPU time, hence a fixture.
+* c40h82_sto3g.json -- the same for C40H82/STO-3G (alkane(40, seed=40),
+  282 basis functions), with the oracle's SCF iteration count; about half
+  an hour on 8 cores.
 
-    python tests/golden/make_golden.py [c20h42]
+    python tests/golden/make_golden.py [c20h42 | c40h82]
 """
 import json
 import os
@@ -47,22 +50,35 @@ def main():
                    "S": S.tolist(), "T": T.tolist(), "V_trapezoid": V.tolist()}, fh)
 
 
-def c20h42():
+def alkane_fixture(n, seed):
+    """The oracle's converged energy, analytic gradient, SCF iteration count
+    and timings for alkane(n, seed) in STO-3G (core-Hamiltonian guess + DIIS,
+    as oracle.scf runs it)."""
+    import time
     import oracle as O
     sys.path.insert(0, os.path.join(ROOT, "pyfacc-scf_b200"))
     from pyfacc import geometry as G
-    sp, xyz = G.alkane(20, seed=1)
+    sp, xyz = G.alkane(n, seed=seed)
     mol = O.molecule(sp, xyz, os.path.join(ROOT, "pyfacc-scf_b200", "data", "basis_set", "sto-3g.txt"))
+    t0 = time.perf_counter()
     r = O.scf(mol)
+    t1 = time.perf_counter()
     g = O.gradient(mol, r)
-    with open(os.path.join(HERE, "c20h42_sto3g.json"), "w") as fh:
-        json.dump({"source": "oracle, alkane(20, seed=1), STO-3G RHF, dE<1e-10, DIIS err<1e-8, Schwarz 1e-12",
+    t2 = time.perf_counter()
+    name = f"c{n}h{2 * n + 2}_sto3g.json"
+    with open(os.path.join(HERE, name), "w") as fh:
+        json.dump({"source": f"oracle, alkane({n}, seed={seed}), STO-3G RHF, dE<1e-10, DIIS err<1e-8, "
+                             "Schwarz 1e-12",
                    "nbf": int(mol.shells.nbf), "energy": r.energy, "converged": bool(r.converged),
+                   "scf_iterations": int(r.n_iter), "oracle_seconds": {"scf": t1 - t0, "gradient": t2 - t1},
+                   "oracle_threads": os.cpu_count(),
                    "gradient": np.asarray(g).tolist()}, fh)
 
 
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "c20h42":
-        c20h42()
+        alkane_fixture(20, 1)
+    elif len(sys.argv) > 1 and sys.argv[1] == "c40h82":
+        alkane_fixture(40, 40)
     else:
         main()

@@ -71,4 +71,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PYFACC_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_reference_args.py <reference checkout> (or set PYFACC_REFERENCE_DIR)")
+    main(ref)

@@ -35,15 +35,24 @@ def test_noalloc_jk_matches_system_jk_twice(engine):
         J_ref, K_ref = s.jk(D)
     m, keep = mol._struct()
     data_dir = N.DATA_DIR.encode()
-    for call in range(2):
+    outs = [(torch.empty(n, n, dtype=torch.float64, device="cuda"), torch.empty(n, n, dtype=torch.float64,
+                                                                                 device="cuda")) for _ in range(2)]
+    free = []
+    for call, (J, K) in enumerate(outs):
         # stale values in the outputs must not leak into the result
-        J = torch.full((n, n), 1e30, dtype=torch.float64, device="cuda")
-        K = torch.full((n, n), -1e30, dtype=torch.float64, device="cuda")
+        J.fill_(1e30)
+        K.fill_(-1e30)
         torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
         st = N.lib().pyfacc_jk_noalloc(ctypes.byref(m), data_dir, 1e-12, D.data_ptr(), J.data_ptr(), K.data_ptr())
         assert st == N.OK, N.lib().pyfacc_last_message()
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
         assert (J - J_ref).abs().max().item() < TOL, call
         assert (K - K_ref).abs().max().item() < TOL, call
+    # the first call may set the device up (module load, symbol lookup); the
+    # second must not change the device's free memory at all
+    assert free[3] == free[2], (free[2], free[3])
 
 
 def test_noalloc_rejects_molecule_beyond_the_static_array(engine):
