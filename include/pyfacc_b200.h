@@ -159,9 +159,10 @@ int pyfacc_run(const pyfacc_molecule *mol, const pyfacc_options *opt, pyfacc_res
 
 /* Many molecules of uneven size converged together on one GPU: the shell
  * quartets of all closed-shell molecules (up to 160 basis functions each)
- * run in the same J/K launches, every SCF iteration of the batch is one CUDA
- * graph (J/K class kernels + one dense-step kernel with a thread block per
- * molecule: Fock matrix, energy, DIIS, TC2 purification), and J/K task widths
+ * run in the same J/K launches, the whole SCF of the batch is one CUDA graph
+ * launch (a conditional WHILE loop whose body selects the build variant on
+ * the device, then J/K class kernels + one dense-step kernel with a thread
+ * block per molecule: Fock matrix, energy, DIIS, TC2 purification), and J/K task widths
  * are picked per quartet class by timing (options.task_width = 0).  Open-shell
  * or larger molecules, results that ask for matrices, and molecules whose
  * batched purification fails run through pyfacc_run.  res[i] as in
@@ -173,7 +174,8 @@ int pyfacc_run_batch(int nmol, const pyfacc_molecule *mols, const pyfacc_options
  * {ms_total, ms_setup, ms_one_electron, ms_tune, ms_scf, ms_polish,
  *  ms_gradient, iterations, flops_fock, flops_gradient, quartets_fp64,
  *  quartets_fp32, task width of the six quartet classes (ss|ss) (ps|ss)
- *  (ps|ps) (pp|ss) (pp|ps) (pp|pp)}. */
+ *  (ps|ps) (pp|ss) (pp|ps) (pp|pp), graph launches of the SCF loop (1 when
+ *  the whole SCF ran as one graph with a device-driven WHILE loop)}. */
 int pyfacc_batch_last_stats(double *out, int n);
 
 /* Handle API: basis, shell pairs and Schwarz factors stay resident on the

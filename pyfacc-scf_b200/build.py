@@ -3,8 +3,9 @@
 
     python pyfacc-scf_b200/build.py [--force] [-j N]
 
-Sources: csrc/*.cu and csrc/*.cpp; eri_classes.cuh is regenerated from
-gen_eri.py when the generator is newer.  Objects go to _build/, the library
+Sources: csrc/*.cu and csrc/*.cpp; the generated headers eri_classes.cuh
+(gen_eri.py) and eri_programs.cuh (gen_programs.py) are rewritten when the
+generators' output changes.  Objects go to _build/, the library
 to lib/libpyfacc_b200.so.
 """
 from __future__ import annotations
@@ -68,7 +69,9 @@ def compile_one(src, force, verbose):
 def build(force=False, jobs=None, verbose=False) -> str:
     sys.path.insert(0, CSRC)
     import gen_eri  # noqa: E402
+    import gen_programs  # noqa: E402
     gen_eri.main()
+    gen_programs.main()
     os.makedirs(OBJ, exist_ok=True)
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     srcs = sources()

@@ -7,8 +7,11 @@
 // Contraction coefficients are used as printed (no renormalisation of the
 // contracted functions).  Sections are delimited by '****', so shell lines
 // of absent elements are never mistaken for element labels (basis.f90:30-60
-// would read an 'S' shell line as sulphur); shell types other than S, P and
-// SP are rejected with PYFACC_ERR_UNSUPPORTED_L instead of being misparsed.
+// would read an 'S' shell line as sulphur).  D lines (Sc and heavier), which
+// basis.f90:76-82 has no branch for, become Cartesian d shells (xx, xy, xz,
+// yy, yz, zz, each component normalised on its own, as the oracle reads
+// them); other shell types are rejected with PYFACC_ERR_UNSUPPORTED_L
+// instead of being misparsed.
 #include <dlfcn.h>
 #include <sys/stat.h>
 
@@ -116,8 +119,9 @@ static Basis basis_template(const std::string& basis_file, const std::vector<std
       std::string kind;
       int nprim = 0;
       hs >> kind >> nprim;
-      if (kind != "S" && kind != "P" && kind != "SP")
-        throw Error(PYFACC_ERR_UNSUPPORTED_L, "shell type '" + kind + "' of " + label + " is not supported (s and p only)");
+      if (kind != "S" && kind != "P" && kind != "SP" && kind != "D")
+        throw Error(PYFACC_ERR_UNSUPPORTED_L,
+                    "shell type '" + kind + "' of " + label + " is not supported (S, P, SP and D only)");
       if (nprim <= 0 || i + nprim > lines.size()) throw Error(PYFACC_ERR_INVALID, "truncated basis section for " + label);
       std::vector<double> ex(nprim), cs(nprim), cp(nprim);
       for (int k = 0; k < nprim; ++k) {
@@ -141,6 +145,7 @@ static Basis basis_template(const std::string& basis_file, const std::vector<std
       };
       if (kind == "S") emit(0, cs);
       else if (kind == "P") emit(1, cs);
+      else if (kind == "D") emit(2, cs);  // Cartesian xx, xy, xz, yy, yz, zz; basis.f90 has no D branch
       else {
         emit(0, cs);
         emit(1, cp);

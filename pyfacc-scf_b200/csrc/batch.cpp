@@ -145,6 +145,7 @@ Batch::~Batch() {
   if (stream) cudaStreamSynchronize(stream);
   for (auto& g : graphs)
     if (g) cudaGraphExecDestroy(g);
+  if (scf_graph) cudaGraphExecDestroy(scf_graph);
   context_release(ctx);
 }
 
@@ -553,6 +554,7 @@ void Batch::alloc() {
   const size_t o_stats = carve(sizeof(JkStats) + 2 * NQCLASS * sizeof(unsigned long long));
   const size_t o_grad = carve(3 * (size_t)natoms_tot * sizeof(double));
   const size_t o_act = carve(sizeof(StepReport));
+  const size_t o_ctl = carve(sizeof(BatchScfCtl));
   mats.ensure(o);
   char* b = mats.as<char>();
   double* mp[nmat];
@@ -565,6 +567,7 @@ void Batch::alloc() {
   stats_dev = reinterpret_cast<unsigned long long*>(b + o_stats);
   grad_dev = reinterpret_cast<double*>(b + o_grad);
   active_dev = reinterpret_cast<int*>(b + o_act);
+  ctl_dev = reinterpret_cast<BatchScfCtl*>(b + o_ctl);
   const size_t st_bytes = (nmol * sizeof(BatchMolState) + 255) / 256 * 256;
   state_buf.ensure(st_bytes + nmol * sizeof(BatchMolDev) + 256);
   BatchMolState* st = state_buf.as<BatchMolState>();
@@ -747,7 +750,7 @@ void Batch::tune() {
 // One SCF iteration of the batch as a CUDA graph: density maxima of Db, the
 // J/K class kernels (full builds screen at schwarz_thresh, incremental ones
 // at incremental_thresh), the count reset and the dense step.
-cudaGraphExec_t Batch::capture(int variant, long long* launches) {
+void Batch::capture_into(cudaGraph_t graph, int variant, bool reset_report, long long* launches) {
   const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
   const double inc_thresh = (mixed && opt.incremental_thresh > 0)
                                 ? std::max(opt.incremental_thresh, opt.schwarz_thresh)
@@ -760,27 +763,86 @@ cudaGraphExec_t Batch::capture(int variant, long long* launches) {
   const double thresh =
       coarse ? std::max(COARSE_SCREEN, opt.schwarz_thresh) : (full ? opt.schwarz_thresh : inc_thresh);
   const long long c0 = launch_count();
-  cudaGraph_t g = nullptr;
-  PF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  PF_CUDA(cudaStreamBeginCaptureToGraph(stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   try {
     // a full rebuild of an incremental run builds P itself (the previous
     // step left P_new - P in Db); the first full build has Db = P already
     if (variant == G_FULL && dargs.incremental) launch_batch_full_density(nmol, da, stream);
     fock_build(mixed, thresh, stats_dev, coarse, true);
-    PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(StepReport), stream));
+    if (reset_report) PF_CUDA(cudaMemsetAsync(active_dev, 0, sizeof(StepReport), stream));
     launch_batch_step(nmol, da, stream);
   } catch (...) {
+    cudaGraph_t g = nullptr;
     cudaStreamEndCapture(stream, &g);
-    if (g) cudaGraphDestroy(g);
     throw;
   }
+  cudaGraph_t g = nullptr;
   PF_CUDA(cudaStreamEndCapture(stream, &g));
+  *launches = launch_count() - c0;
+}
+
+cudaGraphExec_t Batch::capture(int variant, long long* launches) {
+  cudaGraph_t g = nullptr;
+  PF_CUDA(cudaGraphCreate(&g, 0));
+  try {
+    capture_into(g, variant, true, launches);
+  } catch (...) {
+    cudaGraphDestroy(g);
+    throw;
+  }
   cudaGraphExec_t e = nullptr;
   const cudaError_t rc = cudaGraphInstantiate(&e, g, 0);
   cudaGraphDestroy(g);
   if (rc != cudaSuccess) throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
-  *launches = launch_count() - c0;
   return e;
+}
+
+// The whole SCF of the batch as one graph: WHILE { select kernel (clears
+// the step report, sets the SWITCH value from the control state), SWITCH
+// over the four iteration variants, update kernel (counts, convergence of
+// the batch, next variant, WHILE condition) }.  The host launches it once
+// and reads the control state when it is done.
+cudaGraphExec_t Batch::build_scf_graph() {
+  cudaGraph_t g = nullptr;
+  PF_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphExec_t exec = nullptr;
+  try {
+    cudaGraphConditionalHandle hloop, hvar;
+    PF_CUDA(cudaGraphConditionalHandleCreate(&hloop, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams wp{};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hloop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wn = nullptr;
+    PF_CUDA(cudaGraphAddNode(&wn, g, nullptr, 0, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    PF_CUDA(cudaGraphConditionalHandleCreate(&hvar, body, 0, 0));
+    cudaGraphNode_t sel = nullptr, sw = nullptr, upd = nullptr;
+    add_batch_select_node(body, &sel, ctl_dev, active_dev, hvar);
+    cudaGraphNodeParams sp{};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hvar;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = G_N;
+    PF_CUDA(cudaGraphAddNode(&sw, body, &sel, 1, &sp));
+    const bool mixed = opt.precision == PYFACC_PRECISION_MIXED;
+    const bool coarse = mixed && dargs.incremental && opt.coarse_err > 0;
+    for (int v = 0; v < G_N; ++v) {
+      const bool used = v == G_FULL || (v == G_INC && dargs.incremental) || ((v == G_CFULL || v == G_CINC) && coarse);
+      if (!used) continue;  // an empty branch
+      capture_into(sp.conditional.phGraph_out[v], v, false, &graph_launches[v]);
+    }
+    add_batch_update_node(body, &upd, &sw, ctl_dev, active_dev, hloop);
+    const cudaError_t rc = cudaGraphInstantiate(&exec, g, 0);
+    if (rc != cudaSuccess)
+      throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate (SCF graph): ") + cudaGetErrorString(rc));
+  } catch (...) {
+    cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraphDestroy(g);
+  return exec;
 }
 
 void Batch::run(bool gradient) {
@@ -820,38 +882,73 @@ void Batch::run(bool gradient) {
   // molecule engine); the next build is a full mixed one, which restarts the
   // incremental chain.
   bool coarse = mixed && dargs.incremental && opt.coarse_err > 0;
-  if (!graphs[G_FULL]) graphs[G_FULL] = capture(G_FULL, &graph_launches[G_FULL]);
-  if (dargs.incremental && !graphs[G_INC]) graphs[G_INC] = capture(G_INC, &graph_launches[G_INC]);
-  if (coarse && !graphs[G_CFULL]) graphs[G_CFULL] = capture(G_CFULL, &graph_launches[G_CFULL]);
-  if (coarse && !graphs[G_CINC]) graphs[G_CINC] = capture(G_CINC, &graph_launches[G_CINC]);
-  int it = 0, since_full = 0;
-  bool restart = false;
-  for (it = 1; it <= dargs.max_iter; ++it) {
-    int v;
-    if (coarse) {
-      v = it == 1 ? G_CFULL : G_CINC;
-    } else {
-      const bool full = !dargs.incremental || it == 1 || restart || since_full + 1 >= dargs.rebuild_every;
-      v = full ? G_FULL : G_INC;
-      since_full = full ? 0 : since_full + 1;
-      restart = false;
-    }
-    PF_CUDA(cudaGraphLaunch(graphs[v], stream));
-    count_launches(graph_launches[v]);
-    PF_CUDA(cudaMemcpyAsync(&report, active_dev, sizeof(StepReport), cudaMemcpyDeviceToHost, stream));
-    PF_CUDA(cudaStreamSynchronize(stream));
-    if (report.active == 0) break;
-    if (coarse) {
-      double err;
-      std::memcpy(&err, &report.max_err, sizeof(err));
-      if (err < opt.coarse_err || it >= COARSE_MAX_ITER) {
-        coarse = false;
-        restart = true;
-      }
+  int it = 0;
+  if (!scf_graph && !scf_graph_failed) {
+    try {
+      scf_graph = build_scf_graph();
+    } catch (const Error& e) {
+      // a driver without conditional graph nodes: one graph launch per
+      // iteration instead (below)
+      scf_graph_failed = true;
+      if (opt.verbose) std::fprintf(stderr, "pyfacc batch: whole-SCF graph unavailable (%s)\n", e.what());
     }
   }
-  timing.iterations = std::min(it, dargs.max_iter);
+  if (scf_graph) {
+    BatchScfCtl c{};
+    c.coarse = coarse ? 1 : 0;
+    c.variant = coarse ? G_CFULL : G_FULL;
+    c.incremental = dargs.incremental;
+    c.rebuild_every = dargs.rebuild_every;
+    c.max_iter = dargs.max_iter;
+    c.coarse_max_iter = COARSE_MAX_ITER;
+    c.coarse_err = opt.coarse_err;
+    PF_CUDA(cudaMemcpyAsync(ctl_dev, &c, sizeof(c), cudaMemcpyHostToDevice, stream));
+    PF_CUDA(cudaGraphLaunch(scf_graph, stream));
+    PF_CUDA(cudaMemcpyAsync(&c, ctl_dev, sizeof(c), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaStreamSynchronize(stream));
+    long long nl = 2LL * c.it;  // select + update kernels
+    for (int v = 0; v < G_N; ++v) nl += c.counts[v] * graph_launches[v];
+    count_launches(nl);
+    it = c.it;
+    timing.iterations = std::min(it, dargs.max_iter);
+    scf_launches_last = 1;
+  } else {
+    if (!graphs[G_FULL]) graphs[G_FULL] = capture(G_FULL, &graph_launches[G_FULL]);
+    if (dargs.incremental && !graphs[G_INC]) graphs[G_INC] = capture(G_INC, &graph_launches[G_INC]);
+    if (coarse && !graphs[G_CFULL]) graphs[G_CFULL] = capture(G_CFULL, &graph_launches[G_CFULL]);
+    if (coarse && !graphs[G_CINC]) graphs[G_CINC] = capture(G_CINC, &graph_launches[G_CINC]);
+    int since_full = 0;
+    bool restart = false;
+    scf_launches_last = 0;
+    for (it = 1; it <= dargs.max_iter; ++it) {
+      int v;
+      if (coarse) {
+        v = it == 1 ? G_CFULL : G_CINC;
+      } else {
+        const bool full = !dargs.incremental || it == 1 || restart || since_full + 1 >= dargs.rebuild_every;
+        v = full ? G_FULL : G_INC;
+        since_full = full ? 0 : since_full + 1;
+        restart = false;
+      }
+      PF_CUDA(cudaGraphLaunch(graphs[v], stream));
+      count_launches(graph_launches[v]);
+      ++scf_launches_last;
+      PF_CUDA(cudaMemcpyAsync(&report, active_dev, sizeof(StepReport), cudaMemcpyDeviceToHost, stream));
+      PF_CUDA(cudaStreamSynchronize(stream));
+      if (report.active == 0) break;
+      if (coarse) {
+        double err;
+        std::memcpy(&err, &report.max_err, sizeof(err));
+        if (err < opt.coarse_err || it >= COARSE_MAX_ITER) {
+          coarse = false;
+          restart = true;
+        }
+      }
+    }
+    timing.iterations = std::min(it, dargs.max_iter);
+  }
   timing.ms_scf = wall_ms() - ts;
+  timing.scf_graph_launches = scf_launches_last;
   // ---- FP64 polish of mixed precision: F and E of the final densities
   if (mixed && opt.polish) {
     const double tp = wall_ms();

@@ -60,6 +60,35 @@ struct BatchDenseArgs {
   unsigned long long* max_err;  // largest DIIS error of the step (bits of a non-negative double)
 };
 
+// Iteration-graph variants of a batched SCF: full and incremental builds,
+// and the all-FP32 full and incremental builds of the first mixed iterations.
+enum BatchVariant { G_FULL = 0, G_INC = 1, G_CFULL = 2, G_CINC = 3, G_N = 4 };
+
+// Control state of a batched SCF run as one graph launch: the build variant
+// of every iteration is chosen on the device by the rules the host loop used
+// (coarse phase while the batch's largest DIIS error is above coarse_err,
+// then a full build, then incremental builds with a full rebuild every
+// rebuild_every iterations).
+struct BatchScfCtl {
+  int it;            // iterations done
+  int since_full;    // incremental builds since the last full one
+  int coarse;        // the all-FP32 builds still run
+  int restart;       // the next build must be full (end of the coarse phase)
+  int variant;       // BatchVariant of the iteration in flight
+  int incremental, rebuild_every, max_iter, coarse_max_iter;
+  int stop;          // the loop ended (no molecule active, or max_iter)
+  double coarse_err;
+  long long counts[G_N];  // iterations run per variant
+};
+// At the top of an iteration: clear the step report, select this
+// iteration's variant (the SWITCH node that follows).
+void add_batch_select_node(cudaGraph_t g, cudaGraphNode_t* node, BatchScfCtl* ctl, int* report,
+                           cudaGraphConditionalHandle variant);
+// After the dense step: count, decide the next variant and whether the
+// WHILE loop goes on.
+void add_batch_update_node(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* dep, BatchScfCtl* ctl,
+                           const int* report, cudaGraphConditionalHandle loop);
+
 // X = S^{-1/2} of every molecule (coupled Newton-Schulz), into Xout; F, T1..T3
 // are work space.  A molecule whose iteration does not converge is marked failed.
 void launch_batch_lowdin(int nmol, const BatchDenseArgs& a, double* Xout, cudaStream_t s);
@@ -136,6 +165,7 @@ struct BatchMolHost {
 struct BatchTiming {
   double ms_total = 0, ms_setup = 0, ms_1e = 0, ms_tune = 0, ms_scf = 0, ms_polish = 0, ms_grad = 0;
   int iterations = 0;
+  int scf_graph_launches = 0;  // graph launches of the SCF loop (1 = the whole-SCF graph)
   double flops_fock = 0.0, flops_grad = 0.0;
   unsigned long long quartets[2] = {0, 0};
   int width[NQCLASS] = {32, 32, 32, 32, 32, 32};
@@ -169,8 +199,8 @@ class Batch {
   long long mtot = 0;
   ShellDev shd;
   double4* atoms_dev = nullptr;
-  int2* pairs1e[NCLASS] = {nullptr, nullptr, nullptr};
-  int n1e[NCLASS] = {0, 0, 0};
+  int2* pairs1e[NPAIRCLASS] = {};  // one-electron pair lists (no d shells in a batch)
+  int n1e[NPAIRCLASS] = {};
   int* bf_off_dev = nullptr;
   int* nfun_dev = nullptr;
   int4* mt_dev = nullptr;
@@ -191,11 +221,16 @@ class Batch {
     int pad;
     unsigned long long max_err;  // bits of the largest DIIS error
   } report{};
-  // iteration graphs: full and incremental builds, and the all-FP32 full
-  // and incremental builds of the first mixed iterations
-  enum { G_FULL, G_INC, G_CFULL, G_CINC, G_N };
+  // iteration graphs (BatchVariant), launched one by one only when the
+  // whole-SCF graph cannot be built
   cudaGraphExec_t graphs[G_N] = {nullptr, nullptr, nullptr, nullptr};
   long long graph_launches[G_N] = {0, 0, 0, 0};  // kernels per replay
+  // the whole SCF: WHILE { select, SWITCH { the four variants }, update }
+  cudaGraphExec_t scf_graph = nullptr;
+  bool scf_graph_failed = false;
+  int scf_launches_last = 0;
+  BatchScfCtl* ctl_dev = nullptr;
+  cudaGraphExec_t build_scf_graph();
   std::vector<BatchMolState> st_host;
   std::vector<double> grad_host;
   std::vector<double> occ_host;          // atomic-occupation guess, all molecules' diagonals
@@ -216,6 +251,9 @@ class Batch {
   std::string tune_key() const;
   void tune();
   cudaGraphExec_t capture(int variant, long long* launches);
+  // the work of one iteration of the given variant, captured into graph
+  // (reset_report: clear the step report first, as a standalone graph must)
+  void capture_into(cudaGraph_t graph, int variant, bool reset_report, long long* launches);
   void gradient_run();
 };
 

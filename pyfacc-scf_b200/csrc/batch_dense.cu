@@ -602,6 +602,69 @@ void launch_batch_init(int nmol, const BatchDenseArgs& a, int core_guess, cudaSt
   count_launch();
 }
 
+// ---------------------------------------------------------------------------
+// Control of the whole-SCF graph (one thread each).
+// ---------------------------------------------------------------------------
+__global__ void batch_ctl_select_kernel(const BatchScfCtl* __restrict__ c, int* __restrict__ report,
+                                        cudaGraphConditionalHandle variant) {
+  report[0] = 0;  // active molecules
+  report[1] = 0;
+  report[2] = 0;  // largest DIIS error (bits of a double, two ints)
+  report[3] = 0;
+  cudaGraphSetConditional(variant, (unsigned)c->variant);
+}
+
+__global__ void batch_ctl_update_kernel(BatchScfCtl* __restrict__ c, const int* __restrict__ report,
+                                        cudaGraphConditionalHandle loop) {
+  c->counts[c->variant] += 1;
+  const int it = ++c->it;
+  const int active = report[0];
+  const double err = __longlong_as_double(*reinterpret_cast<const long long*>(report + 2));
+  bool go = active > 0;
+  if (go && c->coarse && (err < c->coarse_err || it >= c->coarse_max_iter)) {
+    c->coarse = 0;
+    c->restart = 1;
+  }
+  if (it >= c->max_iter) go = false;
+  if (go) {
+    int v;
+    if (c->coarse) {
+      v = G_CINC;
+    } else {
+      const bool full = !c->incremental || c->restart || c->since_full + 1 >= c->rebuild_every;
+      c->since_full = full ? 0 : c->since_full + 1;
+      c->restart = 0;
+      v = full ? G_FULL : G_INC;
+    }
+    c->variant = v;
+  }
+  c->stop = go ? 0 : 1;
+  cudaGraphSetConditional(loop, go ? 1u : 0u);
+}
+
+void add_batch_select_node(cudaGraph_t g, cudaGraphNode_t* node, BatchScfCtl* ctl, int* report,
+                           cudaGraphConditionalHandle variant) {
+  const BatchScfCtl* c = ctl;
+  void* args[] = {&c, &report, &variant};
+  cudaKernelNodeParams p{};
+  p.func = reinterpret_cast<void*>(batch_ctl_select_kernel);
+  p.gridDim = dim3(1);
+  p.blockDim = dim3(1);
+  p.kernelParams = args;
+  PF_CUDA(cudaGraphAddKernelNode(node, g, nullptr, 0, &p));
+}
+
+void add_batch_update_node(cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* dep, BatchScfCtl* ctl,
+                           const int* report, cudaGraphConditionalHandle loop) {
+  void* args[] = {&ctl, &report, &loop};
+  cudaKernelNodeParams p{};
+  p.func = reinterpret_cast<void*>(batch_ctl_update_kernel);
+  p.gridDim = dim3(1);
+  p.blockDim = dim3(1);
+  p.kernelParams = args;
+  PF_CUDA(cudaGraphAddKernelNode(node, g, dep, 1, &p));
+}
+
 void launch_batch_step(int nmol, const BatchDenseArgs& a, cudaStream_t s) {
   if (nmol <= 0) return;
   batch_step_kernel<<<nmol, BATCH_THREADS, xs_bytes(a), s>>>(a);

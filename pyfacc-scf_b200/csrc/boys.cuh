@@ -28,7 +28,7 @@
 #define PF_BOYS_STEP 0.1
 #define PF_BOYS_INV_STEP 10.0
 #define PF_BOYS_TMAX 36.0
-#define PF_BOYS_MMAX 6       // highest order needed: (pp|pp) gradient = 5
+#define PF_BOYS_MMAX 9       // highest order needed: (dd|dd) gradient = 9
 #define PF_BOYS_NT 8         // Taylor terms, FP64
 #define PF_BOYS_NTF 5        // Taylor terms, FP32
 #define PF_BOYS_EMAX 100.0   // e^{-T} table end
@@ -37,13 +37,14 @@
 
 namespace pyfacc {
 
-// Grid tables (this header is included by exactly one translation unit,
-// kernels.cu, which fills them per device with cudaMemcpyToSymbol):
+// Grid tables, one copy per translation unit that includes this header
+// (kernels.cu and kernels_d.cu; each fills its copy per device with
+// cudaMemcpyToSymbol, see ensure_boys_tables):
 // g_boys_tl[L][k][j] = F_{L+j}(T_k) / j!, g_boys_exp[k] = e^{-T_k},
 // g_boys_tlf[L][k][j] = F_{L+j}(T_k) / j! in float (j < 5 used).
-__device__ __align__(16) double g_boys_tl[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
-__device__ double g_boys_exp[PF_BOYS_NEXP];
-__device__ __align__(16) float g_boys_tlf[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
+static __device__ __align__(16) double g_boys_tl[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
+static __device__ double g_boys_exp[PF_BOYS_NEXP];
+static __device__ __align__(16) float g_boys_tlf[(PF_BOYS_MMAX + 1) * PF_BOYS_NGRID * PF_BOYS_NT];
 
 // Branch-free: every lane evaluates the Taylor value (from row 0 when T is
 // beyond the grid) and the asymptotic value and selects, so a warp whose
@@ -199,7 +200,10 @@ __device__ __forceinline__ void boys_runtime(int mode, int lmax, double T, doubl
     case 3: boys_fp64<3>(T, F); break;
     case 4: boys_fp64<4>(T, F); break;
     case 5: boys_fp64<5>(T, F); break;
-    default: boys_fp64<6>(T, F); break;
+    case 6: boys_fp64<6>(T, F); break;
+    case 7: boys_fp64<7>(T, F); break;
+    case 8: boys_fp64<8>(T, F); break;
+    default: boys_fp64<9>(T, F); break;
   }
 }
 

@@ -186,7 +186,9 @@ int pyfacc_run_batch(int nmol, const pyfacc_molecule* mols, const pyfacc_options
       if (r) r->energy = std::numeric_limits<double>::quiet_NaN();
       continue;
     }
-    if (uhf || wants_matrices || h.nbf > pyfacc::BATCH_NBF_MAX) {
+    bool has_d = false;  // the batched kernels cover s/p shells; d molecules run on their own
+    for (const auto& sh : h.basis.shells) has_d = has_d || sh.l > 1;
+    if (uhf || wants_matrices || has_d || h.nbf > pyfacc::BATCH_NBF_MAX) {
       single.push_back(i);
     } else {
       in_batch.push_back(i);
@@ -258,7 +260,7 @@ int pyfacc_batch_last_stats(double* out, int n) {
   const double v[] = {b.ms_total, b.ms_setup, b.ms_1e, b.ms_tune, b.ms_scf, b.ms_polish, b.ms_grad,
                       (double)b.iterations, b.flops_fock, b.flops_grad, (double)b.quartets[0],
                       (double)b.quartets[1], (double)b.width[0], (double)b.width[1], (double)b.width[2],
-                      (double)b.width[3], (double)b.width[4], (double)b.width[5]};
+                      (double)b.width[3], (double)b.width[4], (double)b.width[5], (double)b.scf_graph_launches};
   const int nv = (int)(sizeof(v) / sizeof(v[0]));
   for (int k = 0; k < n; ++k) out[k] = k < nv ? v[k] : 0.0;
   return PYFACC_OK;

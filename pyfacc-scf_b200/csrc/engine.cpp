@@ -220,7 +220,8 @@ void System::upload_shells() {
     for (size_t k = 0; k < sh.ex.size(); ++k) {
       const double a = sh.ex[k];
       double nrm = std::pow(2.0 * a / 3.14159265358979323846, 0.75);
-      if (sh.l) nrm *= 2.0 * std::sqrt(a);
+      if (sh.l == 1) nrm *= 2.0 * std::sqrt(a);
+      if (sh.l == 2) nrm *= 4.0 * a;  // 4a / sqrt(3), times sqrt(3) for the mixed components
       mx = std::max(mx, std::fabs(sh.co[k] * nrm));
       mn = std::min(mn, a);
     }
@@ -228,7 +229,7 @@ void System::upload_shells() {
     amin[s] = mn;
   }
   const double lcut = std::log(ONE_E_PAIR_CUT);
-  std::vector<int2> p1[NCLASS];
+  std::vector<int2> p1[NPAIRCLASS];
   for (int a = 0; a < ns; ++a)
     for (int b = a; b < ns; ++b) {
       const Shell &sa = basis.shells[a], &sb = basis.shells[b];
@@ -240,9 +241,10 @@ void System::upload_shells() {
       }
       int x = a, y = b;
       if (basis.shells[x].l < basis.shells[y].l) std::swap(x, y);
-      p1[basis.shells[x].l + basis.shells[y].l].push_back(make_int2(x, y));
+      p1[pair_class(basis.shells[x].l, basis.shells[y].l)].push_back(make_int2(x, y));
     }
-  for (int c = 0; c < NCLASS; ++c) n1e[c] = (int)p1[c].size();
+  int n1e_all = 0;
+  for (int c = 0; c < NPAIRCLASS; ++c) n1e_all += n1e[c] = (int)p1[c].size();
   const size_t nex = std::max<size_t>(ex.size(), 1);
   size_t off = 0;
   auto carve = [&](size_t bytes) {
@@ -252,7 +254,7 @@ void System::upload_shells() {
   };
   const size_t o_cen = carve(ns * sizeof(double4)), o_desc = carve(ns * sizeof(int4)), o_np = carve(ns * sizeof(int)),
                o_ex = carve(nex * sizeof(double)), o_co = carve(nex * sizeof(double)),
-               o_atoms = carve(natoms * sizeof(double4)), o_p1 = carve((n1e[0] + n1e[1] + n1e[2] + 3) * sizeof(int2)),
+               o_atoms = carve(natoms * sizeof(double4)), o_p1 = carve((n1e_all + NPAIRCLASS) * sizeof(int2)),
                o_bfo = carve((ns + 1) * sizeof(int)), o_nf = carve(ns * sizeof(int));
   shd.buf.ensure(off);
   char* base = shd.buf.as<char>();
@@ -264,8 +266,7 @@ void System::upload_shells() {
   shd.co = reinterpret_cast<double*>(base + o_co);
   atoms_dev = reinterpret_cast<double4*>(base + o_atoms);
   pairs1e[0] = reinterpret_cast<int2*>(base + o_p1);
-  pairs1e[1] = pairs1e[0] + n1e[0];
-  pairs1e[2] = pairs1e[1] + n1e[1];
+  for (int c = 1; c < NPAIRCLASS; ++c) pairs1e[c] = pairs1e[c - 1] + n1e[c - 1];
   bf_off_dev = reinterpret_cast<int*>(base + o_bfo);
   nfun_dev = reinterpret_cast<int*>(base + o_nf);
   PF_CUDA(cudaMemcpyAsync(shd.cen, cen.data(), ns * sizeof(double4), cudaMemcpyHostToDevice, stream));
@@ -274,7 +275,7 @@ void System::upload_shells() {
   PF_CUDA(cudaMemcpyAsync(shd.ex, ex.data(), ex.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(shd.co, co.data(), co.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(atoms_dev, atoms.data(), natoms * sizeof(double4), cudaMemcpyHostToDevice, stream));
-  for (int c = 0; c < NCLASS; ++c)
+  for (int c = 0; c < NPAIRCLASS; ++c)
     if (n1e[c]) PF_CUDA(cudaMemcpyAsync(pairs1e[c], p1[c].data(), n1e[c] * sizeof(int2), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(bf_off_dev, bfo.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
   PF_CUDA(cudaMemcpyAsync(nfun_dev, nf.data(), ns * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -286,9 +287,9 @@ void System::upload_shells() {
 double max_prim_prefactor(const Basis& b) {
   double mx = 0.0;
   const double c0 = 5.9149671727956128778;
-  auto nrm = [](int l, double a) {
+  auto nrm = [](int l, double a) {  // the x^l normalisation of gaussian.f90:80-98
     const double n = std::pow(2.0 * a / 3.14159265358979323846, 0.75);
-    return l ? n * 2.0 * std::sqrt(a) : n;
+    return l == 0 ? n : (l == 1 ? n * 2.0 * std::sqrt(a) : n * 4.0 * a / std::sqrt(3.0));
   };
   for (size_t i = 0; i < b.shells.size(); ++i)
     for (size_t j = 0; j <= i; ++j) {
@@ -309,18 +310,20 @@ void System::build_pairs() {
   using clk = std::chrono::steady_clock;
   clk::time_point tq[8];
   tq[0] = clk::now();
-  std::vector<int4> pl0[NCLASS];
+  std::vector<int4> pl0[NPAIRCLASS];
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j <= i; ++j) {
       int a = i, b = j;
       if (basis.shells[a].l < basis.shells[b].l) std::swap(a, b);
-      const int c = basis.shells[a].l + basis.shells[b].l;
+      const int c = pair_class(basis.shells[a].l, basis.shells[b].l);
       pl0[c].push_back(make_int4(a, b, 0, 0));
     }
+  has_d = false;
+  for (int c = NCLASS; c < NPAIRCLASS; ++c) has_d = has_d || !pl0[c].empty();
   std::vector<int4> all0, all1;
-  int off[NCLASS + 1] = {0, 0, 0, 0};
+  int off[NPAIRCLASS + 1] = {0, 0, 0, 0, 0, 0, 0};
   int nprim_tot = 0;
-  for (int c = 0; c < NCLASS; ++c) {
+  for (int c = 0; c < NPAIRCLASS; ++c) {
     off[c + 1] = off[c] + (int)pl0[c].size();
     for (auto p : pl0[c]) {
       p.z = nprim_tot;
@@ -329,7 +332,7 @@ void System::build_pairs() {
       all1.push_back(make_int4(0, nbf, 0, 0));
     }
   }
-  const int np_all = off[NCLASS];
+  const int np_all = off[NPAIRCLASS];
   // scratch: unsorted records
   size_t o = 0;
   auto carve = [&](size_t bytes) {
@@ -366,6 +369,7 @@ void System::build_pairs() {
   launch_build_pairs(shd, np_all, d_pl0, d_pl1, tmp.info0, tmp.info1, tmp.info2, tmp.geom, tmp.prim, cut, d_kept,
                      stream);
   launch_schwarz(tmp, off, d_q, stream, ctx.side, ctx.fork, ctx.join);
+  if (has_d) launch_schwarz_d(tmp, off, d_q, num_sms, stream);
   std::vector<double> q(np_all);
   std::vector<int> kept(np_all);
   PF_CUDA(cudaMemcpyAsync(q.data(), d_q, np_all * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -379,7 +383,7 @@ void System::build_pairs() {
   int nprim_new = 0;
   pd.q_host.clear();
   pd.cls_host.clear();
-  for (int c = 0; c < NCLASS; ++c) {
+  for (int c = 0; c < NPAIRCLASS; ++c) {
     std::vector<int> idx;
     for (int k = off[c]; k < off[c + 1]; ++k)
       if (thr <= 0 || q[k] * qmax >= thr) idx.push_back(k);
@@ -454,7 +458,7 @@ void System::build_tasks() {
   const double thr = std::max(opt.schwarz_thresh, 0.0);
   const double t32 = opt.fp32_thresh;
   quartets_total = 0;
-  for (int bc = 0; bc < NCLASS; ++bc)
+  for (int bc = 0; bc < NPAIRCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) {
       const int nb = pd.class_off[bc + 1] - pd.class_off[bc];
       const int nk = pd.class_off[kc + 1] - pd.class_off[kc];

@@ -38,8 +38,15 @@ struct Error : std::runtime_error {
       throw ::pyfacc::Error(PYFACC_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-constexpr int NCLASS = 3;        // ss, ps, pp
+constexpr int NCLASS = 3;        // ss, ps, pp: the pair classes of the straight-line kernels
 constexpr int NQCLASS = 6;       // (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|pp)
+// With d shells three more pair classes follow: ds, dp, dd (l_a >= l_b);
+// their quartets run in the warp-cooperative kernels of kernels_d.cu.
+constexpr int NPAIRCLASS = 6;
+constexpr int NDQCLASS = 15;     // quartet classes with a d pair: bra class >= ket class
+inline int pair_class(int la, int lb) { return la == 0 ? 0 : (la == 1 ? 1 + lb : 3 + lb); }  // la >= lb
+// index of the d quartet class (bra pair class bc in 3..5, ket class kc <= bc)
+inline int dclass_index(int bc, int kc) { return bc == 3 ? kc : (bc == 4 ? 4 + kc : 9 + kc); }
 // primitive-quartet cut relative to the quartet screening threshold:
 // |K_ab K_cd| max|D| < PRIM_QUARTET_REL * thresh skips a primitive quartet
 // (its integral is at most ~1.5 |K_ab K_cd|, as F_m <= 1 and p + q > 0.4
@@ -127,7 +134,7 @@ struct TaskList {
 // offset and leading dimension of its molecule's matrices).
 struct PairData {
   int npair = 0;
-  int class_off[NCLASS + 1] = {0, 0, 0, 0};
+  int class_off[NPAIRCLASS + 1] = {0, 0, 0, 0, 0, 0, 0};  // s/p classes, then ds, dp, dd
   int nprim = 0;
   int4* info0 = nullptr;     // {bf_a, bf_b, prim_start, n_prim}
   int4* info1 = nullptr;     // {shell_a, shell_b, atom_a, atom_b}
@@ -160,6 +167,9 @@ void count_launch();
 void count_launches(long long n);  // kernels of a replayed CUDA graph
 long long launch_count();
 void ensure_boys_tables(int device);
+// The same FP64 Boys tables for the d-shell kernels' copy (kernels_d.cu),
+// called by ensure_boys_tables on the current device.
+void upload_boys_tables_d(const double* tl, size_t ntl, const double* ex, size_t nex);
 void launch_boys_test(int mode, int fp32, int mmax, int n, const double* x, double* out, cudaStream_t s);
 
 struct ShellDev {  // device copies of the shells (packed over a batch)
@@ -240,6 +250,17 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bra_class, int ke
 
 void launch_eri_tensor(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, int nbf,
                        double* eri, cudaStream_t s);
+
+// Quartets with a d pair (kernels_d.cu), FP64, one warp per quartet.
+// Schwarz factors of the ds, dp, dd pairs (off: unsorted class offsets).
+void launch_schwarz_d(const PairData& pd, const int* off, double* q, int num_sms, cudaStream_t s);
+void launch_jk_d(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, int nk, const JkArgs& a,
+                 int num_sms, cudaStream_t s);
+void launch_grad2e_d(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, const GradArgs& a,
+                     int num_sms, cudaStream_t s);
+// Full ERI tensor images of a d-class list (tests, small systems).
+void launch_eri_tensor_d(const PairData& pd, const TaskList& tl, int bra_class, int ket_class, int nbf, double* eri,
+                         cudaStream_t s);
 
 // One-electron integrals over canonical shell pairs of the shells in sh.
 struct OneEArgs {

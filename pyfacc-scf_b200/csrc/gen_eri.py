@@ -455,7 +455,7 @@ def gen_one_electron(la, lb):
 
 
 CLASSES = [(0, 0, 0, 0), (1, 0, 0, 0), (1, 0, 1, 0), (1, 1, 0, 0), (1, 1, 1, 0), (1, 1, 1, 1)]
-ONE_E_CLASSES = [(0, 0), (1, 0), (1, 1)]
+ONE_E_CLASSES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2)]
 
 
 def generate() -> str:

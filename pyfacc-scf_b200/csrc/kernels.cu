@@ -71,6 +71,7 @@ void ensure_boys_tables(int device) {
     PF_CUDA(cudaMemcpyToSymbol(g_boys_tl, tl.data(), tl.size() * sizeof(double)));
     PF_CUDA(cudaMemcpyToSymbol(g_boys_exp, ex.data(), ex.size() * sizeof(double)));
     PF_CUDA(cudaMemcpyToSymbol(g_boys_tlf, tabf.data(), tabf.size() * sizeof(float)));
+    upload_boys_tables_d(tl.data(), tl.size(), ex.data(), ex.size());
     done[device] = 1;
   }
 }
@@ -110,9 +111,19 @@ void launch_boys_test(int mode, int fp32, int mmax, int n, const double* x, doub
 // Shell pairs
 // ===========================================================================
 __device__ __forceinline__ double prim_norm(int l, double a) {
-  // gaussian.f90:80-98 for l <= 1 (the (2a_x-1)!! product is 1 for s and p)
+  // gaussian.f90:80-98: (2a/pi)^(3/4) (4a)^(l/2) / sqrt((2l-1)!!) for the
+  // x^l component (the (2a_x-1)!! product is 1 for s and p); the other d
+  // components differ by comp_ratio
   double n = pow(2.0 * a * 0.31830988618379067154, 0.75);
-  return l == 0 ? n : n * 2.0 * sqrt(a);
+  if (l == 0) return n;
+  if (l == 1) return n * 2.0 * sqrt(a);
+  return n * 4.0 * a * 0.57735026918962576451;  // 4a / sqrt(3)
+}
+
+// norm of Cartesian component k of an l shell / norm of its x^l component:
+// sqrt(3) for d_xy, d_xz, d_yz, else 1
+__device__ __forceinline__ double comp_ratio(int l, int k) {
+  return (l == 2 && (k == 1 || k == 2 || k == 4)) ? 1.7320508075688772935 : 1.0;
 }
 
 // pl0 = {shell a, shell b, prim_start, first shell of the molecule},
@@ -1235,9 +1246,12 @@ __device__ __forceinline__ void ovl1d(double s00, double PA, double PB, double o
 }
 
 __device__ __forceinline__ void cart_comp(int l, int k, int* c) {
-  // x descending, then y (cartesian.f90:7-23), l <= 1
+  // x descending, then y (cartesian.f90:7-23), l <= 2
   if (l == 0) { c[0] = c[1] = c[2] = 0; return; }
-  c[0] = (k == 0); c[1] = (k == 1); c[2] = (k == 2);
+  if (l == 1) { c[0] = (k == 0); c[1] = (k == 1); c[2] = (k == 2); return; }
+  // xx, xy, xz, yy, yz, zz
+  const int tab[6][3] = {{2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {0, 2, 0}, {0, 1, 1}, {0, 0, 2}};
+  c[0] = tab[k][0]; c[1] = tab[k][1]; c[2] = tab[k][2];
 }
 
 // S_ab and T_ab of unnormalised Cartesian components a, b from 1-D tables
@@ -1363,21 +1377,33 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
       for (int ib = 0; ib < NB; ++ib) {
         const size_t mu = da.z + ia, nu = db.z + ib;
         const int k = ia * NB + ib;
-        if (args.S) { args.S[mo + mu * n + nu] = s[k]; args.S[mo + nu * n + mu] = s[k]; }
-        if (args.T) { args.T[mo + mu * n + nu] = t[k]; args.T[mo + nu * n + mu] = t[k]; }
-        if (args.V) { args.V[mo + mu * n + nu] = v[k]; args.V[mo + nu * n + mu] = v[k]; }
+        const double r = comp_ratio(LA, ia) * comp_ratio(LB, ib);
+        if (args.S) { args.S[mo + mu * n + nu] = r * s[k]; args.S[mo + nu * n + mu] = r * s[k]; }
+        if (args.T) { args.T[mo + mu * n + nu] = r * t[k]; args.T[mo + nu * n + mu] = r * t[k]; }
+        if (args.V) { args.V[mo + mu * n + nu] = r * v[k]; args.V[mo + nu * n + mu] = r * v[k]; }
       }
   }
 }
 
+template <int LA, int LB>
+static void one_electron_launch(int n, const int2* pairs, const ShellDev& sh, const OneEArgs& a, cudaStream_t s) {
+  one_electron_kernel<LA, LB><<<(n + 3) / 4, 128, 0, s>>>(n, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
+}
+
+// pairs[c] for the pair classes c = ss, ps, pp, ds, dp, dd (l_a >= l_b);
+// molecules without d shells have the last three empty
 void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEArgs& a,
                          cudaStream_t s) {
-  for (int c = 0; c < NCLASS; ++c) {
+  for (int c = 0; c < NPAIRCLASS; ++c) {
     if (npair[c] <= 0) continue;
-    dim3 grid((npair[c] + 3) / 4), block(128);
-    if (c == 0) one_electron_kernel<0, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
-    if (c == 1) one_electron_kernel<1, 0><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
-    if (c == 2) one_electron_kernel<1, 1><<<grid, block, 0, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, a);
+    switch (c) {
+      case 0: one_electron_launch<0, 0>(npair[c], pairs[c], sh, a, s); break;
+      case 1: one_electron_launch<1, 0>(npair[c], pairs[c], sh, a, s); break;
+      case 2: one_electron_launch<1, 1>(npair[c], pairs[c], sh, a, s); break;
+      case 3: one_electron_launch<2, 0>(npair[c], pairs[c], sh, a, s); break;
+      case 4: one_electron_launch<2, 1>(npair[c], pairs[c], sh, a, s); break;
+      default: one_electron_launch<2, 2>(npair[c], pairs[c], sh, a, s); break;
+    }
     PF_CUDA(cudaGetLastError());
     count_launch();
   }
@@ -1420,8 +1446,9 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
 #pragma unroll
       for (int ib = 0; ib < NB; ++ib) {
         const size_t k = mo + (size_t)(da.z + ia) * n + db.z + ib;
-        Pd[ia * NB + ib] = wgt * args.P[k];
-        Wd[ia * NB + ib] = wgt * args.W[k];
+        const double r = comp_ratio(LA, ia) * comp_ratio(LB, ib);
+        Pd[ia * NB + ib] = wgt * r * args.P[k];
+        Wd[ia * NB + ib] = wgt * r * args.W[k];
       }
     double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
     const int npp = na * nb;
@@ -1498,6 +1525,14 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
     if (gsh[i] != 0.0) atomicAdd(args.grad + i, gsh[i]);
 }
 
+template <int LA, int LB>
+static void grad1e_launch(int blocks, size_t smem, int use_smem, int n, const int2* pairs, const ShellDev& sh,
+                          const OneEGradArgs& a, cudaStream_t s) {
+  PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<LA, LB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  grad1e_kernel<LA, LB><<<blocks, 128, smem, s>>>(n, pairs, sh.cen, sh.desc, sh.nprim, sh.ex, sh.co, sh.mol, use_smem,
+                                                  a);
+}
+
 void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEGradArgs& a,
                    int num_sms, cudaStream_t s) {
   // per-atom partial sums in shared memory while they fit (one molecule),
@@ -1505,26 +1540,18 @@ void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pair
   const size_t need = 3 * (size_t)a.natoms_total * sizeof(double);
   const int use_smem = need <= 96 * 1024;
   const size_t smem = use_smem ? need : 0;
-  for (int c = 0; c < NCLASS; ++c) {
+  for (int c = 0; c < NPAIRCLASS; ++c) {
     if (npair[c] <= 0) continue;
     // one warp per pair; with global atomics up to 16 blocks per SM (a batch's
     // many pairs), with per-block sums 4 (each block flushes 3 natoms sums)
     const int blocks = std::max(1, std::min((npair[c] + 3) / 4, (use_smem ? 4 : 16) * num_sms));
-    dim3 grid(blocks), block(128);
-    if (c == 0) {
-      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<0, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<0, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
-                                                    sh.mol, use_smem, a);
-    }
-    if (c == 1) {
-      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<1, 0><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
-                                                    sh.mol, use_smem, a);
-    }
-    if (c == 2) {
-      PF_CUDA(cudaFuncSetAttribute(grad1e_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      grad1e_kernel<1, 1><<<grid, block, smem, s>>>(npair[c], pairs[c], sh.cen, sh.desc, sh.nprim, sh.ex, sh.co,
-                                                    sh.mol, use_smem, a);
+    switch (c) {
+      case 0: grad1e_launch<0, 0>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
+      case 1: grad1e_launch<1, 0>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
+      case 2: grad1e_launch<1, 1>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
+      case 3: grad1e_launch<2, 0>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
+      case 4: grad1e_launch<2, 1>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
+      default: grad1e_launch<2, 2>(blocks, smem, use_smem, npair[c], pairs[c], sh, a, s); break;
     }
     PF_CUDA(cudaGetLastError());
     count_launch();

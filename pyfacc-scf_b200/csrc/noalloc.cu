@@ -108,6 +108,8 @@ extern "C" int pyfacc_jk_noalloc(const pyfacc_molecule* mol, const char* data_di
     }
     const Basis B = build_basis(resolve_basis_file(mol->basis, data_dir), species, xyz);
     const int ns = (int)B.shells.size(), nbf = B.nbf;
+    for (const Shell& sh : B.shells)
+      if (sh.l > 1) throw Error(PYFACC_ERR_UNSUPPORTED_L, "pyfacc_jk_noalloc covers s and p shells only");
 
     // ---- shells and the canonical pair list grouped by class (host)
     std::vector<double4> cen(ns);

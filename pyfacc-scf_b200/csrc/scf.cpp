@@ -98,6 +98,11 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
         launch_jk(pd, tasks[bc][kc][0], bc, kc, false, nk, a, num_sms, (nth & 1) ? ctx.side : stream);
       }
     }
+  // quartets with a d pair: FP64, warp-cooperative kernels (full lists,
+  // Schwarz-screened; the density test is made per quartet in the kernel)
+  if (has_d)
+    for (int bc = NCLASS; bc < NPAIRCLASS; ++bc)
+      for (int kc = 0; kc <= bc; ++kc) launch_jk_d(pd, tasks[bc][kc][0], bc, kc, nk, a, num_sms, stream);
   PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
   PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
   if (reducer) {  // partial J/K of this shard -> sums over all shards
@@ -135,6 +140,8 @@ void System::eri_tensor(double* eri) {
   // unscreened canonical quartets: use a system-local zero-threshold task set
   for (int bc = 0; bc < NCLASS; ++bc)
     for (int kc = 0; kc <= bc; ++kc) launch_eri_tensor(pd, tasks[bc][kc][0], bc, kc, nbf, eri, stream);
+  for (int bc = NCLASS; bc < NPAIRCLASS; ++bc)
+    for (int kc = 0; kc <= bc; ++kc) launch_eri_tensor_d(pd, tasks[bc][kc][0], bc, kc, nbf, eri, stream);
 }
 
 // X = U s^-1/2 from S (la.f90:28-57).  cuSOLVER works column-major; S is
@@ -204,18 +211,24 @@ std::vector<double> atomic_occupations(const Basis& basis, const std::vector<int
   std::vector<double> occ(basis.nbf, 0.0);
   double total = 0.0;
   for (int a = 0; a < natoms; ++a) {
-    std::vector<int> ss, ps;
+    std::vector<int> ss, ps, ds;
     for (int s = 0; s < ns; ++s)
-      if (basis.shells[s].atom == a) (basis.shells[s].l == 0 ? ss : ps).push_back(s);
+      if (basis.shells[s].atom == a) (basis.shells[s].l == 0 ? ss : (basis.shells[s].l == 1 ? ps : ds)).push_back(s);
     std::vector<int> order;
     for (size_t k = 0; k < std::max(ss.size(), ps.size() + 1); ++k) {
       if (k < ss.size()) order.push_back(ss[k]);
       if (k >= 1 && k - 1 < ps.size()) order.push_back(ps[k - 1]);
     }
+    // d shells (3d of Sc..Zn, core 3d/4d of heavier atoms) before the
+    // outermost p shell: 4s then 3d then 4p
+    if (!ds.empty() && !order.empty() && basis.shells[order.back()].l == 1)
+      order.insert(order.end() - 1, ds.begin(), ds.end());
+    else
+      order.insert(order.end(), ds.begin(), ds.end());
     double left = Z[a];
     for (int s : order) {
       const int l = basis.shells[s].l, nf = (l + 1) * (l + 2) / 2;
-      const double take = std::min(left, l == 0 ? 2.0 : 6.0);
+      const double take = std::min(left, l == 0 ? 2.0 : (l == 1 ? 6.0 : 10.0));
       left -= take;
       for (int f = 0; f < nf; ++f) occ[basis.bf_off[s] + f] = take / nf;
       total += take;
@@ -709,6 +722,9 @@ void System::gradient(double* g_host) {
         launch_grad2e(pd, tasks[bc][kc][0], bc, kc, false, g2, num_sms, stream);
       }
     }
+  if (has_d)
+    for (int bc = NCLASS; bc < NPAIRCLASS; ++bc)
+      for (int kc = 0; kc <= bc; ++kc) launch_grad2e_d(pd, tasks[bc][kc][0], bc, kc, g2, num_sms, stream);
   PF_CUDA(cudaEventRecord(ctx.join, ctx.side));
   PF_CUDA(cudaStreamWaitEvent(stream, ctx.join, 0));
   if (reducer) reduce(grad_dev, 3LL * natoms);

@@ -50,12 +50,15 @@ struct System {
   // ---- device data
   ShellDev shd;
   double4* atoms_dev = nullptr;
-  int2* pairs1e[NCLASS] = {nullptr, nullptr, nullptr};  // per class, l_a >= l_b
-  int n1e[NCLASS] = {0, 0, 0};
+  int2* pairs1e[NPAIRCLASS] = {};  // per pair class ss, ps, pp, ds, dp, dd (l_a >= l_b)
+  int n1e[NPAIRCLASS] = {};
   int* bf_off_dev = nullptr;
   int* nfun_dev = nullptr;
   PairData pd;
-  TaskList tasks[NCLASS][NCLASS][3];  // [bra class][ket class][full fp64 | mixed fp64 | mixed fp32]
+  // [bra class][ket class][full fp64 | mixed fp64 | mixed fp32]; the d
+  // classes (3..5) use the full lists only (their quartets stay in FP64)
+  TaskList tasks[NPAIRCLASS][NPAIRCLASS][3];
+  bool has_d = false;  // the basis holds d shells
   DeviceBuf task_buf;
   long long quartets_total = 0;
   DynTaskSet dyn;          // per-build task lists (mixed precision)

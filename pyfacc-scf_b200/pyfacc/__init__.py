@@ -231,11 +231,12 @@ _QCLASS_NAMES = ("ss|ss", "ps|ss", "ps|ps", "pp|ss", "pp|ps", "pp|pp")
 
 def batch_stats() -> dict:
     """Timings, counters and task widths of the last run_batch on this thread."""
-    n = len(_BATCH_STAT_KEYS) + len(_QCLASS_NAMES)
+    n = len(_BATCH_STAT_KEYS) + len(_QCLASS_NAMES) + 1
     buf = (ctypes.c_double * n)()
     N.check(lib().pyfacc_batch_last_stats(buf, n), "pyfacc_batch_last_stats")
     out = {k: buf[i] for i, k in enumerate(_BATCH_STAT_KEYS)}
     out["task_width"] = {q: int(buf[len(_BATCH_STAT_KEYS) + i]) for i, q in enumerate(_QCLASS_NAMES)}
+    out["scf_graph_launches"] = int(buf[n - 1])
     return out
 
 

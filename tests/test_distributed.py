@@ -123,3 +123,60 @@ def test_sharded_scf_two_shards_one_gpu(engine):
         assert np.abs(g - ref.gradient).max() < 1e-8
     # each shard evaluated a share of the quartets
     assert 0 < results[0][2] < ref.quartets["fp64"] and 0 < results[1][2] < ref.quartets["fp64"]
+
+
+def _sharded_worker(rank, world, port, out_dir, precision):
+    """One rank of the product's sharded path: pyfacc.distributed.
+    sharded_system (its TorchReducer all-reduces every partial J/K and the
+    two-electron gradient over the process group), SCF + gradient."""
+    import sys
+    sys.path.insert(0, PKG)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    import pyfacc
+    from pyfacc import geometry as G
+    from pyfacc.distributed import sharded_system
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    torch.cuda.set_device(0)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    sp, xyz = G.alkane(8, seed=5)
+    mol = pyfacc.Molecule(sp, xyz, "sto-3g")
+    s = sharded_system(mol, precision=precision)
+    r = s.scf()
+    g = s.gradient()
+    np.save(os.path.join(out_dir, f"rank{rank}.npy"),
+            np.concatenate([[r.energy, float(r.converged), float(r.quartets["fp64"] + r.quartets["fp32"])],
+                            g.ravel()]))
+    s.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sharded_system_two_processes_gloo(engine, tmp_path, precision):
+    """Two processes share one GPU and one molecule through the product's
+    torch.distributed reducer (gloo all-reduces the CUDA buffers on the host
+    side; no kernel of one rank waits on the other): both ranks reproduce
+    the unsharded energy and gradient."""
+    import socket
+    import torch.multiprocessing as mp
+    from pyfacc import geometry as G
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    mp.start_processes(_sharded_worker, args=(2, port, str(tmp_path), precision), nprocs=2, join=True,
+                       start_method="spawn")
+    sp, xyz = G.alkane(8, seed=5)
+    ref = engine.run(engine.Molecule(sp, xyz, "sto-3g"), gradient=True, precision=precision)
+    nq_ref = ref.quartets["fp64"] + ref.quartets["fp32"]
+    for rank in range(2):
+        v = np.load(tmp_path / f"rank{rank}.npy")
+        e, conv, nq, g = v[0], v[1], v[2], v[3:].reshape(-1, 3)
+        assert conv == 1.0
+        tol_e, tol_g = (1e-9, 1e-8) if precision == "fp64" else (1e-6, 1e-5)
+        assert e == pytest.approx(ref.energy, abs=tol_e)
+        assert np.abs(g - ref.gradient).max() < tol_g
+        if precision == "fp64":
+            assert 0 < nq < nq_ref  # each rank evaluated a share of the same static lists

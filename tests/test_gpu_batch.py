@@ -131,3 +131,21 @@ def test_batch_s_only_molecules(engine, precision):
             assert r.converged and rs.converged
             assert r.energy == pytest.approx(rs.energy, abs=1e-7)
             assert np.abs(r.gradient - rs.gradient).max() < 1e-6
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_scf_is_one_graph_launch(engine, precision):
+    """The whole batched SCF is one CUDA graph launch: the build variant of
+    every iteration (all-FP32 coarse, full, incremental) and the loop's end
+    are decided on the device; the results match the molecules run one by
+    one."""
+    from pyfacc import geometry as G
+    mols = _mols(engine, G.water_clusters(count=12, seed=21, nmin=3, nmax=8))
+    rb = engine.run_batch(mols, precision=precision)
+    st = engine.batch_stats()
+    assert st["scf_graph_launches"] == 1
+    assert st["iterations"] >= 5
+    for m, r in zip(mols[:4], rb[:4]):
+        rs = engine.run(m, precision=precision)
+        assert r.converged
+        assert r.energy == pytest.approx(rs.energy, abs=1e-8 if precision == "fp64" else 1e-6)
