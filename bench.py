@@ -189,19 +189,34 @@ def jk_rates(sy, nb=20):
     return out, P
 
 
-def oracle_iterations(wl):
+def oracle_fixture(wl):
     path = os.path.join(ROOT, "tests", "golden", f"{wl}_sto3g.json")
     try:
         with open(path) as fh:
-            d = json.load(fh)
-        if "scf_iterations" in d:
-            return int(d["scf_iterations"]), f"oracle SCF iterations from {os.path.relpath(path, ROOT)}"
+            return json.load(fh), os.path.relpath(path, ROOT)
     except OSError:
-        pass
+        return None, None
+
+
+def oracle_iterations(wl):
+    d, rel = oracle_fixture(wl)
+    if d and "scf_iterations" in d:
+        return int(d["scf_iterations"]), f"oracle SCF iterations from {rel}"
     return ORACLE_SCF_ITERS.get(wl, 24), "oracle SCF iterations measured by running oracle.scf on this molecule"
 
 
-def cpu_sample(wl, P=None, jk_stride=32, grad_stride=256):
+def full_run_note(wl):
+    """The oracle's whole SCF + gradient of this molecule, timed once when its
+    fixture was generated (on that machine's threads), for comparison with
+    the sampled estimate."""
+    d, rel = oracle_fixture(wl)
+    if not d or "oracle_seconds" not in d:
+        return None
+    t = d["oracle_seconds"]
+    return {"s": t.get("scf", 0.0) + t.get("gradient", 0.0), "threads": d.get("oracle_threads"), "source": rel}
+
+
+def cpu_sample(wl, P=None, jk_stride=16, grad_stride=128):
     """The oracle (CPU restatement of the reference path, OpenMP on all host
     cores) on a bounded uniform sample of one energy + gradient of the
     workload, scaled to the whole: one-electron matrices in full, one dense
@@ -246,7 +261,8 @@ def cpu_sample(wl, P=None, jk_stride=32, grad_stride=256):
                        f"gradient (x{grad_stride} = {t_grad:.1f} s); value = 1e + {iters} x (build + dense) + "
                        f"gradient, {src}"),
             "parts_s": {"one_electron": t_1e, "fock_build": t_jk, "dense_step": t_dense, "gradient": t_grad},
-            "scf_iterations": iters}
+            "scf_iterations": iters,
+            "full_run_when_fixture_was_made": full_run_note(wl)}
 
 
 def run_ours(args):
