@@ -1008,7 +1008,9 @@ void Batch::gradient_run() {
   g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
   g2.ns_ld = ns_max;
   g2.thresh = opt.schwarz_thresh;
-  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
+  double cut_scale = 1.0;
+  for (const auto& m : mols) cut_scale = std::min(cut_scale, grad_prim_cut_scale(m.basis));
+  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD * cut_scale;
   g2.natoms_total = natoms_tot;
   g2.uhf = 0;
   g2.grad = grad_dev;

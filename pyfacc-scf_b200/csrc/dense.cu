@@ -1,10 +1,12 @@
 // Dense FP64 work of the single-molecule SCF step on the FP64 tensor cores.
 //
 //  * dgemm_kernel: C = alpha op(A) op(B) + beta Y for row-major matrices,
-//    one warp per 16 x 16 output tile (2 x 2 tiles of mma.sync m8n8k4 f64),
-//    operands read from L2/L1 (the matrices of one molecule are a few MB at
-//    most and stay resident), k unrolled by 4 so that 16 loads per lane are
-//    in flight; optionally only the upper-triangle tiles of a symmetric
+//    one block of four warps per 16 x 16 output tile (2 x 2 tiles of
+//    mma.sync m8n8k4 f64), the k range split four ways between the warps and
+//    the partial tiles added through shared memory; operands read from
+//    L2/L1 (the matrices of one molecule are a few MB at most and stay
+//    resident), 16 loads per lane in flight; optionally only the
+//    upper-triangle tiles of a symmetric
 //    result, mirrored on the store, and optionally op(A) = A - A^T (the
 //    commutator F P S - S P F of the DIIS error).
 //  * TC2 purification (Niklasson 2002) of F' = X^T F X as one CUDA graph per
@@ -67,11 +69,12 @@ __device__ __forceinline__ bool tile_of(int t, int ntm, int ntn, int& ti, int& t
   return true;
 }
 
-// Accumulate the 16 x 16 tile at (i0, j0) of op(A) op(B) over k in [0, K):
-// acc[r][c][0..1] for the 8 x 8 sub-tile (r, c).  Elements outside the
-// matrices read as zero.
+// Accumulate the 16 x 16 tile at (i0, j0) of op(A) op(B) over k in
+// [kb, ke): acc[r][c][0..1] for the 8 x 8 sub-tile (r, c).  Elements outside
+// the matrices read as zero.
 template <bool TA, bool TB, bool ASYMA>
-__device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, double (&acc)[2][2][2]) {
+__device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, int kb, int ke,
+                                             double (&acc)[2][2][2]) {
   const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
 #pragma unroll
   for (int r = 0; r < 2; ++r)
@@ -89,12 +92,12 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
   auto opB = [&](int k, int j) -> double {
     return TB ? __ldg(g.B + (size_t)j * g.ldb + k) : __ldg(g.B + (size_t)k * g.ldb + j);
   };
-  for (int k0 = 0; k0 < g.k; k0 += 16) {
+  for (int k0 = kb; k0 < ke; k0 += 16) {
     double a[4][2], b[4][2];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int kk = k0 + 4 * u + tq;
-      const bool kok = kk < g.k;
+      const bool kok = kk < ke;
 #pragma unroll
       for (int r = 0; r < 2; ++r) a[u][r] = (kok && rok[r]) ? opA(ra[r], kk) : 0.0;
 #pragma unroll
@@ -109,15 +112,40 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
   }
 }
 
+// One 16 x 16 tile per block of SPLITK warps: warp w sums its share of k
+// (the matrices here are at most a few hundred wide, so a warp alone would
+// spend the kernel waiting on one L2 round trip per 16 k; split four ways
+// the waits overlap), then warp 0 adds the other warps' partial tiles from
+// shared memory.  Returns true on warp 0, whose acc holds the tile.
+constexpr int SPLITK = 4;
+template <bool TA, bool TB, bool ASYMA>
+__device__ __forceinline__ bool block_tile(const GemmArgs& g, int i0, int j0, double (&acc)[2][2][2]) {
+  __shared__ double part[SPLITK - 1][8][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nchunk = (g.k + 15) >> 4, per = (nchunk + SPLITK - 1) / SPLITK;
+  const int kb = min(warp * per * 16, g.k), ke = min((warp + 1) * per * 16, g.k);
+  tile_product<TA, TB, ASYMA>(g, i0, j0, kb, ke, acc);
+  if (warp > 0) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) part[warp - 1][q][lane] = acc[q >> 2][(q >> 1) & 1][q & 1];
+  }
+  __syncthreads();
+  if (warp > 0) return false;
+#pragma unroll
+  for (int w = 0; w < SPLITK - 1; ++w)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q >> 2][(q >> 1) & 1][q & 1] += part[w][q][lane];
+  return true;
+}
+
 template <bool TA, bool TB, bool SYM, bool ASYMA>
-__global__ void __launch_bounds__(64) dgemm_kernel(const GemmArgs g) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+__global__ void __launch_bounds__(32 * SPLITK) dgemm_kernel(const GemmArgs g) {
   const int ntm = (g.m + 15) >> 4, ntn = (g.n + 15) >> 4;
   int ti, tj;
-  if (!tile_of<SYM>(warp, ntm, ntn, ti, tj)) return;
+  if (!tile_of<SYM>(blockIdx.x, ntm, ntn, ti, tj)) return;
   const int i0 = ti << 4, j0 = tj << 4;
   double acc[2][2][2];
-  tile_product<TA, TB, ASYMA>(g, i0, j0, acc);
+  if (!block_tile<TA, TB, ASYMA>(g, i0, j0, acc)) return;
   const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
 #pragma unroll
   for (int r = 0; r < 2; ++r)
@@ -139,8 +167,7 @@ template <bool TA, bool TB, bool SYM, bool ASYMA>
 void gemm_launch(const GemmArgs& g, cudaStream_t s) {
   const int ntm = (g.m + 15) / 16, ntn = (g.n + 15) / 16;
   const long long tiles = SYM ? (long long)ntn * (ntn + 1) / 2 : (long long)ntm * ntn;
-  const int blocks = (int)((tiles + 1) / 2);
-  dgemm_kernel<TA, TB, SYM, ASYMA><<<blocks, 64, 0, s>>>(g);
+  dgemm_kernel<TA, TB, SYM, ASYMA><<<(int)tiles, 32 * SPLITK, 0, s>>>(g);
 }
 
 // ---------------------------------------------------------------------------
@@ -231,7 +258,7 @@ struct Tc2StepArgs {
 // 2 Tr X - Tr X^2, else (2, -1) -- the choice every warp makes from the
 // traces of Xin that the previous step accumulated.  Once Tr X - Tr X^2 <
 // 1e-9 at the right trace, two more steps run, then the iterate is copied.
-__global__ void __launch_bounds__(64) tc2g_step_kernel(const Tc2StepArgs s) {
+__global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArgs s) {
   const double* cin = s.st + ST_CTL + 8 * s.parity;
   double* cout = s.st + ST_CTL + 8 * (1 - s.parity);
   const double countdown0 = cin[0];
@@ -268,16 +295,16 @@ __global__ void __launch_bounds__(64) tc2g_step_kernel(const Tc2StepArgs s) {
     if (s.set_cond) cudaGraphSetConditional(s.cond, (now_done || failed) ? 0u : 1u);
   }
   const int n = s.n;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nt = (n + 15) >> 4;
   int ti, tj;
-  if (!tile_of<true>(warp, nt, nt, ti, tj)) return;
+  if (!tile_of<true>(blockIdx.x, nt, nt, ti, tj)) return;
   const int i0 = ti << 4, j0 = tj << 4;
   double acc[2][2][2];
   if (!was_done) {
     GemmArgs g{n, n, n, s.Xin, n, s.Xin, n, nullptr, n, 1.0, nullptr, n, 0.0};
-    tile_product<false, false, false>(g, i0, j0, acc);
+    if (!block_tile<false, false, false>(g, i0, j0, acc)) return;
   } else {
+    if (threadIdx.x >= 32) return;
     a = 1.0;
     b = 0.0;
 #pragma unroll
@@ -395,7 +422,7 @@ cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, d
     PF_CUDA(cudaGraphAddNode(&nw, graph, &ni, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     const int nt = (n + 15) / 16;
-    const int blocks = (nt * (nt + 1) / 2 + 1) / 2;
+    const int blocks = nt * (nt + 1) / 2;
     cudaGraphNode_t s0 = nullptr, s1 = nullptr;
     for (int par = 0; par < 2; ++par) {
       Tc2StepArgs a;
@@ -412,7 +439,7 @@ cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, d
       cudaKernelNodeParams p{};
       p.func = reinterpret_cast<void*>(tc2g_step_kernel);
       p.gridDim = dim3(blocks);
-      p.blockDim = dim3(64);
+      p.blockDim = dim3(32 * SPLITK);
       p.kernelParams = args;
       if (par == 0) PF_CUDA(cudaGraphAddKernelNode(&s0, body, nullptr, 0, &p));
       else PF_CUDA(cudaGraphAddKernelNode(&s1, body, &s0, 1, &p));

@@ -59,6 +59,11 @@ constexpr double PRIM_QUARTET_REL = 1e-2;
 // C20H42..C100H202 by ~1e-9 Ha/bohr and leaves it translationally invariant
 // (the fourth centre is minus the sum of the other three)
 constexpr double PRIM_QUARTET_REL_GRAD = 1.0;
+// The derivative factor 2 alpha grows with the tightest primitive: above an
+// exponent of 100 (core shells of P and heavier atoms, the STO-6G carbon 1s)
+// the gradient cut shrinks by 100 / alpha_max (grad_prim_cut_scale below;
+// ZnH2: the unscaled cut left 2e-7 Ha/bohr against the oracle's gradient).
+constexpr double GRAD_CUT_ALPHA = 100.0;
 // quartet screening threshold of the all-FP32 builds of the first mixed
 // iterations (their error is discarded by the full build that ends them);
 // 1e-8 costs C100H202 an extra iteration
@@ -91,6 +96,15 @@ struct Basis {
   std::vector<int> bf_off;  // nshell + 1
   int nbf = 0;
 };
+
+// Scale of the gradient's primitive-quartet cut for a basis (min(1,
+// GRAD_CUT_ALPHA / largest exponent)).
+inline double grad_prim_cut_scale(const Basis& b) {
+  double amax = 0.0;
+  for (const Shell& s : b.shells)
+    for (double a : s.ex) amax = a > amax ? a : amax;
+  return amax > GRAD_CUT_ALPHA ? GRAD_CUT_ALPHA / amax : 1.0;
+}
 
 // Argument checks of a molecule (engine.cpp): pointers and finite
 // coordinates; throws PYFACC_ERR_INVALID.

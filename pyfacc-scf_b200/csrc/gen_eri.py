@@ -86,6 +86,11 @@ def fma_chain(terms, tail=None):
     return expr
 
 
+def plain_sum(terms):
+    """sum of the products a * b of terms as a plain expression."""
+    return " + ".join(f"{a} * {b}" for a, b in terms)
+
+
 class Emitter:
     def __init__(self):
         self.lines = []
@@ -103,10 +108,15 @@ class Emitter:
 class Vrr:
     """Symbolic OS VRR on one primitive quartet."""
 
-    def __init__(self, em: Emitter, L: int):
+    def __init__(self, em: Emitter, L: int, packed: bool = True):
+        # packed: pf_fma chains (the J/K routines, instantiated for the packed
+        # float pair too); else plain sums, which the compiler contracts and
+        # schedules more freely in the large gradient routines (their pf_fma
+        # form spilled to local memory)
         self.em = em
         self.L = L
         self.memo = {}
+        self.packed = packed
 
     def V(self, e, f, m):
         key = (e, f, m)
@@ -121,21 +131,27 @@ class Vrr:
             terms, fl = [(f"PA[{i}]", self.V(e1, f, m)), (f"WP[{i}]", self.V(e1, f, m + 1))], 3
             if e1[i] > 0:
                 e2 = down(e1, i)
-                terms.append((scaled(e1[i], "o2p"), f"pf_fma(nrp, {self.V(e2, f, m + 1)}, {self.V(e2, f, m)})"))
+                if self.packed:
+                    terms.append((scaled(e1[i], "o2p"), f"pf_fma(nrp, {self.V(e2, f, m + 1)}, {self.V(e2, f, m)})"))
+                else:
+                    terms.append((scaled(e1[i], "o2p"), f"({self.V(e2, f, m)} + nrp * {self.V(e2, f, m + 1)})"))
                 fl += 4 + (1 if e1[i] > 1 else 0)
-            r = em.tmp(fma_chain(terms), fl)
+            r = em.tmp(fma_chain(terms) if self.packed else plain_sum(terms), fl)
         else:
             i = first_axis(f)
             f1 = down(f, i)
             terms, fl = [(f"QC[{i}]", self.V(e, f1, m)), (f"WQ[{i}]", self.V(e, f1, m + 1))], 3
             if f1[i] > 0:
                 f2 = down(f1, i)
-                terms.append((scaled(f1[i], "o2q"), f"pf_fma(nrq, {self.V(e, f2, m + 1)}, {self.V(e, f2, m)})"))
+                if self.packed:
+                    terms.append((scaled(f1[i], "o2q"), f"pf_fma(nrq, {self.V(e, f2, m + 1)}, {self.V(e, f2, m)})"))
+                else:
+                    terms.append((scaled(f1[i], "o2q"), f"({self.V(e, f2, m)} + nrq * {self.V(e, f2, m + 1)})"))
                 fl += 4 + (1 if f1[i] > 1 else 0)
             if e[i] > 0:
                 terms.append((scaled(e[i], "o2pq"), self.V(down(e, i), f1, m + 1)))
                 fl += 2 + (1 if e[i] > 1 else 0)
-            r = em.tmp(fma_chain(terms), fl)
+            r = em.tmp(fma_chain(terms) if self.packed else plain_sum(terms), fl)
         self.memo[key] = r
         return r
 
@@ -143,11 +159,12 @@ class Vrr:
 class Hrr:
     """Symbolic HGP HRR.  base(e, f) gives the name of [e0|f0]."""
 
-    def __init__(self, em: Emitter, base):
+    def __init__(self, em: Emitter, base, packed: bool = True):
         self.em = em
         self.base = base
         self.mb = {}
         self.mk = {}
+        self.packed = packed
 
     def bra(self, a, b, f):
         key = (a, b, f)
@@ -157,7 +174,8 @@ class Hrr:
             r = self.base(a, f)
         else:
             i = first_axis(b)
-            r = self.em.tmp(f"pf_fma(AB[{i}], {self.bra(a, down(b, i), f)}, {self.bra(up(a, i), down(b, i), f)})", 2)
+            x, y = self.bra(up(a, i), down(b, i), f), self.bra(a, down(b, i), f)
+            r = self.em.tmp(f"pf_fma(AB[{i}], {y}, {x})" if self.packed else f"{x} + AB[{i}] * {y}", 2)
         self.mb[key] = r
         return r
 
@@ -169,8 +187,8 @@ class Hrr:
             r = self.bra(a, b, c)
         else:
             i = first_axis(d)
-            r = self.em.tmp(f"pf_fma(CD[{i}], {self.full(a, b, c, down(d, i))}, {self.full(a, b, up(c, i), down(d, i))})",
-                            2)
+            x, y = self.full(a, b, up(c, i), down(d, i)), self.full(a, b, c, down(d, i))
+            r = self.em.tmp(f"pf_fma(CD[{i}], {y}, {x})" if self.packed else f"{x} + CD[{i}] * {y}", 2)
         self.mk[key] = r
         return r
 
@@ -240,8 +258,8 @@ def gen_class(la, lb, lc, ld):
     grad_flops = 0
     for ctr in range(3 if L >= 4 else 0):
         em = Emitter()
-        v = Vrr(em, L + 1)
-        h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
+        v = Vrr(em, L + 1, packed=False)
+        h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0), packed=False)
         outs = []
         for x in range(3):
             up_terms, dn_terms = [], []
@@ -260,12 +278,12 @@ def gen_class(la, lb, lc, ld):
                                 qd[ctr] = down(q[ctr], x)
                                 dn_terms.append((scaled(cnt, f"gam[{k}]"), h.full(*qd)))
                             k += 1
-            su = em.tmp(fma_chain(up_terms), 2 * len(up_terms) - 1)
+            su = em.tmp(plain_sum(up_terms), 2 * len(up_terms) - 1)
             expr = f"tw * {su}"
             fl = 2
             if dn_terms:
-                sd = em.tmp(fma_chain(dn_terms), 2 * len(dn_terms) - 1)
-                expr = f"pf_fma(tw, {su}, R(-1.0f) * {sd})"
+                sd = em.tmp(plain_sum(dn_terms), 2 * len(dn_terms) - 1)
+                expr = f"tw * {su} - {sd}"
                 fl += 1
             em.flops += fl
             outs.append(expr)
@@ -285,8 +303,8 @@ def gen_class(la, lb, lc, ld):
     for ctr in range(0 if L >= 4 else 3):
         for x in range(3):
             em = Emitter()
-            v = Vrr(em, L + 1)
-            h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0))
+            v = Vrr(em, L + 1, packed=False)
+            h = Hrr(em, lambda e, f, v=v: v.V(e, f, 0), packed=False)
             up_terms, dn_terms = [], []
             k = 0
             for a in comps(la):
@@ -303,12 +321,12 @@ def gen_class(la, lb, lc, ld):
                                 qd[ctr] = down(q[ctr], x)
                                 dn_terms.append((scaled(cnt, f"gam[{k}]"), h.full(*qd)))
                             k += 1
-            su = em.tmp(fma_chain(up_terms), 2 * len(up_terms) - 1)
+            su = em.tmp(plain_sum(up_terms), 2 * len(up_terms) - 1)
             expr = f"tw * {su}"
             fl = 2
             if dn_terms:
-                sd = em.tmp(fma_chain(dn_terms), 2 * len(dn_terms) - 1)
-                expr = f"pf_fma(tw, {su}, R(-1.0f) * {sd})"
+                sd = em.tmp(plain_sum(dn_terms), 2 * len(dn_terms) - 1)
+                expr = f"tw * {su} - {sd}"
                 fl += 1
             em.flops += fl
             grad_flops += em.flops

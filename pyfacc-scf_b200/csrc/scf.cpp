@@ -684,7 +684,7 @@ void System::gradient(double* g_host) {
   g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
   g2.ns_ld = ns;
   g2.thresh = opt.schwarz_thresh;
-  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD;
+  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD * grad_prim_cut_scale(basis);
   g2.natoms_total = natoms;
   g2.uhf = uhf ? 1 : 0;
   g2.grad = grad_dev;

@@ -19,8 +19,10 @@ def test_max_iter_returns_last_energy_not_converged(engine):
     r = engine.run(mol, max_iter=1, check=False)
     assert r.status == N.ERR_NOT_CONVERGED and not r.converged and r.n_iter == 1
     assert math.isfinite(r.energy)
+    # (the first iteration's energy is that of the guess density, which need
+    # not be idempotent, so it is not an upper bound of the converged one)
     full = engine.run(mol)
-    assert full.converged and full.energy < r.energy + 1e-6
+    assert full.converged and full.n_iter > 1
     # the drop-in entry point: the energy of the last iteration, status kept
     L = N.lib()
     sp, xyz = G.water()
