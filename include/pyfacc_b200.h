@@ -84,8 +84,9 @@ typedef struct pyfacc_options {
   double gradient_fp32_thresh; /* mixed gradient: derivative quartets with
                                Q_ab Q_cd max|P| (in a batch: Q_ab Q_cd)
                                below this run in FP32
-                               (|dG| ~3e-9 Ha/bohr at 1e-3 for C20H42..
-                               C100H202); <= 0: fp32_thresh            (1e-3) */
+                               (|dG| ~6e-8 Ha/bohr at 1e-2, ~3e-9 at 1e-3
+                               for C40H82..C100H202); <= 0: fp32_thresh
+                                                                      (1e-2) */
   double coarse_err;        /* mixed: while the DIIS error is above this every
                                quartet runs in FP32; the first build below it
                                is a full mixed build that restarts the
@@ -195,7 +196,11 @@ int pyfacc_system_jk(pyfacc_system *sys, const double *Dj_dev, int nk, const dou
 /* Statistics of the last pyfacc_system_jk call on this system:
  * out[0..n) = {ms (CUDA events on the engine stream around the build),
  * algorithmic flops of the FP64 quartets, of the FP32 quartets, contracted
- * quartets FP64, FP32, primitive quartets FP64, FP32}. */
+ * quartets FP64, FP32, primitive quartets FP64, FP32}, then per s/p quartet
+ * class in the order (ss|ss) (ps|ss) (ps|ps) (pp|ss) (pp|ps) (pp|pp):
+ * out[7..13) quartets FP64, out[13..19) quartets FP32, out[19..25)
+ * primitive quartets FP64, out[25..31) primitive quartets FP32.  Entries
+ * beyond 31 are zero. */
 int pyfacc_system_jk_stats(const pyfacc_system *sys, double *out, int n);
 /* Full (nbf^4) ERI tensor on the device, small systems only (tests). */
 int pyfacc_system_eri_tensor(pyfacc_system *sys, double *eri_dev);

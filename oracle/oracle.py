@@ -466,6 +466,32 @@ def gradient(mol: Molecule, res: ScfResult, boys_mode=0, thresh=1e-12, parts=Fal
     return total
 
 
+def gradient_at_density(mol: Molecule, Ds, uhf: bool, thresh=1e-12):
+    """Analytic gradient at given spin densities Ds = [D_alpha, D_beta]
+    (RHF: [P/2, P/2]): the Fock matrices from these densities, the energy-
+    weighted density W = sum_s D_s F_s D_s (the stationarity identity that
+    replaces sum_i eps_i C_i C_i^T at a converged density), then the same
+    derivative integrals as gradient().  Compares two programs at one
+    density, free of the SCF convergence error of either."""
+    S, T, V = one_electron(mol)
+    H = T + V
+    Ds = [np.ascontiguousarray(D) for D in Ds]
+    Pt = Ds[0] + Ds[1]
+    if uhf:
+        J, K = jk(mol, np.stack(Ds), thresh)
+        Jt = J[0] + J[1]
+        Fs = [H + Jt - K[0], H + Jt - K[1]]
+    else:
+        J, K = jk(mol, Pt, thresh)
+        Fs = [H + J - 0.5 * K] * 2
+    W = Ds[0] @ Fs[0] @ Ds[0] + Ds[1] @ Fs[1] @ Ds[1]
+    na = mol.natoms
+    g = [np.zeros((na, 3)) for _ in range(4)]
+    lib().orc_gradient(*mol.shells.args(), na, _ptr(mol.xyz), _ptr(mol.Z), 0, _ptr(np.ascontiguousarray(Pt)),
+                       _ptr(Ds[0]), _ptr(Ds[1]), _ptr(np.ascontiguousarray(W)), thresh, *[_ptr(x) for x in g])
+    return g[0] + g[1] + g[2] + g[3]
+
+
 def energy(species, xyz_bohr, basis_file, **kw) -> float:
     charge = kw.pop('charge', 0)
     mol = molecule(species, xyz_bohr, basis_file, charge=charge)

@@ -369,6 +369,10 @@ void Batch::build_pairs() {
     }
   });
   const long long nprim_new = ppos[nseg];
+  for (int c = 0; c < NPAIRCLASS; ++c) pd.class_maxprim[c] = 0;
+  for (int c = 0; c < NCLASS; ++c)
+    for (int i = pd.class_off[c]; i < pd.class_off[c + 1]; ++i)
+      pd.class_maxprim[c] = std::max(pd.class_maxprim[c], kept[perm[i]]);
   pd.q_host.clear();
   pd.cls_host.clear();
   pd.mol_host.clear();

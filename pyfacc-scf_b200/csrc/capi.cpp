@@ -104,7 +104,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->task_width = 0;
   o->gradient_precision = -1;
   o->polish = 0;
-  o->gradient_fp32_thresh = 1e-3;
+  o->gradient_fp32_thresh = 1e-2;
   o->coarse_err = 1e-3;
 }
 
@@ -334,7 +334,7 @@ int pyfacc_system_jk(pyfacc_system* sys, const double* Dj_dev, int nk, const dou
     PF_CUDA(cudaEventRecord(s.ev1, s.stream));
     PF_CUDA(cudaStreamSynchronize(s.stream));
     double c[6];
-    s.jk_counters(nk, c);
+    s.jk_counters(nk, c, s.last_jk + 7);
     s.last_jk[0] = s.elapsed(s.ev0, s.ev1);
     for (int k = 0; k < 6; ++k) s.last_jk[1 + k] = c[k];
   });
@@ -342,7 +342,7 @@ int pyfacc_system_jk(pyfacc_system* sys, const double* Dj_dev, int nk, const dou
 
 int pyfacc_system_jk_stats(const pyfacc_system* sys, double* out, int n) {
   if (!sys || !out || n <= 0) return PYFACC_ERR_INVALID;
-  for (int k = 0; k < n; ++k) out[k] = k < 7 ? sys->impl->last_jk[k] : 0.0;
+  for (int k = 0; k < n; ++k) out[k] = k < System::JK_STATS_N ? sys->impl->last_jk[k] : 0.0;
   return PYFACC_OK;
 }
 

@@ -92,8 +92,8 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
   auto opB = [&](int k, int j) -> double {
     return TB ? __ldg(g.B + (size_t)j * g.ldb + k) : __ldg(g.B + (size_t)k * g.ldb + j);
   };
-  for (int k0 = kb; k0 < ke; k0 += 16) {
-    double a[4][2], b[4][2];
+  // the operands of the 16-wide k chunk at k0 (zero beyond ke)
+  auto load = [&](int k0, double (&a)[4][2], double (&b)[4][2]) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int kk = k0 + 4 * u + tq;
@@ -103,12 +103,32 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
 #pragma unroll
       for (int c = 0; c < 2; ++c) b[u][c] = (kok && cok[c]) ? opB(kk, cb[c]) : 0.0;
     }
+  };
+  if (kb >= ke) return;
+  // register double buffering: the next chunk's loads are in flight while
+  // the current chunk's products run, so a warp waits for one load latency
+  // instead of one per chunk
+  double a[4][2], b[4][2];
+  load(kb, a, b);
+  for (int k0 = kb; k0 < ke; k0 += 16) {
+    double an[4][2], bn[4][2];
+    const bool more = k0 + 16 < ke;
+    if (more) load(k0 + 16, an, bn);
 #pragma unroll
     for (int u = 0; u < 4; ++u)
 #pragma unroll
       for (int r = 0; r < 2; ++r)
 #pragma unroll
         for (int c = 0; c < 2; ++c) mma_f64(acc[r][c][0], acc[r][c][1], a[u][r], b[u][c]);
+    if (more) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          a[u][r] = an[u][r];
+          b[u][r] = bn[u][r];
+        }
+    }
   }
 }
 

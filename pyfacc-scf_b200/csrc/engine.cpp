@@ -388,7 +388,9 @@ void System::build_pairs() {
     for (int k = off[c]; k < off[c + 1]; ++k)
       if (thr <= 0 || q[k] * qmax >= thr) idx.push_back(k);
     std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return q[x] > q[y]; });
+    pd.class_maxprim[c] = 0;
     for (int k : idx) {
+      pd.class_maxprim[c] = std::max(pd.class_maxprim[c], kept[k]);
       perm.push_back(k);
       new_ps.push_back(nprim_new);
       nprim_new += kept[k];

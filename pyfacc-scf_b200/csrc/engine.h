@@ -61,8 +61,9 @@ constexpr double PRIM_QUARTET_REL = 1e-2;
 constexpr double PRIM_QUARTET_REL_GRAD = 1.0;
 // The derivative factor 2 alpha grows with the tightest primitive: above an
 // exponent of 100 (core shells of P and heavier atoms, the STO-6G carbon 1s)
-// the gradient cut shrinks by 100 / alpha_max (grad_prim_cut_scale below;
-// ZnH2: the unscaled cut left 2e-7 Ha/bohr against the oracle's gradient).
+// the gradient cut shrinks by 100 / alpha_max (grad_prim_cut_scale below),
+// so that the bound on a skipped derivative integral stays where it is for
+// the light atoms.
 constexpr double GRAD_CUT_ALPHA = 100.0;
 // quartet screening threshold of the all-FP32 builds of the first mixed
 // iterations (their error is discarded by the full build that ends them);
@@ -150,6 +151,7 @@ struct PairData {
   int npair = 0;
   int class_off[NPAIRCLASS + 1] = {0, 0, 0, 0, 0, 0, 0};  // s/p classes, then ds, dp, dd
   int nprim = 0;
+  int class_maxprim[NPAIRCLASS] = {0, 0, 0, 0, 0, 0};  // largest kept primitive-pair count per class
   int4* info0 = nullptr;     // {bf_a, bf_b, prim_start, n_prim}
   int4* info1 = nullptr;     // {shell_a, shell_b, atom_a, atom_b}
   int4* info2 = nullptr;     // {mat_off lo, mat_off hi, ld, molecule}

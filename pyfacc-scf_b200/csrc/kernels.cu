@@ -233,8 +233,17 @@ template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
 // both loops stop at the first primitive quartet with |K_ab K_cd| < kcut.
 // With kq_step > 1 only the ket primitives kq0, kq0 + kq_step, ... are
 // summed (a share of the quartet; the shares add up to the integral).
+// With kPrefetchKet the ket primitive loop loads the next ket primitive's
+// records before the bra loop of the current one.  Measured at C40H82 it
+// costs more (registers: FP64 (ss|ss) 64 -> 80) than the hidden latency
+// returns (FP64 build 4.03 -> 4.40 ms), so it is off.
+constexpr bool kPrefetchKet = false;
+
+// brec: the bra pair's first primitive record (in global memory, or the
+// copy a warp staged in shared memory); prim: all records (the kets').
 template <typename R, int LA, int LB, int LC, int LD>
-__device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __restrict__ prim, int4 bi0, int4 ki0,
+__device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __restrict__ prim,
+                                                  const typename Rec<R>::T* brec, int4 bi0, int4 ki0,
                                                   const double4& bgeo, const double4& kgeo,
                                                   R out[EriClass<R, LA, LB, LC, LD>::NOUT], double kcut = 0.0,
                                                   int kq0 = 0, int kq_step = 1) {
@@ -246,17 +255,29 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
   // the cut is compared in the records' precision (no FP64 work in the FP32
   // loop); a cut beyond the float range becomes +inf, which skips everything
   const R cut = (R)kcut;
-  const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
+  const R kab_max = fabs((R)brec[0].z);
   int nprim = 0;
+  const V* kr = prim + 3 * (size_t)ki0.z;
+  V k0 = {}, k1 = {}, k2 = {};
+  if (kq0 < ki0.w) {
+    k0 = kr[3 * kq0];
+    k1 = kr[3 * kq0 + 1];
+    k2 = kr[3 * kq0 + 2];
+  }
   for (int kq = kq0; kq < ki0.w; kq += kq_step) {
-    const V* kr = prim + 3 * (size_t)(ki0.z + kq);
-    const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const int kn = kq + kq_step;
+    V n0 = k0, n1 = k1, n2 = k2;
+    if (kPrefetchKet && kn < ki0.w) {
+      n0 = kr[3 * kn];
+      n1 = kr[3 * kn + 1];
+      n2 = kr[3 * kn + 2];
+    }
     const R kcd = fabs((R)k0.z);
     if (kab_max * kcd < cut) break;
     const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
 #pragma unroll 1
     for (int kp = 0; kp < bi0.w; ++kp) {
-      const V* br = prim + 3 * (size_t)(bi0.z + kp);
+      const V* br = brec + 3 * kp;
       const V b0 = br[0], b1 = br[1], b2 = br[2];
       if (fabs((R)b0.z) * kcd < cut) break;
       const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
@@ -264,6 +285,17 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
       C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.nrp, g.o2q, g.nrq, g.o2pq, acc);
       ++nprim;
+    }
+    if (kn < ki0.w) {
+      if (kPrefetchKet) {
+        k0 = n0;
+        k1 = n1;
+        k2 = n2;
+      } else {
+        k0 = kr[3 * kn];
+        k1 = kr[3 * kn + 1];
+        k2 = kr[3 * kn + 2];
+      }
     }
   }
   const R AB[3] = {(R)bgeo.x, (R)bgeo.y, (R)bgeo.z};
@@ -307,8 +339,8 @@ __device__ __forceinline__ void prim_setup_f2(const float4& blo0, const float4& 
 }
 
 template <int LA, int LB, int LC, int LD>
-__device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ prim, int4 bi0, int4 ki0,
-                                                     const double4& bgeo, const double4& kgeo,
+__device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ prim, const float4* brec, int4 bi0,
+                                                     int4 ki0, const double4& bgeo, const double4& kgeo,
                                                      float out[EriClass<float, LA, LB, LC, LD>::NOUT],
                                                      double kcut = 0.0, int kq0 = 0, int kq_step = 1) {
   using C2 = EriClass<F2, LA, LB, LC, LD>;
@@ -317,17 +349,29 @@ __device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ 
 #pragma unroll
   for (int i = 0; i < C2::NACC; ++i) acc[i] = F2(0.0f);
   const float cut = (float)kcut;
-  const float kab_max = fabsf(prim[3 * (size_t)bi0.z].z);
+  const float kab_max = fabsf(brec[0].z);
   int nprim = 0;
+  const float4* kr = prim + 3 * (size_t)ki0.z;
+  float4 k0 = {}, k1 = {}, k2 = {};
+  if (kq0 < ki0.w) {
+    k0 = kr[3 * kq0];
+    k1 = kr[3 * kq0 + 1];
+    k2 = kr[3 * kq0 + 2];
+  }
   for (int kq = kq0; kq < ki0.w; kq += kq_step) {
-    const float4* kr = prim + 3 * (size_t)(ki0.z + kq);
-    const float4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
+    const int kn = kq + kq_step;
+    float4 n0 = k0, n1 = k1, n2 = k2;
+    if (kPrefetchKet && kn < ki0.w) {
+      n0 = kr[3 * kn];
+      n1 = kr[3 * kn + 1];
+      n2 = kr[3 * kn + 2];
+    }
     const float kcd = fabsf(k0.z);
     if (kab_max * kcd < cut) break;
     const F2 QC[3] = {F2(k2.x), F2(k2.y), F2(k2.z)};
 #pragma unroll 1
     for (int kp = 0; kp < bi0.w; kp += 2) {
-      const float4* br = prim + 3 * (size_t)(bi0.z + kp);
+      const float4* br = brec + 3 * kp;
       const float4 b0 = br[0], b1 = br[1], b2 = br[2];
       if (fabsf(b0.z) * kcd < cut) break;
       // the second primitive, or the first again at zero weight
@@ -350,6 +394,17 @@ __device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ 
       nprim += two ? 2 : 1;
       if (!two) break;
     }
+    if (kn < ki0.w) {
+      if (kPrefetchKet) {
+        k0 = n0;
+        k1 = n1;
+        k2 = n2;
+      } else {
+        k0 = kr[3 * kn];
+        k1 = kr[3 * kn + 1];
+        k2 = kr[3 * kn + 2];
+      }
+    }
   }
   float accs[C1::NACC];
 #pragma unroll
@@ -370,7 +425,7 @@ __global__ void schwarz_kernel(int begin, int end, const int4* __restrict__ info
   double out[C::NOUT];
   const int4 i0 = info0[i];
   const double4 g = geom[i];
-  contracted_quartet<double, LA, LB, LA, LB>(prim, i0, i0, g, g, out);
+  contracted_quartet<double, LA, LB, LA, LB>(prim, prim + 3 * (size_t)i0.z, i0, i0, g, g, out);
   constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
   double mx = 0.0;
 #pragma unroll
@@ -522,6 +577,7 @@ struct JkKernelArgs {
   int nbra, ntasks, bra_base, ket_base, same_class, qclass, prec, task_begin;
   int lwidth;  // log2 of the task width: one warp runs 32 >> lwidth tasks of (1 bra) x (1 << lwidth kets)
   int psplit;  // warps per task (each takes every psplit-th ket primitive)
+  int stage;   // primitive records staged per bra in shared memory (0: read from global memory)
 };
 
 // Warps per task for a list of the given length: lists with too few warps
@@ -591,15 +647,29 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     }
     const unsigned amask = __ballot_sync(0xffffffffu, active);
     if (amask == 0u) continue;
+    // the bra's primitive records, read by every primitive of every lane of
+    // the group: staged once per task into this warp's shared-memory area
+    // (one coalesced copy by the group's lanes) when the launch gave one
+    using V = typename Rec<R>::T;
+    const V* brec = records<R>(args) + 3 * (size_t)bi0.z;
+    if (args.stage > 0) {
+      extern __shared__ __align__(16) unsigned char jk_stage_smem[];
+      V* st = reinterpret_cast<V*>(jk_stage_smem) +
+              ((size_t)(threadIdx.x >> 5) * tpw + (lane >> lw)) * 3 * (size_t)args.stage;
+      __syncwarp();
+      for (int i = sub; i < 3 * bi0.w; i += W) st[i] = brec[i];
+      __syncwarp();
+      brec = st;
+    }
     R out[C::NOUT];
     int nprim = 0;
     if (active) {
       // FP32 quartets: two primitives per step in packed pairs, except
       // (pp|pp), whose 81 packed accumulators would not fit the registers
       if constexpr (sizeof(R) == 4 && C::L < 4)
-        nprim = contracted_quartet_f2<LA, LB, LC, LD>(args.primf, bi0, ki0, bg, kg, out, kcut, slice, ps);
+        nprim = contracted_quartet_f2<LA, LB, LC, LD>(args.primf, brec, bi0, ki0, bg, kg, out, kcut, slice, ps);
       else
-        nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), bi0, ki0, bg, kg, out, kcut, slice, ps);
+        nprim = contracted_quartet<R, LA, LB, LC, LD>(records<R>(args), brec, bi0, ki0, bg, kg, out, kcut, slice, ps);
     } else {
 #pragma unroll
       for (int i = 0; i < C::NOUT; ++i) out[i] = (R)0;
@@ -730,22 +800,30 @@ static int qclass_of(int bc, int kc) {
 }
 
 template <typename R, int LA, int LB, int LC, int LD>
-static void jk_dispatch_nk(int nk, dim3 grid, dim3 block, cudaStream_t s, const JkKernelArgs& k) {
-  if (nk == 1) jk_kernel<R, LA, LB, LC, LD, 1><<<grid, block, 0, s>>>(k);
-  else jk_kernel<R, LA, LB, LC, LD, 2><<<grid, block, 0, s>>>(k);
+static void jk_dispatch_nk(int nk, dim3 grid, dim3 block, size_t smem, cudaStream_t s, const JkKernelArgs& k) {
+  if (nk == 1) jk_kernel<R, LA, LB, LC, LD, 1><<<grid, block, smem, s>>>(k);
+  else jk_kernel<R, LA, LB, LC, LD, 2><<<grid, block, smem, s>>>(k);
 }
 
 template <typename R>
-static void jk_dispatch(int qc, int nk, dim3 grid, dim3 block, cudaStream_t s, const JkKernelArgs& k) {
+static void jk_dispatch(int qc, int nk, dim3 grid, dim3 block, size_t smem, cudaStream_t s, const JkKernelArgs& k) {
   switch (qc) {
-    case 0: jk_dispatch_nk<R, 0, 0, 0, 0>(nk, grid, block, s, k); break;
-    case 1: jk_dispatch_nk<R, 1, 0, 0, 0>(nk, grid, block, s, k); break;
-    case 2: jk_dispatch_nk<R, 1, 0, 1, 0>(nk, grid, block, s, k); break;
-    case 3: jk_dispatch_nk<R, 1, 1, 0, 0>(nk, grid, block, s, k); break;
-    case 4: jk_dispatch_nk<R, 1, 1, 1, 0>(nk, grid, block, s, k); break;
-    default: jk_dispatch_nk<R, 1, 1, 1, 1>(nk, grid, block, s, k); break;
+    case 0: jk_dispatch_nk<R, 0, 0, 0, 0>(nk, grid, block, smem, s, k); break;
+    case 1: jk_dispatch_nk<R, 1, 0, 0, 0>(nk, grid, block, smem, s, k); break;
+    case 2: jk_dispatch_nk<R, 1, 0, 1, 0>(nk, grid, block, smem, s, k); break;
+    case 3: jk_dispatch_nk<R, 1, 1, 0, 0>(nk, grid, block, smem, s, k); break;
+    case 4: jk_dispatch_nk<R, 1, 1, 1, 0>(nk, grid, block, smem, s, k); break;
+    default: jk_dispatch_nk<R, 1, 1, 1, 1>(nk, grid, block, smem, s, k); break;
   }
 }
+
+// Shared memory per 128-thread block for the staged bra records, above
+// which a launch reads them from global memory instead (STO-6G pairs of 36
+// primitive pairs with 8-wide tasks would take 55 KB and cost resident
+// blocks).  Only the FP32 quartets stage: at C40H82 an all-FP32 build gains
+// 3.5% (2.44 -> 2.35 ms), an FP64 build loses 2% (4.03 -> 4.11 ms), the
+// FP64 kernels' bra records being L1 hits already.
+constexpr size_t JK_STAGE_MAX_BYTES = 16 * 1024;
 
 static int width_log2(int w) {
   if (w != 8 && w != 16 && w != 32) throw Error(PYFACC_ERR_INVALID, "task width must be 8, 16 or 32");
@@ -780,8 +858,13 @@ void launch_jk(const PairData& pd, const TaskList& tl, int bc, int kc, bool fp32
   int nblk = grid_for((int)std::min<long long>(warps * k.psplit, 1LL << 30), num_sms);
   nblk = (nblk + 1) / 2 * 2;
   dim3 grid(nblk), block(128);
-  if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, s, k);
-  else jk_dispatch<double>(k.qclass, nk, grid, block, s, k);
+  const size_t rec = fp32 ? sizeof(float4) : sizeof(double4);
+  const int tpw = 32 / tl.width;
+  const size_t smem = (size_t)4 * tpw * 3 * rec * pd.class_maxprim[bc];
+  k.stage = (fp32 && pd.class_maxprim[bc] > 0 && smem <= JK_STAGE_MAX_BYTES) ? pd.class_maxprim[bc] : 0;
+  const size_t dyn = k.stage ? smem : 0;
+  if (fp32) jk_dispatch<float>(k.qclass, nk, grid, block, dyn, s, k);
+  else jk_dispatch<double>(k.qclass, nk, grid, block, dyn, s, k);
   PF_CUDA(cudaGetLastError());
   count_launch();
 }
@@ -1171,7 +1254,8 @@ __global__ void eri_tensor_kernel(const JkKernelArgs args, int n, double* __rest
     const int bp = args.bra_base + ib, kp = args.ket_base + ket;
     const int4 bi0 = args.info0[bp], ki0 = args.info0[kp];
     double out[C::NOUT];
-    contracted_quartet<double, LA, LB, LC, LD>(args.prim, bi0, ki0, args.geom[bp], args.geom[kp], out);
+    contracted_quartet<double, LA, LB, LC, LD>(args.prim, args.prim + 3 * (size_t)bi0.z, bi0, ki0, args.geom[bp],
+                                               args.geom[kp], out);
     for (int a = 0; a < NA; ++a)
       for (int b = 0; b < NB; ++b)
         for (int c = 0; c < NCc; ++c)

@@ -114,7 +114,7 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   st.n_fock++;
 }
 
-void System::jk_counters(int nk, double out[6]) {
+void System::jk_counters(int nk, double out[6], double* per_class) {
   JkStats js;
   PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
   for (int k = 0; k < 6; ++k) out[k] = 0.0;
@@ -125,6 +125,10 @@ void System::jk_counters(int nk, double out[6]) {
                 (double)js.quartets[p][q] * (cf.hrr + digest_flops(q, nk));
       out[2 + p] += (double)js.quartets[p][q];
       out[4 + p] += (double)js.prims[p][q];
+      if (per_class) {
+        per_class[p * NQCLASS + q] = (double)js.quartets[p][q];
+        per_class[(2 + p) * NQCLASS + q] = (double)js.prims[p][q];
+      }
     }
 }
 

@@ -92,9 +92,13 @@ struct System {
   int syev_lwork = 0;
 
   ScfState st;
-  double last_jk[7] = {0, 0, 0, 0, 0, 0, 0};  // pyfacc_system_jk_stats
+  // pyfacc_system_jk_stats: ms, flops FP64/FP32, quartets FP64/FP32,
+  // primitive quartets FP64/FP32, then per s/p quartet class: quartets
+  // FP64, FP32, primitive quartets FP64, FP32 (NQCLASS each)
+  static constexpr int JK_STATS_N = 7 + 4 * NQCLASS;
+  double last_jk[JK_STATS_N] = {};
   // flops and counts of the J/K counters (stats_dev) for nk exchange densities
-  void jk_counters(int nk, double out[6]);
+  void jk_counters(int nk, double out[6], double* per_class = nullptr);
   pyfacc_reduce_fn reducer = nullptr;   // sums shard results across processes
   void* reducer_ctx = nullptr;
   void reduce(double* data, long long count);

@@ -311,10 +311,14 @@ class System:
     def jk_stats(self) -> dict:
         """Timing (CUDA events on the engine stream) and algorithmic flops of
         the last :meth:`jk` build, split by precision."""
-        buf = (ctypes.c_double * 7)()
-        N.check(lib().pyfacc_system_jk_stats(self.handle, buf, 7), "pyfacc_system_jk_stats")
+        buf = (ctypes.c_double * 31)()
+        N.check(lib().pyfacc_system_jk_stats(self.handle, buf, 31), "pyfacc_system_jk_stats")
         keys = ("ms", "flops_fp64", "flops_fp32", "quartets_fp64", "quartets_fp32", "prims_fp64", "prims_fp32")
-        return dict(zip(keys, list(buf)))
+        out = dict(zip(keys, list(buf)))
+        classes = ("ss|ss", "ps|ss", "ps|ps", "pp|ss", "pp|ps", "pp|pp")
+        for i, name in enumerate(("quartets_fp64", "quartets_fp32", "prims_fp64", "prims_fp32")):
+            out["by_class_" + name] = dict(zip(classes, list(buf)[7 + 6 * i:13 + 6 * i]))
+        return out
 
     def eri_tensor(self):
         eri = self._empty(self.nbf, self.nbf, self.nbf, self.nbf)

@@ -54,15 +54,25 @@ def test_d_eri_tensor_and_jk_vs_oracle(engine, oracle):
 
 @pytest.mark.parametrize("mol", [_zn_h2, _sc_h3])
 def test_d_rhf_energy_gradient_vs_oracle(engine, oracle, mol):
+    """Energy against the oracle's own SCF; gradient against the oracle's
+    derivative integrals at the engine's converged density (1e-7), and
+    against the oracle's own SCF gradient only to 1e-6: with Zn's core
+    exponents the gradient moves by ~7e-8 between a DIIS error of 1e-8 and
+    1e-11 in the oracle alone, so two independently converged SCFs differ
+    there by a few 1e-7."""
     sp, xyz = mol()
-    r = engine.run(engine.Molecule(sp, xyz), gradient=True, max_iter=300)
+    with engine.System(engine.Molecule(sp, xyz), max_iter=300) as s:
+        r = s.scf(matrices=True)
+        g = s.gradient()
+    P = r.matrices["P"]
     om = oracle.molecule(sp, xyz, basis_file())
     ro = oracle.scf(om, max_iter=300)
-    go = oracle.gradient(om, ro)
     assert r.converged and ro.converged
     assert r.energy == pytest.approx(ro.energy, abs=1e-8)
-    assert np.abs(r.gradient - go).max() < 1e-7
-    assert np.abs(r.gradient.sum(0)).max() < 1e-8
+    g_at = oracle.gradient_at_density(om, [0.5 * P, 0.5 * P], uhf=False)
+    assert np.abs(g - g_at).max() < 1e-7
+    assert np.abs(g - oracle.gradient(om, ro)).max() < 1e-6
+    assert np.abs(g.sum(0)).max() < 1e-8
 
 
 def _oracle_energy_at(oracle, om, Ds):
