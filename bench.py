@@ -66,8 +66,9 @@ WORKLOADS = {
 ORACLE_SCF_ITERS = {"c20h42": 22, "c10h22": 21, "c40h82": 24}
 # DRAM bytes per launch of the dominant J/K class kernel from one ncu capture
 # (profiles/jk_kernel_fp64_c40h82.md): the working set is L2-resident
-JK_TRAFFIC_BYTES = 2.06e6
-JK_TRAFFIC_NOTE = "dram read + write per launch of jk_kernel<double,1,0,0,0> (ncu, profiles/)"
+JK_TRAFFIC_BYTES = 4.73e6
+JK_TRAFFIC_NOTE = ("dram read + write per launch of jk_kernel<double,1,0,0,0> (the largest class) in a full FP64 "
+                   "C40H82 build (ncu, profiles/jk_kernel_fp64_c40h82.md)")
 
 
 def metric_name(wl):

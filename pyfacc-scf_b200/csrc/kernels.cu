@@ -233,12 +233,6 @@ template <int L> struct NC { static constexpr int v = (L + 1) * (L + 2) / 2; };
 // both loops stop at the first primitive quartet with |K_ab K_cd| < kcut.
 // With kq_step > 1 only the ket primitives kq0, kq0 + kq_step, ... are
 // summed (a share of the quartet; the shares add up to the integral).
-// With kPrefetchKet the ket primitive loop loads the next ket primitive's
-// records before the bra loop of the current one.  Measured at C40H82 it
-// costs more (registers: FP64 (ss|ss) 64 -> 80) than the hidden latency
-// returns (FP64 build 4.03 -> 4.40 ms), so it is off.
-constexpr bool kPrefetchKet = false;
-
 // brec: the bra pair's first primitive record (in global memory, or the
 // copy a warp staged in shared memory); prim: all records (the kets').
 template <typename R, int LA, int LB, int LC, int LD>
@@ -257,21 +251,9 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
   const R cut = (R)kcut;
   const R kab_max = fabs((R)brec[0].z);
   int nprim = 0;
-  const V* kr = prim + 3 * (size_t)ki0.z;
-  V k0 = {}, k1 = {}, k2 = {};
-  if (kq0 < ki0.w) {
-    k0 = kr[3 * kq0];
-    k1 = kr[3 * kq0 + 1];
-    k2 = kr[3 * kq0 + 2];
-  }
   for (int kq = kq0; kq < ki0.w; kq += kq_step) {
-    const int kn = kq + kq_step;
-    V n0 = k0, n1 = k1, n2 = k2;
-    if (kPrefetchKet && kn < ki0.w) {
-      n0 = kr[3 * kn];
-      n1 = kr[3 * kn + 1];
-      n2 = kr[3 * kn + 2];
-    }
+    const V* kr = prim + 3 * (size_t)(ki0.z + kq);
+    const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
     const R kcd = fabs((R)k0.z);
     if (kab_max * kcd < cut) break;
     const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
@@ -285,17 +267,6 @@ __device__ __forceinline__ int contracted_quartet(const typename Rec<R>::T* __re
       prim_setup<R, C::L>(b0, b1, k0, k1, g);
       C::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.nrp, g.o2q, g.nrq, g.o2pq, acc);
       ++nprim;
-    }
-    if (kn < ki0.w) {
-      if (kPrefetchKet) {
-        k0 = n0;
-        k1 = n1;
-        k2 = n2;
-      } else {
-        k0 = kr[3 * kn];
-        k1 = kr[3 * kn + 1];
-        k2 = kr[3 * kn + 2];
-      }
     }
   }
   const R AB[3] = {(R)bgeo.x, (R)bgeo.y, (R)bgeo.z};
@@ -351,21 +322,9 @@ __device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ 
   const float cut = (float)kcut;
   const float kab_max = fabsf(brec[0].z);
   int nprim = 0;
-  const float4* kr = prim + 3 * (size_t)ki0.z;
-  float4 k0 = {}, k1 = {}, k2 = {};
-  if (kq0 < ki0.w) {
-    k0 = kr[3 * kq0];
-    k1 = kr[3 * kq0 + 1];
-    k2 = kr[3 * kq0 + 2];
-  }
   for (int kq = kq0; kq < ki0.w; kq += kq_step) {
-    const int kn = kq + kq_step;
-    float4 n0 = k0, n1 = k1, n2 = k2;
-    if (kPrefetchKet && kn < ki0.w) {
-      n0 = kr[3 * kn];
-      n1 = kr[3 * kn + 1];
-      n2 = kr[3 * kn + 2];
-    }
+    const float4* kr = prim + 3 * (size_t)(ki0.z + kq);
+    const float4 k0 = kr[0], k1 = kr[1], k2 = kr[2];
     const float kcd = fabsf(k0.z);
     if (kab_max * kcd < cut) break;
     const F2 QC[3] = {F2(k2.x), F2(k2.y), F2(k2.z)};
@@ -393,17 +352,6 @@ __device__ __forceinline__ int contracted_quartet_f2(const float4* __restrict__ 
       C2::vrr(g.I, PA, g.WP, QC, g.WQ, g.o2p, g.nrp, g.o2q, g.nrq, g.o2pq, acc);
       nprim += two ? 2 : 1;
       if (!two) break;
-    }
-    if (kn < ki0.w) {
-      if (kPrefetchKet) {
-        k0 = n0;
-        k1 = n1;
-        k2 = n2;
-      } else {
-        k0 = kr[3 * kn];
-        k1 = kr[3 * kn + 1];
-        k2 = kr[3 * kn + 2];
-      }
     }
   }
   float accs[C1::NACC];
@@ -652,7 +600,9 @@ __global__ void __launch_bounds__(128) jk_kernel(const JkKernelArgs args) {
     // (one coalesced copy by the group's lanes) when the launch gave one
     using V = typename Rec<R>::T;
     const V* brec = records<R>(args) + 3 * (size_t)bi0.z;
-    if (args.stage > 0) {
+    // FP32 kernels only: the FP64 ones read their bra records from L1
+    // (staging measured 2% slower there, and its mere branch 2.5%)
+    if (sizeof(R) == 4 && args.stage > 0) {
       extern __shared__ __align__(16) unsigned char jk_stage_smem[];
       V* st = reinterpret_cast<V*>(jk_stage_smem) +
               ((size_t)(threadIdx.x >> 5) * tpw + (lane >> lw)) * 3 * (size_t)args.stage;
