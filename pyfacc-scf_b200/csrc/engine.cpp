@@ -589,8 +589,9 @@ void System::alloc_matrices() {
   small = m; m += 48;
   pstate = m; m += 48;  // purification graph state (24 doubles used)
   dmax = reinterpret_cast<float*>(m);
+  const size_t red_bytes = (size_t)RED_BLOCKS * std::max(nd, 3) * sizeof(double);
   small_buf.ensure(2 * nbf * sizeof(double) + 256 + sizeof(JkStats) + 256 + 64 * sizeof(double*) + 256 +
-                   3 * natoms * sizeof(double) + 256 + 256);
+                   3 * natoms * sizeof(double) + 256 + 256 + red_bytes + 256);
   {
     char* b = small_buf.as<char>();
     size_t o = 0;
@@ -600,6 +601,7 @@ void System::alloc_matrices() {
     stats_dev = reinterpret_cast<unsigned long long*>(take(sizeof(JkStats)));
     ptrs_dev = reinterpret_cast<const double**>(take(64 * sizeof(double*)));
     grad_dev = reinterpret_cast<double*>(take(3 * natoms * sizeof(double)));
+    red_part = reinterpret_cast<double*>(take(red_bytes));
   }
   int lwork = 0;
   PF_CUSOLVER(cusolverDnDsyevd_bufferSize(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W1, nbf,
@@ -615,6 +617,7 @@ void System::release_extra() {
   stats_dev = nullptr;
   ptrs_dev = nullptr;
   grad_dev = nullptr;
+  red_part = nullptr;
 }
 
 }  // namespace pyfacc

@@ -69,6 +69,12 @@ constexpr double GRAD_CUT_ALPHA = 100.0;
 // iterations (their error is discarded by the full build that ends them);
 // 1e-8 costs C100H202 an extra iteration
 constexpr double COARSE_SCREEN = 1e-9;
+// ... and how many times looser it may be while the DIIS error is still
+// far above coarse_err (it scales with err / coarse_err, capped here).
+// 100: C40H82 mixed step 30.0 -> 28.8 ms, C100H202 170 -> 162 ms at the
+// same iteration counts; 1000 costs C40H82 an iteration, 10000 C100H202
+// three.
+constexpr double COARSE_SCREEN_SPAN = 100.0;
 // the all-FP32 phase ends after this many builds even if the DIIS error
 // stays above coarse_err (an oscillating start must still reach the
 // mixed builds, on which alone the SCF may converge)
@@ -311,12 +317,17 @@ void launch_identity(int n, double* A, cudaStream_t s);                  // A = 
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
                  cudaStream_t s);                                          // F = H + J - kf K
-void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s);
+// Blocks of the DIIS / energy reductions (their partial sums are combined
+// in a fixed order: the results do not depend on scheduling).
+constexpr int RED_BLOCKS = 64;
+// part: scratch of RED_BLOCKS x max(m, 3) doubles
+void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, double* part,
+                     cudaStream_t s);
 // out = sum_k c[k] src[k] (m host-side pointers and coefficients, any m >= 1)
 void launch_lincomb(long long n, int m, const double* const* src, const double* c, double* out, cudaStream_t s);
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb,
                        const double* Fa, const double* Fb, const double* Ea, const double* Eb,
-                       const double* Pa_old, const double* Pb_old, double* out, cudaStream_t s);
+                       const double* Pa_old, const double* Pb_old, double* out, double* part, cudaStream_t s);
 void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
                  const double* C, float* dmax, cudaStream_t s);
 void launch_zero(void* p, size_t bytes, cudaStream_t s);

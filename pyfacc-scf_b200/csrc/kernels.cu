@@ -1656,15 +1656,38 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
   return v;
 }
 
-// out[j] = <x, ys[j]>, one block per j (deterministic order).
-__global__ void dot_many_kernel(long long n, const double* __restrict__ x, const double* const* ys, double* out) {
+// out[j] = <x, ys[j]>: RED_BLOCKS blocks per j write partial sums into
+// part[j * RED_BLOCKS + b]; sum_parts_kernel adds them in a fixed order, so
+// the result does not depend on scheduling.
+__global__ void dot_many_kernel(long long n, const double* __restrict__ x, const double* const* ys,
+                                double* __restrict__ part) {
   __shared__ double sh[32];
-  const double* y = ys[blockIdx.x];
+  const double* y = ys[blockIdx.y];
   double acc = 0.0;
-  for (long long i = threadIdx.x; i < n; i += blockDim.x) acc += x[i] * y[i];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    acc += x[i] * y[i];
   acc = block_sum(acc, sh);
-  if (threadIdx.x == 0) out[blockIdx.x] = acc;
+  if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = acc;
 }
+
+// out[j] = sum_b part[j * nb + b] (or the max for the rows flagged in
+// max_rows), one warp per row, lanes in a fixed order
+__global__ void sum_parts_kernel(const double* __restrict__ part, int rows, int nb, unsigned max_rows,
+                                 double* __restrict__ out) {
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int j = w; j < rows; j += blockDim.x >> 5) {
+    const bool mx = (max_rows >> j) & 1u;
+    double v = 0.0;
+    for (int b = l; b < nb; b += 32) v = mx ? fmax(v, part[j * nb + b]) : v + part[j * nb + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_xor_sync(0xffffffffu, v, o);
+      v = mx ? fmax(v, u) : v + u;
+    }
+    if (l == 0) out[j] = v;
+  }
+}
+
 struct LinCombArgs {
   const double* src[8];
   double c[8];
@@ -1697,24 +1720,28 @@ void launch_lincomb(long long n, int m, const double* const* src, const double* 
   }
 }
 
-void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, cudaStream_t s) {
+void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, double* part,
+                     cudaStream_t s) {
   if (m <= 0) return;
-  dot_many_kernel<<<m, 512, 0, s>>>(n, x, ys, out);
+  dot_many_kernel<<<dim3(RED_BLOCKS, m), 256, 0, s>>>(n, x, ys, part);
   PF_CUDA(cudaGetLastError());
-  count_launch();
+  sum_parts_kernel<<<1, 256, 0, s>>>(part, m, RED_BLOCKS, 0u, out);
+  PF_CUDA(cudaGetLastError());
+  count_launches(2);
 }
 
-// One block: out[0] = sum Pt H + sum Pa Fa + sum Pb Fb (x 1/2 applied by the
-// caller), out[1] = max |Ea|,|Eb|, out[2] = ||dP||_F^2.
+// out[0] = sum Pt H + sum Pa Fa + sum Pb Fb (x 1/2 applied by the caller),
+// out[1] = max |Ea|,|Eb|, out[2] = ||dP||_F^2: RED_BLOCKS blocks write
+// partials part[{0,1,2} * RED_BLOCKS + b], sum_parts_kernel combines them.
 __global__ void scf_reduce_kernel(long long n, int uhf, const double* __restrict__ H, const double* __restrict__ Pa,
                                   const double* __restrict__ Pb, const double* __restrict__ Fa,
                                   const double* __restrict__ Fb, const double* __restrict__ Ea,
                                   const double* __restrict__ Eb, const double* __restrict__ Pa_old,
-                                  const double* __restrict__ Pb_old, double* out) {
+                                  const double* __restrict__ Pb_old, double* __restrict__ part) {
   __shared__ double sh[32];
   double e = 0.0, dp = 0.0;
   double emx = 0.0;
-  for (long long i = threadIdx.x; i < n; i += blockDim.x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     if (uhf) {
       e += (Pa[i] + Pb[i]) * H[i] + Pa[i] * Fa[i] + Pb[i] * Fb[i];
       emx = fmax(emx, fmax(fabs(Ea[i]), fabs(Eb[i])));
@@ -1742,17 +1769,19 @@ __global__ void scf_reduce_kernel(long long n, int uhf, const double* __restrict
   if (threadIdx.x == 0) {
     double m = 0.0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmax(m, sh[k]);
-    out[0] = e;
-    out[1] = m;
-    out[2] = dp;
+    part[blockIdx.x] = e;
+    part[gridDim.x + blockIdx.x] = m;
+    part[2 * gridDim.x + blockIdx.x] = dp;
   }
 }
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb, const double* Fa,
                        const double* Fb, const double* Ea, const double* Eb, const double* Pa_old,
-                       const double* Pb_old, double* out, cudaStream_t s) {
-  scf_reduce_kernel<<<1, 1024, 0, s>>>(n, uhf, H, Pa, Pb, Fa, Fb, Ea, Eb, Pa_old, Pb_old, out);
+                       const double* Pb_old, double* out, double* part, cudaStream_t s) {
+  scf_reduce_kernel<<<RED_BLOCKS, 256, 0, s>>>(n, uhf, H, Pa, Pb, Fa, Fb, Ea, Eb, Pa_old, Pb_old, part);
   PF_CUDA(cudaGetLastError());
-  count_launch();
+  sum_parts_kernel<<<1, 96, 0, s>>>(part, 3, RED_BLOCKS, 2u, out);
+  PF_CUDA(cudaGetLastError());
+  count_launches(2);
 }
 
 

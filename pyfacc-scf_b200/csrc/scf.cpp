@@ -416,7 +416,8 @@ void System::run_scf() {
   bool coarse = mixed && opt.coarse_err > 0 && opt.shard_count <= 1;
   bool restart = false;
   const double t32_coarse = 1e300;
-  const double coarse_screen = std::max(COARSE_SCREEN, opt.schwarz_thresh);
+  const double coarse_base = std::max(COARSE_SCREEN, opt.schwarz_thresh);
+  double err_prev = -1.0;  // DIIS error of the previous iteration (none before the first)
   const double* Pspin[2] = {P[0], P[1]};
   for (int it = 1; it <= opt.max_iter; ++it) {
     st.n_iter = it;
@@ -424,6 +425,13 @@ void System::run_scf() {
     PF_CUDA(cudaEventRecord(a0, stream));
     const bool full = !incremental || it == 1 || restart || since_full + 1 >= std::max(opt.rebuild_every, 1);
     const bool coarse_build = coarse;
+    // the coarse threshold follows the DIIS error: COARSE_SCREEN once the
+    // error nears coarse_err, up to COARSE_SCREEN_SPAN times looser while
+    // it is far above (the first build, with no error yet, at the loosest)
+    const double span = (err_prev < 0 || opt.coarse_err <= 0)
+                            ? COARSE_SCREEN_SPAN
+                            : std::min(COARSE_SCREEN_SPAN, std::max(1.0, err_prev / opt.coarse_err));
+    const double coarse_screen = coarse_base * span;
     const double t32 = coarse_build ? t32_coarse : -1.0;
     const double full_thresh = coarse_build ? coarse_screen : -1.0;
     const double step_thresh = coarse_build ? std::max(coarse_screen, inc_thresh) : inc_thresh;
@@ -477,7 +485,7 @@ void System::run_scf() {
                    stream);
     }
     launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Err[0],
-                      uhf ? Err[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, stream);
+                      uhf ? Err[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, red_part, stream);
     // ---- DIIS bookkeeping: store F and the error vector, overlaps with the stored errors
     int slot = -1;
     if (ndiis > 0) {
@@ -487,7 +495,7 @@ void System::run_scf() {
         PF_CUDA(cudaMemcpyAsync(diis_F[slot] + s * n2, F[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         PF_CUDA(cudaMemcpyAsync(diis_E[slot] + s * n2, Err[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
       }
-      launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, stream);
+      launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, red_part, stream);
     }
     double red[8 + 64];
     PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -500,6 +508,7 @@ void System::run_scf() {
     ms_fock += ms_build;
     const double E = 0.5 * red[0];
     const double err = red[1];
+    err_prev = err;
     const double dD = std::sqrt(red[2]);
     const double dE = std::fabs(E - E_old);
     st.last_de = dE;
@@ -600,7 +609,7 @@ void System::run_scf() {
     for (int s = 0; s < nsp; ++s) launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
     PF_CUDA(cudaEventRecord(a1, stream));
     launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Err[0],
-                      uhf ? Err[1] : nullptr, nullptr, nullptr, small, stream);
+                      uhf ? Err[1] : nullptr, nullptr, nullptr, small, red_part, stream);
     double red[4];
     PF_CUDA(cudaMemcpyAsync(red, small, 4 * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
@@ -618,6 +627,9 @@ void System::run_scf() {
     std::fprintf(stderr, "pyfacc phases (ms): total %.3f  one-electron %.3f  orthogonaliser %.3f  Fock %.3f  "
                  "density %.3f  rest (DIIS, energy, guess) %.3f\n", st.ms_total, st.ms_1e, ms_orth, ms_fock, ms_diag,
                  st.ms_total - st.ms_1e - ms_orth - ms_fock - ms_diag);
+  if (opt.verbose)
+    std::fprintf(stderr, "pyfacc purification: %d TC2 steps in all, %d eigensolver fallbacks\n", purify_steps,
+                 purify_fallbacks);
   JkStats js;
   PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
   st.quartets[0] = st.quartets[1] = 0;

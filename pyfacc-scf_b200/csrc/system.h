@@ -70,6 +70,7 @@ struct System {
   double *P[2] = {nullptr, nullptr}, *Pbuilt[2] = {nullptr, nullptr}, *Pold[2] = {nullptr, nullptr};
   double *W1 = nullptr, *W2 = nullptr, *W3 = nullptr, *Err[2] = {nullptr, nullptr};
   double *Cm[2] = {nullptr, nullptr}, *Wm = nullptr, *small = nullptr;
+  double* red_part = nullptr;  // partial sums of the DIIS / energy reductions
   double *Pu[4] = {nullptr, nullptr, nullptr, nullptr};  // purification work matrices
   double* pstate = nullptr;                      // TC2 state, two buffers of 8 (device)
   bool orbitals_ready = false;
