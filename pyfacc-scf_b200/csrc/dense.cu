@@ -1,8 +1,8 @@
 // Dense FP64 work of the single-molecule SCF step on the FP64 tensor cores.
 //
 //  * dgemm_kernel: C = alpha op(A) op(B) + beta Y for row-major matrices,
-//    one block of four warps per 16 x 16 output tile (2 x 2 tiles of
-//    mma.sync m8n8k4 f64), the k range split four ways between the warps and
+//    one block of eight warps per 16 x 16 output tile (2 x 2 tiles of
+//    mma.sync m8n8k4 f64), the k range split eight ways between the warps and
 //    the partial tiles added through shared memory; operands read from
 //    L2/L1 (the matrices of one molecule are a few MB at most and stay
 //    resident), 16 loads per lane in flight; optionally only the
@@ -134,10 +134,11 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
 
 // One 16 x 16 tile per block of SPLITK warps: warp w sums its share of k
 // (the matrices here are at most a few hundred wide, so a warp alone would
-// spend the kernel waiting on one L2 round trip per 16 k; split four ways
-// the waits overlap), then warp 0 adds the other warps' partial tiles from
-// shared memory.  Returns true on warp 0, whose acc holds the tile.
-constexpr int SPLITK = 4;
+// spend the kernel waiting on one L2 round trip per 16 k; split eight ways
+// the waits overlap, and at n = 282 each warp has at most three k chunks),
+// then warp 0 adds the other warps' partial tiles from shared memory.
+// Returns true on warp 0, whose acc holds the tile.
+constexpr int SPLITK = 8;
 template <bool TA, bool TB, bool ASYMA>
 __device__ __forceinline__ bool block_tile(const GemmArgs& g, int i0, int j0, double (&acc)[2][2][2]) {
   __shared__ double part[SPLITK - 1][8][32];
@@ -279,6 +280,27 @@ struct Tc2StepArgs {
 // traces of Xin that the previous step accumulated.  Once Tr X - Tr X^2 <
 // 1e-9 at the right trace, two more steps run, then the iterate is copied.
 __global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArgs s) {
+  const int n = s.n;
+  const int nt = (n + 15) >> 4;
+  int ti = 0, tj = 0;
+  tile_of<true>(blockIdx.x, nt, nt, ti, tj);  // the grid is the upper-triangle tile count
+  const int i0 = ti << 4, j0 = tj << 4;
+  const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
+  // Every load that does not depend on the control words is issued first,
+  // so that one L2 round trip covers them all: this lane's entries of X for
+  // the update (warp 0), the control words, all three trace slots, and the
+  // product's operands (evaluated even after convergence, when the update
+  // discards it, rather than waiting for the done flag).
+  double xin[2][2][2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int c = 0; c < 2; ++c)
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = i0 + 8 * r + gr, col = j0 + 8 * c + 2 * tq + h;
+        xin[r][c][h] = (threadIdx.x < 32 && row < n && col < n) ? s.Xin[(size_t)row * n + col] : 0.0;
+      }
   const double* cin = s.st + ST_CTL + 8 * s.parity;
   double* cout = s.st + ST_CTL + 8 * (1 - s.parity);
   const double countdown0 = cin[0];
@@ -286,7 +308,14 @@ __global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArg
   const double steps = cin[2];
   const int k = (int)cin[3];
   const double failed0 = cin[4];
-  const double t1 = s.st[ST_ACC + 2 * (k % 3)], t2 = s.st[ST_ACC + 2 * (k % 3) + 1];
+  double tr[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) tr[q] = s.st[ST_ACC + q];
+  double acc[2][2][2];
+  const GemmArgs g{n, n, n, s.Xin, n, s.Xin, n, nullptr, n, 1.0, nullptr, n, 0.0};
+  const bool warp0 = block_tile<false, false, false>(g, i0, j0, acc);
+  const int k3 = k % 3;
+  const double t1 = tr[2 * k3], t2 = tr[2 * k3 + 1];
   double a = 0.0, b = 1.0;
   if (!(fabs(t2 - s.nocc) < fabs(2.0 * t1 - t2 - s.nocc))) {
     a = 2.0;
@@ -314,25 +343,11 @@ __global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArg
     s.st[ST_ACC + 2 * ((k + 2) % 3) + 1] = 0.0;
     if (s.set_cond) cudaGraphSetConditional(s.cond, (now_done || failed) ? 0u : 1u);
   }
-  const int n = s.n;
-  const int nt = (n + 15) >> 4;
-  int ti, tj;
-  if (!tile_of<true>(blockIdx.x, nt, nt, ti, tj)) return;
-  const int i0 = ti << 4, j0 = tj << 4;
-  double acc[2][2][2];
-  if (!was_done) {
-    GemmArgs g{n, n, n, s.Xin, n, s.Xin, n, nullptr, n, 1.0, nullptr, n, 0.0};
-    if (!block_tile<false, false, false>(g, i0, j0, acc)) return;
-  } else {
-    if (threadIdx.x >= 32) return;
+  if (!warp0) return;
+  if (was_done) {  // converged: the iterate is copied unchanged
     a = 1.0;
     b = 0.0;
-#pragma unroll
-    for (int r = 0; r < 2; ++r)
-#pragma unroll
-      for (int c = 0; c < 2; ++c) acc[r][c][0] = acc[r][c][1] = 0.0;
   }
-  const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
   double s1 = 0.0, s2 = 0.0;
 #pragma unroll
   for (int r = 0; r < 2; ++r)
@@ -343,9 +358,8 @@ __global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArg
         const int row = i0 + 8 * r + gr, col = j0 + 8 * c + 2 * tq + h;
         if (row >= n || col >= n) continue;
         if (ti == tj && row > col) continue;
-        const size_t q = (size_t)row * n + col;
-        const double v = a * s.Xin[q] + b * acc[r][c][h];
-        s.Xout[q] = v;
+        const double v = a * xin[r][c][h] + b * acc[r][c][h];
+        s.Xout[(size_t)row * n + col] = v;
         if (row != col) {
           s.Xout[(size_t)col * n + row] = v;
           s2 += 2.0 * v * v;

@@ -267,13 +267,16 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   launch_dgemm(n, n, n, false, X, n, false, W1, n, Fp, n, 1.0, nullptr, n, 0.0, true, false, stream);
   // the whole TC2 iteration is one graph launch (conditional WHILE loop on
   // the device); the host reads the outcome once
+  if (opt.verbose) PF_CUDA(cudaEventRecord(ctx.ev0, stream));
   PF_CUDA(cudaGraphLaunch(tc2_graph(nocc), stream));
+  if (opt.verbose) PF_CUDA(cudaEventRecord(ctx.ev1, stream));
   double ctl[8];
   PF_CUDA(cudaMemcpyAsync(ctl, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   const int steps = (int)ctl[2];
   count_launches(2 + steps + (steps & 1));
   purify_steps += steps;
+  if (opt.verbose) purify_ms += elapsed(ctx.ev0, ctx.ev1);
   if (ctl[1] == 0.0 || ctl[4] != 0.0) return false;
   // P = scale R^T Xp R
   launch_dgemm(n, n, n, false, Xa, n, false, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
@@ -372,6 +375,7 @@ void System::run_scf() {
   const float ms_orth = elapsed(a0, a1);
   orbitals_ready = false;
   purify_steps = purify_fallbacks = 0;
+  purify_ms = 0.0;
   if (opt.guess == PYFACC_GUESS_CORE) {
     // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144)
     for (int s = 0; s < nsp; ++s) density_step(H, nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
@@ -628,8 +632,8 @@ void System::run_scf() {
                  "density %.3f  rest (DIIS, energy, guess) %.3f\n", st.ms_total, st.ms_1e, ms_orth, ms_fock, ms_diag,
                  st.ms_total - st.ms_1e - ms_orth - ms_fock - ms_diag);
   if (opt.verbose)
-    std::fprintf(stderr, "pyfacc purification: %d TC2 steps in all, %d eigensolver fallbacks\n", purify_steps,
-                 purify_fallbacks);
+    std::fprintf(stderr, "pyfacc purification: %d TC2 steps in all, %.3f ms in the TC2 graphs, %d eigensolver "
+                 "fallbacks\n", purify_steps, purify_ms, purify_fallbacks);
   JkStats js;
   PF_CUDA(cudaMemcpy(&js, stats_dev, sizeof(JkStats), cudaMemcpyDeviceToHost));
   st.quartets[0] = st.quartets[1] = 0;

@@ -76,6 +76,7 @@ struct System {
   bool orbitals_ready = false;
   int task_width = TASK_WIDTH;  // kets per J/K task
   int purify_steps = 0, purify_fallbacks = 0;
+  double purify_ms = 0.0;  // CUDA-event time of the TC2 graphs (verbose runs only)
   float* dmax = nullptr;
   std::vector<double*> diis_F, diis_E;
   double* eps_dev = nullptr;
