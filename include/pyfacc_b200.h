@@ -143,8 +143,27 @@ void run_scf_interface_py(int32_t *natoms, int32_t *nelectrons, int32_t *charge,
                           int32_t *max_iter, double *final_energy, const char *basis_set_c,
                           int32_t *len_basis_set, int32_t *z_num);
 
-/* Status of the last run_scf_c / run_scf_interface_py call on this thread
- * (the originals return nothing; la.f90:22-25 only prints). */
+/* One-body integrals of one shell pair: src/cpp/libint_wrapper.cpp:16-105
+ * (libint_overlap_c), :114-212 (libint_kinetic_c), :220-327
+ * (libint_potential_c), same symbols and arguments.  am*: angular momentum
+ * (0..2 here); contrdepth*: primitives (1..32); A, B (and C): bohr;
+ * alpha*, c*: exponents and contraction coefficients, applied as given to
+ * unnormalised Cartesian primitives x^i y^j z^k exp(-alpha r^2) (no
+ * normalisation is added); the result is the nint(amA) x nint(amB) block,
+ * row-major, components in x-descending-then-y order; the potential is that
+ * of a unit positive charge at C, int phi_a phi_b / |r - C|.  Computed on
+ * the current CUDA device, synchronously on the legacy default stream.
+ * void like the originals: on failure the block is NaN and the status is
+ * kept for pyfacc_last_status(). */
+void libint_overlap_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB,
+                      int contrdepthB, double B[], double alphaB[], double cB[], double overlapAB[]);
+void libint_kinetic_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB,
+                      int contrdepthB, double B[], double alphaB[], double cB[], double kineticAB[]);
+void libint_potential_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB,
+                        int contrdepthB, double B[], double alphaB[], double cB[], double C[], double potAB[]);
+
+/* Status of the last run_scf_c / run_scf_interface_py / libint_*_c call on
+ * this thread (the originals return nothing; la.f90:22-25 only prints). */
 int pyfacc_last_status(void);
 const char *pyfacc_status_string(int status);
 /* Text of the most recent failure on this thread (extension). */

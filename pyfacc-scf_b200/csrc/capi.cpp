@@ -112,6 +112,42 @@ void pyfacc_default_options(pyfacc_options* o) {
 // The Fortran side stops at max_iter and returns the last energy (rscf.f90:
 // 118-164); this engine does the same with DIIS, converging on |dE| < eps_scf
 // and ||D - D_old||_F < eps_scf as rscf.f90:152-155 does.
+// libint_overlap_c / libint_kinetic_c / libint_potential_c: the one-body
+// shell-pair interface of the reference's Libint wrapper
+// (src/cpp/libint_wrapper.cpp:16-105, 114-212, 220-327), same symbols and
+// arguments, computed on the GPU.  Like the wrapper they return nothing; a
+// failure (an l above 2, a contraction deeper than 32, no device) fills the
+// block with NaN and leaves the status for pyfacc_last_status().
+namespace {
+void libint_block(int kind, int amA, int nA, const double* A, const double* alphaA, const double* cA, int amB,
+                  int nB, const double* B, const double* alphaB, const double* cB, const double* C, double* out) {
+  const int st = guarded([&] {
+    pyfacc::libint_one_body(kind, amA, nA, A, alphaA, cA, amB, nB, B, alphaB, cB, C, out);
+  });
+  g_last_status = st;
+  // the caller sized out as nint(amA) x nint(amB) (any l, as for Libint)
+  if (st != PYFACC_OK && out && amA >= 0 && amB >= 0 && amA <= 20 && amB <= 20) {
+    const int n = ((amA + 1) * (amA + 2) / 2) * ((amB + 1) * (amB + 2) / 2);
+    for (int i = 0; i < n; ++i) out[i] = std::numeric_limits<double>::quiet_NaN();
+  }
+}
+}  // namespace
+
+void libint_overlap_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB, int contrdepthB,
+                      double B[], double alphaB[], double cB[], double overlapAB[]) {
+  libint_block(0, amA, contrdepthA, A, alphaA, cA, amB, contrdepthB, B, alphaB, cB, nullptr, overlapAB);
+}
+
+void libint_kinetic_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB, int contrdepthB,
+                      double B[], double alphaB[], double cB[], double kineticAB[]) {
+  libint_block(1, amA, contrdepthA, A, alphaA, cA, amB, contrdepthB, B, alphaB, cB, nullptr, kineticAB);
+}
+
+void libint_potential_c(int amA, int contrdepthA, double A[], double alphaA[], double cA[], int amB, int contrdepthB,
+                        double B[], double alphaB[], double cB[], double C[], double potAB[]) {
+  libint_block(2, amA, contrdepthA, A, alphaA, cA, amB, contrdepthB, B, alphaB, cB, C, potAB);
+}
+
 void run_scf_c(int natoms, int nelectrons, int charge, int nalpha, int nbeta, const char* species, double* coords,
                double eps_scf, int max_iter, double* final_energy, const char* basis_set_c, int32_t* z_num) {
   (void)nelectrons;

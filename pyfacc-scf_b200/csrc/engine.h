@@ -90,6 +90,8 @@ constexpr double ONE_E_PAIR_CUT = 1e-25;
 // which it counts as linearly dependent (PYFACC_ERR_LINDEP)
 constexpr double LINDEP_PIVOT = 1e-10;
 constexpr int TASK_WIDTH = 32;   // default kets per task = lanes per warp
+// largest contraction depth of a shell in the libint_*_c one-body entry points
+constexpr int LIBINT1E_MAX_PRIM = 32;
 
 // ---------------------------------------------------------------- host basis
 struct Shell {
@@ -295,6 +297,12 @@ struct OneEArgs {
   int nbf;
 };
 // pairs[c]: the shell pairs (a, b) of class c = l_a + l_b with l_a >= l_b.
+// One shell pair's overlap (kind 0), kinetic (1) or unit-charge potential
+// at C (2) integrals with the caller's coefficients on unnormalised
+// primitives, into out (host, nint(la) x nint(lb) row-major); synchronous,
+// on the current device's legacy default stream (kernels.cu).
+void libint_one_body(int kind, int la, int na, const double* A, const double* ea, const double* ca, int lb, int nb,
+                     const double* B, const double* eb, const double* cb, const double* C, double* out);
 void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const* pairs, const OneEArgs& a,
                          cudaStream_t s);
 

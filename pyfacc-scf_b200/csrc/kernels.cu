@@ -1317,8 +1317,9 @@ struct Prim1e {
   double P[3], PA[3], PB[3];
 };
 
+// normalize = false: the coefficients multiply unnormalised primitives
 __device__ __forceinline__ void prim1e_setup(double al, double ca, int la, double be, double cb, int lb,
-                                             const double4& A, const double4& B, Prim1e& g) {
+                                             const double4& A, const double4& B, Prim1e& g, bool normalize = true) {
   g.al = al; g.be = be; g.p = al + be; g.o2p = 0.5 / g.p;
   const double A3[3] = {A.x, A.y, A.z}, B3[3] = {B.x, B.y, B.z};
   double ab2 = 0.0;
@@ -1329,7 +1330,7 @@ __device__ __forceinline__ void prim1e_setup(double al, double ca, int la, doubl
     g.PB[x] = g.P[x] - B3[x];
     ab2 += (A3[x] - B3[x]) * (A3[x] - B3[x]);
   }
-  g.w = ca * cb * prim_norm(la, al) * prim_norm(lb, be) * exp(-al * be / g.p * ab2);
+  g.w = ca * cb * (normalize ? prim_norm(la, al) * prim_norm(lb, be) : 1.0) * exp(-al * be / g.p * ab2);
 }
 
 // 1-D overlap tables of one primitive pair: (pi/p)^{3/2} w carried by z.
@@ -1441,6 +1442,123 @@ void launch_one_electron(const ShellDev& sh, const int* npair, const int2* const
     PF_CUDA(cudaGetLastError());
     count_launch();
   }
+}
+
+// ---------------------------------------------------------------------------
+// One-body integrals of a single shell pair with caller-given contraction
+// coefficients, for the libint_*_c entry points (the reference's unused
+// Libint one-body wrapper, src/cpp/libint_wrapper.cpp:16-327): the
+// coefficients multiply unnormalised Cartesian primitives x^i y^j z^k
+// exp(-a r^2) as given, and the potential is that of a unit positive
+// charge at C, int phi_a phi_b / |r - C| (Libint's elecpot sign).  One warp;
+// its lanes take the primitive pairs.  la >= lb; a transposed request
+// writes out[ib * NA + ia].
+// ---------------------------------------------------------------------------
+struct Libint1eArgs {
+  int kind;  // 0 overlap, 1 kinetic, 2 potential
+  int na, nb, transpose;
+  double A[3], B[3], C[3];
+  double ea[LIBINT1E_MAX_PRIM], ca[LIBINT1E_MAX_PRIM], eb[LIBINT1E_MAX_PRIM], cb[LIBINT1E_MAX_PRIM];
+};
+
+static __device__ double g_libint1e_out[36];  // up to 6 x 6 components (d|d)
+
+template <int LA, int LB>
+__global__ void __launch_bounds__(32) libint_1e_kernel(const Libint1eArgs a) {
+  using NCl = NucClass<double, LA, LB>;
+  constexpr int NA = NC<LA>::v, NB = NC<LB>::v;
+  const int lane = threadIdx.x & 31;
+  const double4 A = make_double4(a.A[0], a.A[1], a.A[2], 0.0), B = make_double4(a.B[0], a.B[1], a.B[2], 0.0);
+  const double AB[3] = {A.x - B.x, A.y - B.y, A.z - B.z};
+  double acc[NA * NB];
+#pragma unroll
+  for (int i = 0; i < NA * NB; ++i) acc[i] = 0.0;
+  for (int pp = lane; pp < a.na * a.nb; pp += 32) {
+    const int ka = pp / a.nb, kb = pp % a.nb;
+    Prim1e g;
+    prim1e_setup(a.ea[ka], a.ca[ka], LA, a.eb[kb], a.cb[kb], LB, A, B, g, false);
+    if (a.kind < 2) {
+      double S[3][LA + 2][LB + 2];
+      st_tables<LA + 2, LB + 2>(g, S);
+#pragma unroll
+      for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+        for (int ib = 0; ib < NB; ++ib) {
+          int c1[3], c2[3];
+          cart_comp(LA, ia, c1);
+          cart_comp(LB, ib, c2);
+          acc[ia * NB + ib] += a.kind == 0 ? ovl3(S, c1, c2) : kin3(S, c1, c2, g.al, g.be);
+        }
+    } else {
+      const double PC[3] = {g.P[0] - a.C[0], g.P[1] - a.C[1], g.P[2] - a.C[2]};
+      double F[PF_BOYS_MMAX + 1];
+      boys_runtime(0, LA + LB, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
+      const double pref = g.w * 6.2831853071795864769 / g.p;
+      double I[LA + LB + 1];
+#pragma unroll
+      for (int m = 0; m <= LA + LB; ++m) I[m] = pref * F[m];
+      NCl::vint(I, g.PA, PC, g.o2p, AB, acc);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NA * NB; ++i) acc[i] = warp_sum(acc[i]);
+  if (lane == 0)
+#pragma unroll
+    for (int ia = 0; ia < NA; ++ia)
+#pragma unroll
+      for (int ib = 0; ib < NB; ++ib)
+        g_libint1e_out[a.transpose ? ib * NA + ia : ia * NB + ib] = acc[ia * NB + ib];
+}
+
+void libint_one_body(int kind, int la, int na, const double* A, const double* ea, const double* ca, int lb, int nb,
+                     const double* B, const double* eb, const double* cb, const double* C, double* out) {
+  if (kind < 0 || kind > 2) throw Error(PYFACC_ERR_INVALID, "unknown one-body integral kind");
+  if (la < 0 || lb < 0 || la > 2 || lb > 2)
+    throw Error(PYFACC_ERR_UNSUPPORTED_L, "one-body shell pairs up to d (l <= 2)");
+  if (na <= 0 || nb <= 0 || na > LIBINT1E_MAX_PRIM || nb > LIBINT1E_MAX_PRIM)
+    throw Error(PYFACC_ERR_INVALID, "contraction depth must be 1.." + std::to_string(LIBINT1E_MAX_PRIM));
+  if (!A || !B || !ea || !ca || !eb || !cb || !out || (kind == 2 && !C))
+    throw Error(PYFACC_ERR_INVALID, "null argument");
+  int device = 0;
+  PF_CUDA(cudaGetDevice(&device));
+  ensure_boys_tables(device);
+  // the kernel's class has l_a >= l_b; a (lower | higher) request is the
+  // transposed (higher | lower) one
+  const bool swap = la < lb;
+  Libint1eArgs a{};
+  a.kind = kind;
+  a.transpose = swap ? 1 : 0;
+  a.na = swap ? nb : na;
+  a.nb = swap ? na : nb;
+  for (int x = 0; x < 3; ++x) {
+    a.A[x] = swap ? B[x] : A[x];
+    a.B[x] = swap ? A[x] : B[x];
+    a.C[x] = kind == 2 ? C[x] : 0.0;
+  }
+  for (int k = 0; k < a.na; ++k) {
+    a.ea[k] = swap ? eb[k] : ea[k];
+    a.ca[k] = swap ? cb[k] : ca[k];
+  }
+  for (int k = 0; k < a.nb; ++k) {
+    a.eb[k] = swap ? ea[k] : eb[k];
+    a.cb[k] = swap ? ca[k] : cb[k];
+  }
+  const int L1 = swap ? lb : la, L2 = swap ? la : lb;
+  // calls share the 36-double result array on the device: one at a time
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  switch (L1 * 3 + L2) {
+    case 0: libint_1e_kernel<0, 0><<<1, 32>>>(a); break;
+    case 3: libint_1e_kernel<1, 0><<<1, 32>>>(a); break;
+    case 4: libint_1e_kernel<1, 1><<<1, 32>>>(a); break;
+    case 6: libint_1e_kernel<2, 0><<<1, 32>>>(a); break;
+    case 7: libint_1e_kernel<2, 1><<<1, 32>>>(a); break;
+    default: libint_1e_kernel<2, 2><<<1, 32>>>(a); break;
+  }
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+  const int n = ((la + 1) * (la + 2) / 2) * ((lb + 1) * (lb + 2) / 2);
+  PF_CUDA(cudaMemcpyFromSymbol(out, g_libint1e_out, n * sizeof(double)));
 }
 
 // Gradient of the one-electron energy: sum P (dT + dV) - sum W dS over the

@@ -82,6 +82,12 @@ SIGNATURES = {
                          c_char_p, P_int32]),
     "run_scf_interface_py": (None, [P_int32, P_int32, P_int32, P_int32, P_int32, c_void_p, P_double, P_double,
                                     P_int32, P_double, c_char_p, P_int32, P_int32]),
+    "libint_overlap_c": (None, [c_int, c_int, P_double, P_double, P_double, c_int, c_int, P_double, P_double,
+                                P_double, P_double]),
+    "libint_kinetic_c": (None, [c_int, c_int, P_double, P_double, P_double, c_int, c_int, P_double, P_double,
+                                P_double, P_double]),
+    "libint_potential_c": (None, [c_int, c_int, P_double, P_double, P_double, c_int, c_int, P_double, P_double,
+                                  P_double, P_double, P_double]),
     "pyfacc_last_status": (c_int, []),
     "pyfacc_status_string": (c_char_p, [c_int]),
     "pyfacc_last_message": (c_char_p, []),
