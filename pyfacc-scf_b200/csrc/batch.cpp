@@ -1061,7 +1061,8 @@ void Batch::gradient_run() {
   for (auto& e : ev) cudaEventDestroy(e);
   timing.flops_grad = 0.0;
   for (int q = 0; q < NQCLASS; ++q)
-    timing.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false));
+    timing.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false)) +
+                       (double)cnt[q] * class_flops(q).gfin;
   // nuclear repulsion (molecule.f90:31-52 differentiated)
   for (const auto& M : mols)
     for (int i = 0; i < M.natoms; ++i)

@@ -178,7 +178,11 @@ struct JkStats {
 };
 
 // Algorithmic flop counts of the generated class routines (eri_classes.cuh).
-struct ClassFlops { int L, nout, vrr, hrr, grad; };
+// Generated operation counts of a class: J/K VRR per primitive quartet and
+// HRR per contracted quartet; gradient per primitive quartet (grad) and per
+// contracted quartet (gfin: the HRR after the primitive sum, 0 for the
+// classes that contract per primitive).
+struct ClassFlops { int L, nout, vrr, hrr, grad, gfin; };
 const ClassFlops& class_flops(int qclass);
 // Flops charged per primitive quartet outside the VRR (prefactors + Boys)
 // and per contracted quartet for the J/K digestion.

@@ -349,11 +349,115 @@ def gen_class(la, lb, lc, ld):
         for x in range(3):
             src.append(f"    g[{x}] += grad{c}{'xyz'[x]}(I, PA, WP, QC, WQ, o2p, nrp, o2q, nrq, o2pq, AB, CD, tw, gam);")
         src.append("  }")
+    gsrc, ginfo = gen_contracted_grad(la, lb, lc, ld)
+    src.extend(gsrc)
     src.append(f"  static constexpr int VRR_FLOPS = {vrr_flops};")
     src.append(f"  static constexpr int HRR_FLOPS = {hrr_flops};")
     src.append(f"  static constexpr int GRAD_FLOPS = {grad_flops};")
     src.append("};")
-    return "\n".join(src), dict(tag=tag, L=L, nacc=nacc, nout=nout, vrr=vrr_flops, hrr=hrr_flops, grad=grad_flops)
+    return "\n".join(src), dict(tag=tag, L=L, nacc=nacc, nout=nout, vrr=vrr_flops, hrr=hrr_flops, grad=grad_flops,
+                                **ginfo)
+
+
+# Classes whose gradient is contracted before the HRR (gen_contracted_grad):
+# their exponent-weighted accumulators fit the register file (10, 25, 69 and
+# 66 of them); (pp|ps) and (pp|pp) would need 240 and 585.
+GCON_CLASSES = {(0, 0, 0, 0), (1, 0, 0, 0), (1, 0, 1, 0), (1, 1, 0, 0)}
+
+
+def gen_contracted_grad(la, lb, lc, ld):
+    """Nuclear-gradient contraction with the HRR after the primitive sum.
+
+    d/dA_x phi_a = 2 alpha phi_{a+1x} - a_x phi_{a-1x}, and the HRR that
+    turns [e0|f0] into (ab|cd) has primitive-independent coefficients (AB,
+    CD), so sum_prim 2 alpha (a+1x b|cd)_prim is the HRR of the contracted
+    accumulators U_A[e, f] = sum_prim 2 alpha [e0|f0]_prim (likewise U_B with
+    2 beta, U_C with 2 gamma, and the plain sum V for the a_x (a-1x b|cd)
+    terms).  ``gacc`` adds one primitive quartet into these accumulators
+    (VRR to L + 1 and one multiply-add per accumulator); ``gfin`` runs the
+    HRR on them once per contracted quartet and contracts with gam, giving
+    the same g[0..8] as the per-primitive routines gradA/B/C summed over the
+    primitives."""
+    if (la, lb, lc, ld) not in GCON_CLASSES:
+        return ["  static constexpr bool GCON = false;", "  static constexpr int NGACC = 1;",
+                "  static constexpr int GACC_FLOPS = 0;", "  static constexpr int GFIN_FLOPS = 0;"], \
+            dict(ngacc=0, gacc=0, gfin=0)
+    L = la + lb + lc + ld
+    idx, order = {}, []
+
+    def base(kind):
+        def f(e, ff):
+            key = (kind, e, ff)
+            if key not in idx:
+                idx[key] = len(order)
+                order.append(key)
+            return f"acc[{idx[key]}]"
+        return f
+
+    em = Emitter()
+    hs = [Hrr(em, base(k), packed=False) for k in range(4)]  # U_A, U_B, U_C, V
+    out = []
+    for ctr in range(3):
+        for x in range(3):
+            up_terms, dn_terms = [], []
+            k = 0
+            for a in comps(la):
+                for b in comps(lb):
+                    for c in comps(lc):
+                        for d in comps(ld):
+                            q = [a, b, c, d]
+                            qu = list(q)
+                            qu[ctr] = up(q[ctr], x)
+                            up_terms.append((f"gam[{k}]", hs[ctr].full(*qu)))
+                            cnt = q[ctr][x]
+                            if cnt > 0:
+                                qd = list(q)
+                                qd[ctr] = down(q[ctr], x)
+                                dn_terms.append((scaled(cnt, f"gam[{k}]"), hs[3].full(*qd)))
+                            k += 1
+            expr = em.tmp(plain_sum(up_terms), 2 * len(up_terms) - 1)
+            if dn_terms:
+                sd = em.tmp(plain_sum(dn_terms), 2 * len(dn_terms) - 1)
+                expr = f"{expr} - {sd}"
+                em.flops += 1
+            out.append(f"    g[{3 * ctr + x}] += {expr};")
+            em.flops += 1
+    fin_lines, fin_flops = em.lines, em.flops
+    em = Emitter()
+    v = Vrr(em, L + 1, packed=False)
+    weight = ["ta", "tb", "tc", None]
+    acc_lines = []
+    for key in order:
+        kind, e, ff = key
+        val = v.V(e, ff, 0)
+        if weight[kind]:
+            acc_lines.append(f"    acc[{idx[key]}] += {weight[kind]} * {val};")
+            em.flops += 2
+        else:
+            acc_lines.append(f"    acc[{idx[key]}] += {val};")
+            em.flops += 1
+    src = ["  static constexpr bool GCON = true;",
+           f"  static constexpr int NGACC = {len(order)};",
+           "  // one primitive quartet into the exponent-weighted accumulators",
+           "  // (ta, tb, tc = 2 alpha, 2 beta, 2 gamma of the primitive)",
+           "  __device__ static __forceinline__ void gacc(const R* __restrict__ I, const R* __restrict__ PA,",
+           "      const R* __restrict__ WP, const R* __restrict__ QC, const R* __restrict__ WQ, R o2p, R nrp,",
+           "      R o2q, R nrq, R o2pq, R ta, R tb, R tc, R* __restrict__ acc) {"]
+    src.extend(em.lines)
+    src.extend(acc_lines)
+    src.append("    (void)PA; (void)WP; (void)QC; (void)WQ; (void)o2p; (void)nrp; (void)o2q; (void)nrq; (void)o2pq;")
+    src.append("    (void)ta; (void)tb; (void)tc;")
+    src.append("  }")
+    src.append("  // the contracted accumulators through the HRR, contracted with gam: g[0..8] += d/dA, d/dB, d/dC")
+    src.append("  __device__ static __forceinline__ void gfin(const R* __restrict__ acc, const R* __restrict__ AB,")
+    src.append("      const R* __restrict__ CD, const R* __restrict__ gam, R* __restrict__ g) {")
+    src.extend(fin_lines)
+    src.extend(out)
+    src.append("    (void)AB; (void)CD;")
+    src.append("  }")
+    src.append(f"  static constexpr int GACC_FLOPS = {em.flops};")
+    src.append(f"  static constexpr int GFIN_FLOPS = {fin_flops};")
+    return src, dict(ngacc=len(order), gacc=em.flops, gfin=fin_flops)
 
 
 class Vrr1e:
@@ -496,9 +600,11 @@ def generate() -> str:
     for cl in ONE_E_CLASSES:
         parts.append(gen_one_electron(*cl))
         parts.append("")
-    parts.append("// class | L | accumulators | outputs | vrr flops/prim | hrr flops/contr | grad flops/prim")
+    parts.append("// class | L | accumulators | outputs | vrr flops/prim | hrr flops/contr | grad flops/prim"
+                 " | contracted-gradient accumulators | flops/prim | flops/contr")
     for t in table:
-        parts.append(f"//  {t['tag']}  | {t['L']} | {t['nacc']:3d} | {t['nout']:3d} | {t['vrr']:5d} | {t['hrr']:4d} | {t['grad']:6d}")
+        parts.append(f"//  {t['tag']}  | {t['L']} | {t['nacc']:3d} | {t['nout']:3d} | {t['vrr']:5d} | {t['hrr']:4d} | {t['grad']:6d}"
+                     f" | {t['ngacc']:3d} | {t['gacc']:4d} | {t['gfin']:5d}")
     return "\n".join(parts) + "\n"
 
 

@@ -1030,64 +1030,102 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       const size_t mo = (size_t)bi2.x;
       const int ld = bi2.y;
       const int ma = bi0.x, mb = bi0.y, mc = ki0.x, md = ki0.y;
-      // the (pp|pp) derivative routines are compiled out of line and read
-      // the density products through a pointer: for that class they live
-      // in shared memory (after the per-atom sums) rather than in local
-      // memory, which spilled to DRAM
-      R gam_reg[kGamSmem ? 1 : C::NOUT];
-      R* gam = kGamSmem ? reinterpret_cast<R*>(gsh + nsm) + (size_t)threadIdx.x * C::NOUT : gam_reg;
+      // the density products Gamma_abcd of the quartet
+      auto fill_gam = [&](R* gam) {
 #pragma unroll
-      for (int a = 0; a < NA; ++a)
+        for (int a = 0; a < NA; ++a)
 #pragma unroll
-        for (int b = 0; b < NB; ++b)
+          for (int b = 0; b < NB; ++b)
 #pragma unroll
-          for (int c = 0; c < NCc; ++c)
+            for (int c = 0; c < NCc; ++c)
 #pragma unroll
-            for (int d = 0; d < ND; ++d) {
-              const size_t mu = ma + a, nu = mb + b, la = mc + c, si = md + d;
-              const double* Pt = A.Pt + mo;
-              double v = __ldg(Pt + mu * ld + nu) * __ldg(Pt + la * ld + si);
-              if (A.uhf) {
-                const double* Pa = A.Pa + mo;
-                const double* Pb = A.Pb + mo;
-                v -= 0.5 * (__ldg(Pa + mu * ld + la) * __ldg(Pa + nu * ld + si) +
-                            __ldg(Pa + mu * ld + si) * __ldg(Pa + nu * ld + la));
-                v -= 0.5 * (__ldg(Pb + mu * ld + la) * __ldg(Pb + nu * ld + si) +
-                            __ldg(Pb + mu * ld + si) * __ldg(Pb + nu * ld + la));
-              } else {
-                v -= 0.25 * (__ldg(Pt + mu * ld + la) * __ldg(Pt + nu * ld + si) +
-                             __ldg(Pt + mu * ld + si) * __ldg(Pt + nu * ld + la));
+              for (int d = 0; d < ND; ++d) {
+                const size_t mu = ma + a, nu = mb + b, la = mc + c, si = md + d;
+                const double* Pt = A.Pt + mo;
+                double v = __ldg(Pt + mu * ld + nu) * __ldg(Pt + la * ld + si);
+                if (A.uhf) {
+                  const double* Pa = A.Pa + mo;
+                  const double* Pb = A.Pb + mo;
+                  v -= 0.5 * (__ldg(Pa + mu * ld + la) * __ldg(Pa + nu * ld + si) +
+                              __ldg(Pa + mu * ld + si) * __ldg(Pa + nu * ld + la));
+                  v -= 0.5 * (__ldg(Pb + mu * ld + la) * __ldg(Pb + nu * ld + si) +
+                              __ldg(Pb + mu * ld + si) * __ldg(Pb + nu * ld + la));
+                } else {
+                  v -= 0.25 * (__ldg(Pt + mu * ld + la) * __ldg(Pt + nu * ld + si) +
+                               __ldg(Pt + mu * ld + si) * __ldg(Pt + nu * ld + la));
+                }
+                gam[((a * NB + b) * NCc + c) * ND + d] = (R)v;
               }
-              gam[((a * NB + b) * NCc + c) * ND + d] = (R)v;
-            }
+      };
       const R AB[3] = {(R)bg.x, (R)bg.y, (R)bg.z};
       const R CD[3] = {(R)kg.x, (R)kg.y, (R)kg.z};
       R gr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       const V* prim = grecords<R>(args);
       const R cut = (R)kcut;
       const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
+      if constexpr (C::GCON) {
+        // exponent-weighted sums over the primitive quartets, then one HRR
+        // and one contraction with Gamma per contracted quartet
+        R acc[C::NGACC];
+#pragma unroll
+        for (int i = 0; i < C::NGACC; ++i) acc[i] = (R)0;
 #pragma unroll 1
-      for (int kq = slice; kq < ki0.w; kq += ps) {
-        const V* kr = prim + 3 * (size_t)(ki0.z + kq);
-        const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
-        const R kcd = fabs((R)k0.z);
-        if (kab_max * kcd < cut) break;
-        const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+        for (int kq = slice; kq < ki0.w; kq += ps) {
+          const V* kr = prim + 3 * (size_t)(ki0.z + kq);
+          const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+          const R kcd = fabs((R)k0.z);
+          if (kab_max * kcd < cut) break;
+          const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+          const R tc = (R)(2 * k0.w);
 #pragma unroll 1
-        for (int kpp = 0; kpp < bi0.w; ++kpp) {
-          const V* br = prim + 3 * (size_t)(bi0.z + kpp);
-          const V b0 = br[0], b1 = br[1], b2 = br[2];
-          if (fabs((R)b0.z) * kcd < cut) break;
-          ++nprim;
-          const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
-          PrimGeo<R> pg;
-          prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
-          C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * b0.w), gam,
-                   gr);
-          C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD,
-                   (R)(2 * (b0.x - b0.w)), gam, gr + 3);
-          C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * k0.w), gam,
-                   gr + 6);
+          for (int kpp = 0; kpp < bi0.w; ++kpp) {
+            const V* br = prim + 3 * (size_t)(bi0.z + kpp);
+            const V b0 = br[0], b1 = br[1], b2 = br[2];
+            if (fabs((R)b0.z) * kcd < cut) break;
+            ++nprim;
+            const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
+            PrimGeo<R> pg;
+            prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
+            C::gacc(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, (R)(2 * b0.w),
+                    (R)(2 * (b0.x - b0.w)), tc, acc);
+          }
+        }
+        if (nprim > 0) {
+          R gam[C::NOUT];
+          fill_gam(gam);
+          C::gfin(acc, AB, CD, gam, gr);
+        }
+      } else {
+        // the (pp|pp) derivative routines are compiled out of line and read
+        // the density products through a pointer: for that class they live
+        // in shared memory (after the per-atom sums) rather than in local
+        // memory, which spilled to DRAM
+        R gam_reg[kGamSmem ? 1 : C::NOUT];
+        R* gam = kGamSmem ? reinterpret_cast<R*>(gsh + nsm) + (size_t)threadIdx.x * C::NOUT : gam_reg;
+        fill_gam(gam);
+#pragma unroll 1
+        for (int kq = slice; kq < ki0.w; kq += ps) {
+          const V* kr = prim + 3 * (size_t)(ki0.z + kq);
+          const V k0 = kr[0], k1 = kr[1], k2 = kr[2];
+          const R kcd = fabs((R)k0.z);
+          if (kab_max * kcd < cut) break;
+          const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
+#pragma unroll 1
+          for (int kpp = 0; kpp < bi0.w; ++kpp) {
+            const V* br = prim + 3 * (size_t)(bi0.z + kpp);
+            const V b0 = br[0], b1 = br[1], b2 = br[2];
+            if (fabs((R)b0.z) * kcd < cut) break;
+            ++nprim;
+            const R PA[3] = {(R)b2.x, (R)b2.y, (R)b2.z};
+            PrimGeo<R> pg;
+            prim_setup<R, C::L + 1>(b0, b1, k0, k1, pg);
+            C::gradA(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * b0.w), gam,
+                     gr);
+            C::gradB(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD,
+                     (R)(2 * (b0.x - b0.w)), gam, gr + 3);
+            C::gradC(pg.I, PA, pg.WP, QC, pg.WQ, pg.o2p, pg.nrp, pg.o2q, pg.nrq, pg.o2pq, AB, CD, (R)(2 * k0.w), gam,
+                     gr + 6);
+          }
         }
       }
       double fac = 4.0;
@@ -2132,12 +2170,12 @@ const ClassFlops& class_flops(int qc) {
   using C4 = EriClass<double, 1, 1, 1, 0>;
   using C5 = EriClass<double, 1, 1, 1, 1>;
   static const ClassFlops tab[NQCLASS] = {
-      {C0::L, C0::NOUT, C0::VRR_FLOPS, C0::HRR_FLOPS, C0::GRAD_FLOPS},
-      {C1::L, C1::NOUT, C1::VRR_FLOPS, C1::HRR_FLOPS, C1::GRAD_FLOPS},
-      {C2::L, C2::NOUT, C2::VRR_FLOPS, C2::HRR_FLOPS, C2::GRAD_FLOPS},
-      {C3::L, C3::NOUT, C3::VRR_FLOPS, C3::HRR_FLOPS, C3::GRAD_FLOPS},
-      {C4::L, C4::NOUT, C4::VRR_FLOPS, C4::HRR_FLOPS, C4::GRAD_FLOPS},
-      {C5::L, C5::NOUT, C5::VRR_FLOPS, C5::HRR_FLOPS, C5::GRAD_FLOPS},
+      {C0::L, C0::NOUT, C0::VRR_FLOPS, C0::HRR_FLOPS, C0::GCON ? C0::GACC_FLOPS : C0::GRAD_FLOPS, C0::GFIN_FLOPS},
+      {C1::L, C1::NOUT, C1::VRR_FLOPS, C1::HRR_FLOPS, C1::GCON ? C1::GACC_FLOPS : C1::GRAD_FLOPS, C1::GFIN_FLOPS},
+      {C2::L, C2::NOUT, C2::VRR_FLOPS, C2::HRR_FLOPS, C2::GCON ? C2::GACC_FLOPS : C2::GRAD_FLOPS, C2::GFIN_FLOPS},
+      {C3::L, C3::NOUT, C3::VRR_FLOPS, C3::HRR_FLOPS, C3::GCON ? C3::GACC_FLOPS : C3::GRAD_FLOPS, C3::GFIN_FLOPS},
+      {C4::L, C4::NOUT, C4::VRR_FLOPS, C4::HRR_FLOPS, C4::GCON ? C4::GACC_FLOPS : C4::GRAD_FLOPS, C4::GFIN_FLOPS},
+      {C5::L, C5::NOUT, C5::VRR_FLOPS, C5::HRR_FLOPS, C5::GCON ? C5::GACC_FLOPS : C5::GRAD_FLOPS, C5::GFIN_FLOPS},
   };
   return tab[qc];
 }

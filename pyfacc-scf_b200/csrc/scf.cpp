@@ -757,7 +757,8 @@ void System::gradient(double* g_host) {
   PF_CUDA(cudaMemcpy(cnt, gstats, sizeof(cnt), cudaMemcpyDeviceToHost));
   st.flops_grad = 0.0;
   for (int q = 0; q < NQCLASS; ++q)
-    st.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false));
+    st.flops_grad += (double)cnt[NQCLASS + q] * (class_flops(q).grad + prim_overhead_flops(q, false)) +
+                       (double)cnt[q] * class_flops(q).gfin;
   nuclear_repulsion_gradient(g.data());
   grad_host = g;
   if (g_host) std::memcpy(g_host, g.data(), g.size() * sizeof(double));
