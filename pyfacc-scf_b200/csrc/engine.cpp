@@ -571,7 +571,7 @@ void System::build_tasks() {
 
 void System::alloc_matrices() {
   const size_t n2 = (size_t)nbf * nbf;
-  const int nmat = 28 + 4 * std::max(opt.diis_size, 1);
+  const int nmat = 30 + 4 * std::max(opt.diis_size, 1);
   mats.ensure(nmat * n2 * sizeof(double) + 96 * sizeof(double) + ns * ns * sizeof(float) + 1024);
   double* m = mats.as<double>();
   auto take = [&]() { double* r = m; m += n2; return r; };
@@ -581,6 +581,7 @@ void System::alloc_matrices() {
   W1 = take(); W2 = take(); W3 = take(); Err[0] = take(); Err[1] = take(); Cm[0] = take(); Cm[1] = take();
   Wm = take();
   Pu[0] = take(); Pu[1] = take(); Pu[2] = take(); Pu[3] = take();
+  Pp[0] = take(); Pp[1] = take();
   const int nd = std::max(opt.diis_size, 1);
   for (int i = 0; i < nd; ++i) {
     diis_F.push_back(m); m += 2 * n2;

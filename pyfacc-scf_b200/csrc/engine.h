@@ -327,6 +327,7 @@ void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pair
 void launch_symmetrize_add(int n, double* A, cudaStream_t s);
 void launch_identity(int n, double* A, cudaStream_t s);                  // A = I (n x n)             // A = A + A^T
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
+void launch_antisym(int n, const double* B, double* E, cudaStream_t s);  // E = B - B^T (n x n)
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
                  cudaStream_t s);                                          // F = H + J - kf K
 // Blocks of the DIIS / energy reductions (their partial sums are combined

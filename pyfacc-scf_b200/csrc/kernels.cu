@@ -1777,6 +1777,19 @@ void launch_symmetrize_add(int n, double* A, cudaStream_t s) {
   count_launch();
 }
 
+// E = B - B^T (the commutator F'P' - P'F' from B = F'P' with F', P' symmetric)
+__global__ void antisym_kernel(int n, const double* __restrict__ B, double* __restrict__ E) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || j >= n) return;
+  E[(size_t)i * n + j] = B[(size_t)i * n + j] - B[(size_t)j * n + i];
+}
+void launch_antisym(int n, const double* B, double* E, cudaStream_t s) {
+  dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
+  antisym_kernel<<<g, b, 0, s>>>(n, B, E);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
 __global__ void axpby_kernel(long long n, double a, const double* __restrict__ x, double b, double* __restrict__ y) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     y[i] = a * x[i] + b * y[i];

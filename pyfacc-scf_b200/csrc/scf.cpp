@@ -187,6 +187,15 @@ void System::orthogonalizer() {
                         &one, L, nbf, X, nbf));
 }
 
+// Eigenpairs of F' = X^T F X (= R F R^T, symmetric) given directly, C = X C'.
+void System::diagonalize_orth(const double* Fp, double* C, double* eps) {
+  const double one = 1.0, zero = 0.0;
+  PF_CUDA(cudaMemcpyAsync(W2, Fp, (size_t)nbf * nbf * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  PF_CUSOLVER(cusolverDnDsyevd(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W2, nbf, eps,
+                               syev_work.as<double>(), syev_lwork, info_dev));
+  PF_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, nbf, nbf, nbf, &one, X, nbf, W2, nbf, &zero, C, nbf));
+}
+
 // F' = X^T F X, eigenpairs, C = X C' (all column-major).
 void System::diagonalize(const double* Fm, double* C, double* eps) {
   const double one = 1.0, zero = 0.0;
@@ -250,21 +259,36 @@ std::vector<double> System::atomic_occupations() const {
 // The buffer X holds, read row-major, R = L^{-1} (cuBLAS wrote X = L^{-T}
 // column-major), so X^T F X = R F R^T and X P' X^T = R^T P' R in the
 // row-major products of dense.cu.
-bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
+bool System::purify(const double* Fm, int nocc, double scale, double* Pm, double* Pp) {
   const int n = nbf;
+  if (nocc > 0 && nocc < n) {  // F' = R F R^T into the graph's input
+    launch_dgemm(n, n, n, false, Fm, n, true, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
+    launch_dgemm(n, n, n, false, X, n, false, W1, n, Pu[0], n, 1.0, nullptr, n, 0.0, true, false, stream);
+  }
+  return purify_core(nocc, scale, Pm, Pp);
+}
+
+bool System::purify_orth(const double* Fp, int nocc, double scale, double* Pm, double* Pp) {
+  if (nocc > 0 && nocc < nbf && Fp != Pu[0])
+    PF_CUDA(cudaMemcpyAsync(Pu[0], Fp, (size_t)nbf * nbf * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+  return purify_core(nocc, scale, Pm, Pp);
+}
+
+// TC2 on F' (in Pu[0]): P = scale R^T P' R, and P' into Pp when given.
+bool System::purify_core(int nocc, double scale, double* Pm, double* Pp) {
+  const int n = nbf;
+  const size_t bytes = (size_t)n * n * sizeof(double);
   if (nocc <= 0) {
-    launch_zero(Pm, (size_t)n * n * sizeof(double), stream);
+    launch_zero(Pm, bytes, stream);
+    if (Pp) launch_zero(Pp, bytes, stream);
     return true;
   }
-  if (nocc >= n) {  // every orbital occupied: P = scale * X X^T = scale * S^-1
+  if (nocc >= n) {  // every orbital occupied: P = scale * X X^T = scale * S^-1, P' = I
     launch_dgemm(n, n, n, true, X, n, false, X, n, Pm, n, scale, nullptr, n, 0.0, true, false, stream);
+    if (Pp) launch_identity(n, Pp, stream);
     return true;
   }
-  double* Fp = Pu[0];
   double* Xa = Pu[1];
-  // F' = R F R^T
-  launch_dgemm(n, n, n, false, Fm, n, true, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
-  launch_dgemm(n, n, n, false, X, n, false, W1, n, Fp, n, 1.0, nullptr, n, 0.0, true, false, stream);
   // the whole TC2 iteration is one graph launch (conditional WHILE loop on
   // the device); the host reads the outcome once
   if (opt.verbose) PF_CUDA(cudaEventRecord(ctx.ev0, stream));
@@ -278,6 +302,7 @@ bool System::purify(const double* Fm, int nocc, double scale, double* Pm) {
   purify_steps += steps;
   if (opt.verbose) purify_ms += elapsed(ctx.ev0, ctx.ev1);
   if (ctl[1] == 0.0 || ctl[4] != 0.0) return false;
+  if (Pp) PF_CUDA(cudaMemcpyAsync(Pp, Xa, bytes, cudaMemcpyDeviceToDevice, stream));
   // P = scale R^T Xp R
   launch_dgemm(n, n, n, false, Xa, n, false, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
   launch_dgemm(n, n, n, true, X, n, false, W1, n, Pm, n, scale, nullptr, n, 0.0, true, false, stream);
@@ -296,11 +321,22 @@ cudaGraphExec_t System::tc2_graph(int nocc) {
 
 // New density from a Fock matrix: purification, or eigenvectors when the
 // purification does not converge (no gap at the occupation number).
-void System::density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps) {
-  if (purify(Fm, nocc, scale, Pm)) return;
+bool System::density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps,
+                          double* Pp) {
+  if (purify(Fm, nocc, scale, Pm, Pp)) return Pp != nullptr;
   purify_fallbacks++;
   diagonalize(Fm, C, eps);
   density_from(C, nocc, scale, Pm);
+  return false;
+}
+
+bool System::density_step_orth(const double* Fp, int nocc, double scale, double* Pm, double* C, double* eps,
+                               double* Pp) {
+  if (purify_orth(Fp, nocc, scale, Pm, Pp)) return Pp != nullptr;
+  purify_fallbacks++;
+  diagonalize_orth(Fp, C, eps);
+  density_from(C, nocc, scale, Pm);
+  return false;
 }
 
 // Orbitals of the final Fock matrices, for the caller's outputs.
@@ -376,9 +412,16 @@ void System::run_scf() {
   orbitals_ready = false;
   purify_steps = purify_fallbacks = 0;
   purify_ms = 0.0;
+  // DIIS on the orthonormal-basis Fock matrices F' = R F R^T: with P =
+  // scale R^T P' R the error R (F P S - S P F) R^T is scale (F' P' - P' F'),
+  // and the extrapolated F' goes to the purification as it is (5 dense
+  // products per iteration instead of 8).  pp_ok: Pp holds P' of the
+  // current density (not after the atomic guess or an eigensolver fallback).
+  const bool orth_diis = opt.diis_size > 0;
+  bool pp_ok[2] = {false, false};
   if (opt.guess == PYFACC_GUESS_CORE) {
     // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144)
-    for (int s = 0; s < nsp; ++s) density_step(H, nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
+    for (int s = 0; s < nsp; ++s) pp_ok[s] = density_step(H, nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf, Pp[s]);
   } else {
     const std::vector<double> occ = atomic_occupations();
     const double ne = (double)(nalpha + nbeta);
@@ -477,30 +520,44 @@ void System::run_scf() {
     // ---- DIIS error X^T (F P S - S P F) X and energy
     // R (F P S - S P F) R^T with R = L^{-1} the row-major view of X (the
     // error's sign and transpose do not matter: only max |E| and <E_i, E_j>
-    // are used); FPS - SPF = A - A^T with A = F P S
+    // are used); FPS - SPF = A - A^T with A = F P S, or scale (F'P' - P'F')
+    // = B - B^T with B = scale F' P' when P' is known
+    int slot = -1;
+    if (ndiis > 0) {
+      slot = head;
+      head = (head + 1) % ndiis;
+    }
+    const bool use_pp = orth_diis && pp_ok[0] && (nsp == 1 || pp_ok[1]);
+    double* Eo[2] = {Err[0], Err[1]};
     for (int s = 0; s < nsp; ++s) {
+      if (slot >= 0) Eo[s] = diis_E[slot] + s * n2;
+      if (orth_diis) {  // F' = R F R^T, the stored DIIS vector
+        double* Fo = diis_F[slot] + s * n2;
+        launch_dgemm(nbf, nbf, nbf, false, F[s], nbf, true, X, nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, false,
+                     stream);
+        launch_dgemm(nbf, nbf, nbf, false, X, nbf, false, W1, nbf, Fo, nbf, 1.0, nullptr, nbf, 0.0, true, false,
+                     stream);
+        if (use_pp) {
+          launch_dgemm(nbf, nbf, nbf, false, Fo, nbf, false, Pp[s], nbf, W1, nbf, pscale, nullptr, nbf, 0.0, false,
+                       false, stream);
+          launch_antisym(nbf, W1, Eo[s], stream);
+          continue;
+        }
+      }
       launch_dgemm(nbf, nbf, nbf, false, F[s], nbf, false, P[s], nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, false,
                    stream);
       launch_dgemm(nbf, nbf, nbf, false, W1, nbf, false, S, nbf, W2, nbf, 1.0, nullptr, nbf, 0.0, false, false,
                    stream);
       launch_dgemm(nbf, nbf, nbf, false, W2, nbf, true, X, nbf, W1, nbf, 1.0, nullptr, nbf, 0.0, false, true,
                    stream);
-      launch_dgemm(nbf, nbf, nbf, false, X, nbf, false, W1, nbf, Err[s], nbf, 1.0, nullptr, nbf, 0.0, false, false,
+      launch_dgemm(nbf, nbf, nbf, false, X, nbf, false, W1, nbf, Eo[s], nbf, 1.0, nullptr, nbf, 0.0, false, false,
                    stream);
     }
-    launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Err[0],
-                      uhf ? Err[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, red_part, stream);
-    // ---- DIIS bookkeeping: store F and the error vector, overlaps with the stored errors
-    int slot = -1;
-    if (ndiis > 0) {
-      slot = head;
-      head = (head + 1) % ndiis;
-      for (int s = 0; s < nsp; ++s) {
-        PF_CUDA(cudaMemcpyAsync(diis_F[slot] + s * n2, F[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-        PF_CUDA(cudaMemcpyAsync(diis_E[slot] + s * n2, Err[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-      }
-      launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, red_part, stream);
-    }
+    launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Eo[0],
+                      uhf ? Eo[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, red_part, stream);
+    // ---- DIIS bookkeeping: F' and the error vector are in their slot;
+    // overlaps with the stored errors
+    if (ndiis > 0) launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, red_part, stream);
     double red[8 + 64];
     PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
     PF_CUDA(cudaStreamSynchronize(stream));
@@ -541,6 +598,10 @@ void System::run_scf() {
       PF_CUDA(cudaMemcpyAsync(Pold[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     // ---- extrapolate
     const double* Fuse[2] = {F[0], F[1]};
+    if (orth_diis) {
+      Fuse[0] = diis_F[slot];
+      Fuse[1] = diis_F[slot] + n2;
+    }
     if (ndiis > 0) {
       slot_age[slot] = it;
       for (int k = 0; k < ndiis; ++k) {
@@ -566,8 +627,9 @@ void System::run_scf() {
           }
           b[m] = -1.0;
           if (solve_small(m + 1, A, b, x)) {
-            // F_diis = sum c_i F_i  (into W3 / Wm as the stacked spins)
-            double* Fd = W3;
+            // F'_diis = sum c_i F'_i (into W3 / Wm as the stacked spins; a
+            // closed shell's straight into the purification's input)
+            double* Fd = uhf ? W3 : Pu[0];
             std::vector<const double*> src(m);
             for (int i = 0; i < m; ++i) src[i] = diis_F[use[i]];
             launch_lincomb((long long)n2, m, src.data(), x.data(), Fd, stream);
@@ -590,7 +652,9 @@ void System::run_scf() {
     // ---- diagonalise and rebuild the density (timed at the next sync, so
     // the host queues the next Fock build while this one runs)
     PF_CUDA(cudaEventRecord(d0, stream));
-    for (int s = 0; s < nsp; ++s) density_step(Fuse[s], nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
+    for (int s = 0; s < nsp; ++s)
+      pp_ok[s] = orth_diis ? density_step_orth(Fuse[s], nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf, Pp[s])
+                           : density_step(Fuse[s], nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf);
     PF_CUDA(cudaEventRecord(d1, stream));
     diag_pending = true;
   }

@@ -72,6 +72,7 @@ struct System {
   double *Cm[2] = {nullptr, nullptr}, *Wm = nullptr, *small = nullptr;
   double* red_part = nullptr;  // partial sums of the DIIS / energy reductions
   double *Pu[4] = {nullptr, nullptr, nullptr, nullptr};  // purification work matrices
+  double *Pp[2] = {nullptr, nullptr};  // projectors P' of the current density per spin (P = scale R^T P' R)
   double* pstate = nullptr;                      // TC2 state, two buffers of 8 (device)
   bool orbitals_ready = false;
   int task_width = TASK_WIDTH;  // kets per J/K task
@@ -131,8 +132,18 @@ struct System {
   void density_from(const double* C, int nocc, double scale, double* Pm);
   // P = scale * projector onto the nocc lowest eigenvectors of F (TC2
   // purification of X^T F X); false if it did not converge.
-  bool purify(const double* Fm, int nocc, double scale, double* Pm);
-  void density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps);
+  // With Pp: also the projector P' of the orthonormal basis (P = scale
+  // R^T P' R) into Pp.  density_step returns whether Pp was written (not
+  // after an eigensolver fallback).
+  bool purify(const double* Fm, int nocc, double scale, double* Pm, double* Pp = nullptr);
+  bool density_step(const double* Fm, int nocc, double scale, double* Pm, double* C, double* eps,
+                    double* Pp = nullptr);
+  // The same from the orthonormal-basis Fock matrix F' = R F R^T.
+  bool purify_orth(const double* Fp, int nocc, double scale, double* Pm, double* Pp);
+  bool density_step_orth(const double* Fp, int nocc, double scale, double* Pm, double* C, double* eps,
+                         double* Pp);
+  void diagonalize_orth(const double* Fp, double* C, double* eps);
+  bool purify_core(int nocc, double scale, double* Pm, double* Pp);
   void final_orbitals();
   // Diagonal starting density from atomic aufbau occupations of the
   // minimal-basis shells (total electrons, spread over 2 s / 6 p per shell).
