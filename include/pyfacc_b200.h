@@ -84,9 +84,9 @@ typedef struct pyfacc_options {
   double gradient_fp32_thresh; /* mixed gradient: derivative quartets with
                                Q_ab Q_cd max|P| (in a batch: Q_ab Q_cd)
                                below this run in FP32
-                               (|dG| ~6e-8 Ha/bohr at 1e-2, ~3e-9 at 1e-3
-                               for C40H82..C100H202); <= 0: fp32_thresh
-                                                                      (1e-2) */
+                               (max |dG| vs FP64 ~1e-6 Ha/bohr at 1e-1,
+                               ~1e-7 at 1e-2 for C40H82, C100H202, rna1,
+                               gly30); <= 0: fp32_thresh              (1e-1) */
   double coarse_err;        /* mixed: while the DIIS error is above this every
                                quartet runs in FP32; the first build below it
                                is a full mixed build that restarts the

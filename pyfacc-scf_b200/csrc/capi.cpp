@@ -104,7 +104,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->task_width = 0;
   o->gradient_precision = -1;
   o->polish = 0;
-  o->gradient_fp32_thresh = 1e-2;
+  o->gradient_fp32_thresh = 1e-1;
   o->coarse_err = 1e-3;
 }
 
