@@ -11,9 +11,10 @@
 //    commutator F P S - S P F of the DIIS error).
 //  * TC2 purification (Niklasson 2002) of F' = X^T F X as one CUDA graph per
 //    occupation number: Gershgorin bounds, X_0, then a conditional WHILE node
-//    whose body is two fused steps X <- X^2 or 2X - X^2 (product, update,
-//    traces of the new iterate), so a whole purification is one graph launch
-//    and the host reads the outcome once.  This replaces the rscf.f90:140-
+//    whose body is four fused steps X <- X^2 or 2X - X^2 (product, update,
+//    traces of the new iterate) chained by programmatic-dependent-launch
+//    edges, so a whole purification is one graph launch and the host reads
+//    the outcome once.  This replaces the rscf.f90:140-
 //    156 / la.f90:28-57 diagonalisation (dsyev of X^T F X, then D = 2 C C^T)
 //    by the equivalent projector onto the nocc lowest eigenvectors.
 #include <cuda_runtime.h>
@@ -286,6 +287,12 @@ __global__ void __launch_bounds__(32 * SPLITK) tc2g_step_kernel(const Tc2StepArg
   tile_of<true>(blockIdx.x, nt, nt, ti, tj);  // the grid is the upper-triangle tile count
   const int i0 = ti << 4, j0 = tj << 4;
   const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
+  // Programmatic dependent launch: within a WHILE body the next step's grid
+  // is launched while this one runs (its blocks wait here), so a step does
+  // not pay the whole launch latency.  Nothing of X, the traces or the
+  // control words is read before the previous step has completed.
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   // Every load that does not depend on the control words is issued first,
   // so that one L2 round trip covers them all: this lane's entries of X for
   // the update (warp 0), the control words, all three trace slots, and the
@@ -410,10 +417,12 @@ void launch_dgemm(int m, int n, int k, bool ta, const double* A, int lda, bool t
 }
 
 // The purification graph of one occupation number (see above): bounds,
-// X_0, WHILE { step parity 0 (Xa -> Xb), step parity 1 (Xb -> Xa) }.  The
+// X_0, WHILE { TC2_BODY_STEPS steps of alternating parity: 0 (Xa -> Xb),
+// 1 (Xb -> Xa), ... }.  The
 // result is in Xa; st[ST_CTL + 1] (done), [+2] (steps), [+4] (failed) of
 // parity 0 tell the outcome.
-cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, double* Xb, double* st, int kmax) {
+static cudaGraphExec_t build_tc2_graph_impl(int n, int nocc, const double* Fp, double* Xa, double* Xb, double* st,
+                                            int kmax, bool programmatic) {
   cudaGraph_t graph = nullptr;
   PF_CUDA(cudaGraphCreate(&graph, 0));
   cudaGraphExec_t exec = nullptr;
@@ -457,8 +466,13 @@ cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, d
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     const int nt = (n + 15) / 16;
     const int blocks = nt * (nt + 1) / 2;
-    cudaGraphNode_t s0 = nullptr, s1 = nullptr;
-    for (int par = 0; par < 2; ++par) {
+    // TC2_BODY_STEPS steps per WHILE iteration, chained by programmatic
+    // edges (the next step's launch overlaps the current one; the kernel
+    // waits for its predecessor's completion before reading anything), or
+    // by plain edges where the runtime does not take programmatic ones
+    cudaGraphNode_t prev = nullptr;
+    for (int q = 0; q < TC2_BODY_STEPS; ++q) {
+      const int par = q & 1;
       Tc2StepArgs a;
       a.n = n;
       a.nocc = (double)nocc;
@@ -468,15 +482,25 @@ cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, d
       a.parity = par;
       a.kmax = kmax;
       a.cond = h;
-      a.set_cond = par == 1;
+      a.set_cond = q == TC2_BODY_STEPS - 1;
       void* args[] = {&a};
       cudaKernelNodeParams p{};
       p.func = reinterpret_cast<void*>(tc2g_step_kernel);
       p.gridDim = dim3(blocks);
       p.blockDim = dim3(32 * SPLITK);
       p.kernelParams = args;
-      if (par == 0) PF_CUDA(cudaGraphAddKernelNode(&s0, body, nullptr, 0, &p));
-      else PF_CUDA(cudaGraphAddKernelNode(&s1, body, &s0, 1, &p));
+      cudaGraphNode_t node = nullptr;
+      PF_CUDA(cudaGraphAddKernelNode(&node, body, nullptr, 0, &p));
+      if (prev) {
+        cudaGraphEdgeData ed{};
+        ed.from_port = cudaGraphKernelNodePortProgrammatic;
+        ed.type = cudaGraphDependencyTypeProgrammatic;
+        if (!programmatic || cudaGraphAddDependencies_v2(body, &prev, &node, &ed, 1) != cudaSuccess) {
+          (void)cudaGetLastError();
+          PF_CUDA(cudaGraphAddDependencies(body, &prev, &node, 1));
+        }
+      }
+      prev = node;
     }
     const cudaError_t rc = cudaGraphInstantiate(&exec, graph, 0);
     if (rc != cudaSuccess) throw Error(PYFACC_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(rc));
@@ -486,6 +510,15 @@ cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, d
   }
   cudaGraphDestroy(graph);
   return exec;
+}
+
+cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, double* Xb, double* st, int kmax) {
+  try {
+    return build_tc2_graph_impl(n, nocc, Fp, Xa, Xb, st, kmax, true);
+  } catch (const Error&) {  // a runtime that does not instantiate programmatic edges in a WHILE body
+    (void)cudaGetLastError();
+    return build_tc2_graph_impl(n, nocc, Fp, Xa, Xb, st, kmax, false);
+  }
 }
 
 }  // namespace pyfacc

@@ -364,6 +364,7 @@ void launch_dgemm(int m, int n, int k, bool ta, const double* A, int lda, bool t
 // which st[9] (done), st[10] (steps) and st[12] (failed) give the outcome.
 cudaGraphExec_t build_tc2_graph(int n, int nocc, const double* Fp, double* Xa, double* Xb, double* st, int kmax);
 constexpr int TC2_KMAX = 200;
+constexpr int TC2_BODY_STEPS = 4;  // TC2 steps per WHILE iteration (even: the result ends in Xa)
 
 double probe_fp64(int device, double* fp32);
 

@@ -298,7 +298,7 @@ bool System::purify_core(int nocc, double scale, double* Pm, double* Pp) {
   PF_CUDA(cudaMemcpyAsync(ctl, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
   const int steps = (int)ctl[2];
-  count_launches(2 + steps + (steps & 1));
+  count_launches(2 + (steps + TC2_BODY_STEPS - 1) / TC2_BODY_STEPS * TC2_BODY_STEPS);
   purify_steps += steps;
   if (opt.verbose) purify_ms += elapsed(ctx.ev0, ctx.ev1);
   if (ctl[1] == 0.0 || ctl[4] != 0.0) return false;
