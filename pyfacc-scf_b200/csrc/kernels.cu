@@ -970,6 +970,8 @@ struct GradKernelArgs {
   int lwidth;
   int smem_atoms;  // atoms summed in shared memory (0: global atomics)
   int psplit;      // warps per task: warp k of a group takes ket primitives k, k + psplit, ...
+  int stage;       // FP32: bra primitive records staged per task in shared memory (0: global)
+  int stage_off;   // byte offset of the staging area in the dynamic shared memory
 };
 
 template <typename R> __device__ __forceinline__ const typename Rec<R>::T* grecords(const GradKernelArgs& a);
@@ -1024,6 +1026,17 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
     }
     const unsigned amask = __ballot_sync(0xffffffffu, active);
     if (amask == 0u) continue;
+    // the bra's primitive records; FP32 kernels stage them once per task in
+    // this warp's shared-memory area, as jk_kernel does
+    const V* brec = grecords<R>(args) + 3 * (size_t)bi0.z;
+    if (sizeof(R) == 4 && args.stage > 0) {
+      V* st = reinterpret_cast<V*>(reinterpret_cast<unsigned char*>(gsh) + args.stage_off) +
+              ((size_t)(threadIdx.x >> 5) * tpw + (lane >> lw)) * 3 * (size_t)args.stage;
+      __syncwarp();
+      for (int i = sub; i < 3 * bi0.w; i += W) st[i] = brec[i];
+      __syncwarp();
+      brec = st;
+    }
     int nprim = 0;
     double g[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     if (active) {
@@ -1062,7 +1075,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
       R gr[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       const V* prim = grecords<R>(args);
       const R cut = (R)kcut;
-      const R kab_max = fabs((R)prim[3 * (size_t)bi0.z].z);
+      const R kab_max = fabs((R)brec[0].z);
       if constexpr (C::GCON) {
         // exponent-weighted sums over the primitive quartets, then one HRR
         // and one contraction with Gamma per contracted quartet
@@ -1079,7 +1092,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
           const R tc = (R)(2 * k0.w);
 #pragma unroll 1
           for (int kpp = 0; kpp < bi0.w; ++kpp) {
-            const V* br = prim + 3 * (size_t)(bi0.z + kpp);
+            const V* br = brec + 3 * kpp;
             const V b0 = br[0], b1 = br[1], b2 = br[2];
             if (fabs((R)b0.z) * kcd < cut) break;
             ++nprim;
@@ -1112,7 +1125,7 @@ __global__ void __launch_bounds__(128) grad2e_kernel(const GradKernelArgs args) 
           const R QC[3] = {(R)k2.x, (R)k2.y, (R)k2.z};
 #pragma unroll 1
           for (int kpp = 0; kpp < bi0.w; ++kpp) {
-            const V* br = prim + 3 * (size_t)(bi0.z + kpp);
+            const V* br = brec + 3 * kpp;
             const V b0 = br[0], b1 = br[1], b2 = br[2];
             if (fabs((R)b0.z) * kcd < cut) break;
             ++nprim;
@@ -1209,8 +1222,12 @@ void launch_grad2e(const PairData& pd, const TaskList& tl, int bc, int kc, bool 
   k.smem_atoms = (a.natoms_total > 0 && a.natoms_total <= 256) ? a.natoms_total : 0;
   // the (pp|pp) kernels keep each thread's density products in shared memory
   const size_t gam_bytes = k.qclass == NQCLASS - 1 ? 128 * 81 * (fp32 ? sizeof(float) : sizeof(double)) : 0;
-  const size_t smem = 3 * (size_t)k.smem_atoms * sizeof(double) + gam_bytes;
   const int tpw = 32 / tl.width;
+  const size_t base = 3 * (size_t)k.smem_atoms * sizeof(double) + gam_bytes;
+  const size_t stage_bytes = (size_t)4 * tpw * 3 * sizeof(float4) * pd.class_maxprim[bc];
+  k.stage_off = (int)((base + 15) / 16 * 16);
+  k.stage = (fp32 && pd.class_maxprim[bc] > 0 && stage_bytes <= JK_STAGE_MAX_BYTES) ? pd.class_maxprim[bc] : 0;
+  const size_t smem = k.stage ? (size_t)k.stage_off + stage_bytes : base;
   const long long warps = (tl.ntasks + tpw - 1) / tpw;
   k.psplit = primitive_split(warps, num_sms);
   int nblk = grid_for((int)std::min<long long>(warps * k.psplit, 1LL << 30), num_sms);
