@@ -51,7 +51,7 @@ typedef struct pyfacc_options {
   double eps_diis;          /* max |X^T (FDS - SDF) X| < eps_diis     (1e-8)  */
   double eps_density;       /* ||D_n - D_{n-1}||_F < eps_density; <=0 off (0) */
   int max_iter;             /* (100)                                           */
-  int diis_size;            /* Pulay subspace; 0 = plain Roothaan     (8)     */
+  int diis_size;            /* Pulay subspace, 0..64; 0 = plain Roothaan (8) */
   int scf_type;             /* PYFACC_SCF_*                           (AUTO)  */
   int precision;            /* PYFACC_PRECISION_*                     (FP64)  */
   int boys_mode;            /* PYFACC_BOYS_* for the V matrix         (ACCURATE) */

@@ -73,6 +73,8 @@ System::System(const pyfacc_molecule& m, const pyfacc_options& o) : opt(o) {
   if (opt.task_width != 0 && opt.task_width != 8 && opt.task_width != 16 && opt.task_width != 32)
     throw Error(PYFACC_ERR_INVALID, "task_width must be 0, 8, 16 or 32");
   if (opt.task_width) task_width = opt.task_width;
+  if (opt.diis_size < 0 || opt.diis_size > MAX_DIIS)
+    throw Error(PYFACC_ERR_INVALID, "diis_size must be 0.." + std::to_string(MAX_DIIS));
   // host-side parsing first: argument, element and basis errors are
   // reported before (and without) any device work
   natoms = m.natoms;

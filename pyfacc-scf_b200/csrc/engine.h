@@ -333,6 +333,7 @@ void launch_fock(long long n, const double* H, const double* J, double kf, const
 // Blocks of the DIIS / energy reductions (their partial sums are combined
 // in a fixed order: the results do not depend on scheduling).
 constexpr int RED_BLOCKS = 64;
+constexpr int MAX_DIIS = 64;  // largest Pulay subspace (diis_size)
 // part: scratch of RED_BLOCKS x max(m, 3) doubles
 void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, double* part,
                      cudaStream_t s);

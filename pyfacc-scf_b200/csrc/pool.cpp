@@ -97,6 +97,8 @@ GpuContext context_acquire(int dev) {
   PF_CUDA(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
   PF_CUDA(cudaEventCreateWithFlags(&c.fork, cudaEventDisableTiming));
   PF_CUDA(cudaEventCreateWithFlags(&c.join, cudaEventDisableTiming));
+  PF_CUDA(cudaEventCreateWithFlags(&c.ready, cudaEventDisableTiming));
+  PF_CUDA(cudaMallocHost(&c.pinned, PINNED_DOUBLES * sizeof(double)));
   return c;
 }
 

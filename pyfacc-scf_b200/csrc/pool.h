@@ -27,7 +27,12 @@ struct GpuContext {
   // half of a mixed Fock build or gradient), forked and joined by events
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // pinned host words for the per-iteration readbacks (asynchronous copies,
+  // so work queued after them runs while the host waits on `ready`)
+  double* pinned = nullptr;
+  cudaEvent_t ready = nullptr;
 };
+constexpr int PINNED_DOUBLES = 256;
 GpuContext context_acquire(int device);   // the current device must be `device`
 void context_release(const GpuContext& c);
 

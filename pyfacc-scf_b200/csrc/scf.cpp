@@ -294,19 +294,25 @@ bool System::purify_core(int nocc, double scale, double* Pm, double* Pp) {
   if (opt.verbose) PF_CUDA(cudaEventRecord(ctx.ev0, stream));
   PF_CUDA(cudaGraphLaunch(tc2_graph(nocc), stream));
   if (opt.verbose) PF_CUDA(cudaEventRecord(ctx.ev1, stream));
-  double ctl[8];
-  PF_CUDA(cudaMemcpyAsync(ctl, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
-  PF_CUDA(cudaStreamSynchronize(stream));
-  const int steps = (int)ctl[2];
-  count_launches(2 + (steps + TC2_BODY_STEPS - 1) / TC2_BODY_STEPS * TC2_BODY_STEPS);
-  purify_steps += steps;
-  if (opt.verbose) purify_ms += elapsed(ctx.ev0, ctx.ev1);
-  if (ctl[1] == 0.0 || ctl[4] != 0.0) return false;
+  // the outcome into pinned memory; the projector's copy and the
+  // back-transform are queued before it is read, so they run while the host
+  // waits (after a failed purification the eigensolver fallback overwrites
+  // Pm, and the caller does not use Pp)
+  double* ctl_pinned = ctx.pinned + 128;
+  PF_CUDA(cudaMemcpyAsync(ctl_pinned, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaEventRecord(ctx.ready, stream));
   if (Pp) PF_CUDA(cudaMemcpyAsync(Pp, Xa, bytes, cudaMemcpyDeviceToDevice, stream));
   // P = scale R^T Xp R
   launch_dgemm(n, n, n, false, Xa, n, false, X, n, W1, n, 1.0, nullptr, n, 0.0, false, false, stream);
   launch_dgemm(n, n, n, true, X, n, false, W1, n, Pm, n, scale, nullptr, n, 0.0, true, false, stream);
-  return true;
+  PF_CUDA(cudaEventSynchronize(ctx.ready));
+  double ctl[8];
+  std::memcpy(ctl, ctl_pinned, sizeof(ctl));
+  const int steps = (int)ctl[2];
+  count_launches(2 + (steps + TC2_BODY_STEPS - 1) / TC2_BODY_STEPS * TC2_BODY_STEPS);
+  purify_steps += steps;
+  if (opt.verbose) purify_ms += elapsed(ctx.ev0, ctx.ev1);
+  return !(ctl[1] == 0.0 || ctl[4] != 0.0);
 }
 
 // The purification graph of one occupation number (dense.cu): built once
@@ -558,9 +564,16 @@ void System::run_scf() {
     // ---- DIIS bookkeeping: F' and the error vector are in their slot;
     // overlaps with the stored errors
     if (ndiis > 0) launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, red_part, stream);
+    // energy, errors and DIIS overlaps into pinned memory; the copy of P
+    // for the next iteration's |dP| runs while the host waits
+    const int nred = 8 + std::max(ndiis, 0);
+    PF_CUDA(cudaMemcpyAsync(ctx.pinned, small, nred * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    PF_CUDA(cudaEventRecord(ctx.ready, stream));
+    for (int s = 0; s < nsp; ++s)
+      PF_CUDA(cudaMemcpyAsync(Pold[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    PF_CUDA(cudaEventSynchronize(ctx.ready));
     double red[8 + 64];
-    PF_CUDA(cudaMemcpyAsync(red, small, (8 + std::max(ndiis, 0)) * sizeof(double), cudaMemcpyDeviceToHost, stream));
-    PF_CUDA(cudaStreamSynchronize(stream));
+    std::memcpy(red, ctx.pinned, nred * sizeof(double));
     if (diag_pending) {  // the previous iteration's density step, timed now
       ms_diag += elapsed(d0, d1);
       diag_pending = false;
@@ -594,8 +607,6 @@ void System::run_scf() {
       break;
     }
     E_old = E;
-    for (int s = 0; s < nsp; ++s)
-      PF_CUDA(cudaMemcpyAsync(Pold[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     // ---- extrapolate
     const double* Fuse[2] = {F[0], F[1]};
     if (orth_diis) {

@@ -90,3 +90,13 @@ def test_inconsistent_spin_is_invalid(engine):
     # one electron, doublet: consistent; a charge of 3 leaves -1 electrons
     mol.charge = 3
     assert _run_status(engine, mol) == N.ERR_INVALID
+
+
+@pytest.mark.parametrize("n", [-1, 65])
+def test_diis_size_out_of_range_is_invalid(engine, n):
+    """The Pulay subspace is read back with the energy every iteration into
+    a fixed block of 64 overlaps: a larger (or negative) diis_size is
+    refused before any device work."""
+    from pyfacc import _native as N
+    assert _run_status(engine, engine.Molecule(*_water()), diis_size=n) == N.ERR_INVALID
+    assert b"diis_size" in N.lib().pyfacc_last_message()
