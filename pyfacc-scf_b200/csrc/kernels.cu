@@ -1371,6 +1371,9 @@ struct Prim1e {
   double al, be, p, o2p, w;  // w = c_a c_b N_a N_b exp(-al be/p |AB|^2)
   double P[3], PA[3], PB[3];
 };
+// primitive pairs of a shell pair kept in shared memory by grad1e_kernel
+// (STO-6G: 36); shell pairs with more set them up per nucleus
+constexpr int GRAD1E_MAXPP = 36;
 
 // normalize = false: the coefficients multiply unnormalised primitives
 __device__ __forceinline__ void prim1e_setup(double al, double ca, int la, double be, double cb, int lb,
@@ -1421,15 +1424,17 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
   double s[NA * NB], t[NA * NB], v[NA * NB];
 #pragma unroll
   for (int i = 0; i < NA * NB; ++i) s[i] = t[i] = v[i] = 0.0;
+  // lpp lanes share one primitive pair (its Gaussian product is set up once)
+  // and split the nuclei between them
   const int npp = na * nb;
-  const int work = npp * natoms;
-  for (int idx = lane; idx < work; idx += 32) {
-    const int pp = idx % npp, c = idx / npp;
+  const int lpp = npp >= 32 ? 1 : 32 / npp;
+  const int sub = lane % lpp;
+  for (int pp = lane / lpp; pp < npp; pp += 32 / lpp) {
     const int ka = pp / nb, kb = pp % nb;
     Prim1e g;
     prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
     if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
-    if (c == 0) {
+    if (sub == 0) {
       double S[3][LA + 2][LB + 2];
       st_tables<LA + 2, LB + 2>(g, S);
 #pragma unroll
@@ -1443,15 +1448,18 @@ __global__ void __launch_bounds__(128) one_electron_kernel(int npair, const int2
           t[ia * NB + ib] += kin3(S, ca, cb, g.al, g.be);
         }
     }
-    const double4 Cn = atoms[c];
-    const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
-    double F[PF_BOYS_MMAX + 1];
-    boys_runtime(args.boys_mode, LA + LB, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
-    const double pref = -Cn.w * g.w * 6.2831853071795864769 / g.p;
-    double I[LA + LB + 1];
+    const double wp = g.w * 6.2831853071795864769 / g.p;
+    for (int c = sub; c < natoms; c += lpp) {
+      const double4 Cn = atoms[c];
+      const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
+      double F[PF_BOYS_MMAX + 1];
+      boys_runtime(args.boys_mode, LA + LB, g.p * (PC[0] * PC[0] + PC[1] * PC[1] + PC[2] * PC[2]), F);
+      const double pref = -Cn.w * wp;
+      double I[LA + LB + 1];
 #pragma unroll
-    for (int m = 0; m <= LA + LB; ++m) I[m] = pref * F[m];
-    NCl::vint(I, g.PA, PC, g.o2p, AB, v);
+      for (int m = 0; m <= LA + LB; ++m) I[m] = pref * F[m];
+      NCl::vint(I, g.PA, PC, g.o2p, AB, v);
+    }
   }
 #pragma unroll
   for (int i = 0; i < NA * NB; ++i) {
@@ -1636,6 +1644,7 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
     __syncthreads();
   }
   double* gacc = use_smem ? gsh : args.grad;  // per-atom accumulator (shared or global)
+  __shared__ Prim1e g1e_pp[4][GRAD1E_MAXPP];  // per warp: the current shell pair's primitive pairs
   const int lane = threadIdx.x & 31;
   const int nwarp_total = (gridDim.x * blockDim.x) >> 5;
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < npair; w += nwarp_total) {
@@ -1659,11 +1668,18 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
       }
     double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
     const int npp = na * nb;
+    // the primitive pairs' Gaussian products are set up once (kinetic and
+    // overlap loop) and kept in this warp's shared memory for the nuclear
+    // attraction loop, where every lane needs all of them
+    const bool cached = npp <= GRAD1E_MAXPP;
+    Prim1e* gpp = g1e_pp[threadIdx.x >> 5];
+    __syncwarp();
     // kinetic and overlap: lanes over primitive pairs
     for (int pp = lane; pp < npp; pp += 32) {
       const int ka = pp / nb, kb = pp % nb;
       Prim1e g;
       prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
+      if (cached) gpp[pp] = g;
       if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
       double S[3][LA + 3][LB + 2];
       st_tables<LA + 3, LB + 2>(g, S);
@@ -1691,6 +1707,7 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
           }
         }
     }
+    __syncwarp();
     // nuclear attraction: lanes over nuclei, all primitive pairs each
     for (int c = lane; c < mi.y; c += 32) {
       const double4 Cn = args.atoms[mi.x + c];
@@ -1698,7 +1715,8 @@ __global__ void __launch_bounds__(128) grad1e_kernel(int npair, const int2* __re
       for (int pp = 0; pp < npp; ++pp) {
         const int ka = pp / nb, kb = pp % nb;
         Prim1e g;
-        prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
+        if (cached) g = gpp[pp];
+        else prim1e_setup(ex[da.w + ka], co[da.w + ka], LA, ex[db.w + kb], co[db.w + kb], LB, A, B, g);
         if (fabs(g.w) * 6.2831853071795864769 / g.p < 1e-17) continue;
         const double PC[3] = {g.P[0] - Cn.x, g.P[1] - Cn.y, g.P[2] - Cn.z};
         double F[PF_BOYS_MMAX + 1];
