@@ -594,7 +594,7 @@ void System::alloc_matrices() {
   dmax = reinterpret_cast<float*>(m);
   const size_t red_bytes = (size_t)RED_BLOCKS * std::max(nd, 3) * sizeof(double);
   small_buf.ensure(2 * nbf * sizeof(double) + 256 + sizeof(JkStats) + 256 + 64 * sizeof(double*) + 256 +
-                   3 * natoms * sizeof(double) + 256 + 256 + red_bytes + 256);
+                   3 * natoms * sizeof(double) + 256 + 256 + red_bytes + 256 + nbf * sizeof(double) + 256 + 256);
   {
     char* b = small_buf.as<char>();
     size_t o = 0;
@@ -605,6 +605,12 @@ void System::alloc_matrices() {
     ptrs_dev = reinterpret_cast<const double**>(take(64 * sizeof(double*)));
     grad_dev = reinterpret_cast<double*>(take(3 * natoms * sizeof(double)));
     red_part = reinterpret_cast<double*>(take(red_bytes));
+    occ_dev = reinterpret_cast<double*>(take(nbf * sizeof(double)));
+    pmin_dev = reinterpret_cast<double*>(take(sizeof(double)));
+  }
+  {
+    const std::vector<double> occ = atomic_occupations();
+    PF_CUDA(cudaMemcpy(occ_dev, occ.data(), nbf * sizeof(double), cudaMemcpyHostToDevice));
   }
   int lwork = 0;
   PF_CUSOLVER(cusolverDnDsyevd_bufferSize(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nbf, W1, nbf,
@@ -621,6 +627,8 @@ void System::release_extra() {
   ptrs_dev = nullptr;
   grad_dev = nullptr;
   red_part = nullptr;
+  occ_dev = nullptr;
+  pmin_dev = nullptr;
 }
 
 }  // namespace pyfacc

@@ -325,6 +325,8 @@ void launch_grad1e(const ShellDev& sh, const int* npair, const int2* const* pair
 
 // Small dense helpers.
 void launch_symmetrize_add(int n, double* A, cudaStream_t s);
+void launch_set_diag(int n, const double* d, double f, double* A, cudaStream_t s);  // A = diag(f d)
+void launch_min_diag_sq(int n, const double* L, double* out, cudaStream_t s);   // out = min_i L_ii^2
 void launch_identity(int n, double* A, cudaStream_t s);                  // A = I (n x n)             // A = A + A^T
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_antisym(int n, const double* B, double* E, cudaStream_t s);  // E = B - B^T (n x n)

@@ -1793,6 +1793,44 @@ __global__ void symmetrize_add_kernel(int n, double* A) {
   A[(size_t)i * n + j] = s;
   A[(size_t)j * n + i] = s;
 }
+// A = diag(f d) (n x n)
+__global__ void set_diag_kernel(long long n2, int n, const double* __restrict__ d, double f, double* __restrict__ A) {
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += (long long)gridDim.x * blockDim.x)
+    A[k] = (k % (n + 1) == 0) ? f * d[k / (n + 1)] : 0.0;
+}
+void launch_set_diag(int n, const double* d, double f, double* A, cudaStream_t s) {
+  const long long n2 = (long long)n * n;
+  const int g = (int)std::min<long long>((n2 + 255) / 256, 2048);
+  set_diag_kernel<<<std::max(g, 1), 256, 0, s>>>(n2, n, d, f, A);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// out = min_i L_ii^2 (one block; NaN pivots propagate as NaN)
+__global__ void min_diag_sq_kernel(int n, const double* __restrict__ L, double* __restrict__ out) {
+  __shared__ double part[32];
+  double m = 1e300;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double v = L[(size_t)i * n + i] * L[(size_t)i * n + i];
+    m = (v < m || v != v) ? v : m;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double y = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (y < m || y != y) ? y : m;
+  }
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = (part[w] < m || part[w] != part[w]) ? part[w] : m;
+    *out = m;
+  }
+}
+void launch_min_diag_sq(int n, const double* L, double* out, cudaStream_t s) {
+  min_diag_sq_kernel<<<1, 256, 0, s>>>(n, L, out);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
 __global__ void identity_kernel(long long n2, int n, double* A) {
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n2; k += (long long)gridDim.x * blockDim.x)
     A[k] = (k % (n + 1) == 0) ? 1.0 : 0.0;

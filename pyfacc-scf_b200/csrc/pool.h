@@ -33,6 +33,11 @@ struct GpuContext {
   cudaEvent_t ready = nullptr;
 };
 constexpr int PINNED_DOUBLES = 256;
+// layout of GpuContext::pinned: [0, 72) energy, errors and DIIS overlaps of
+// an SCF iteration; [128, 136) the purification outcome; [200, 202) the
+// overlap factor's smallest pivot and status
+constexpr int PURIFY_PINNED = 128;
+constexpr int ORTHO_PINNED = 200;
 GpuContext context_acquire(int device);   // the current device must be `device`
 void context_release(const GpuContext& c);
 

@@ -164,27 +164,33 @@ void System::orthogonalizer() {
   if ((size_t)lwork * sizeof(double) > syev_work.bytes) syev_work.ensure((size_t)lwork * sizeof(double));
   PF_CUSOLVER(cusolverDnDpotrf(cusolver, CUBLAS_FILL_MODE_LOWER, nbf, L, nbf, syev_work.as<double>(), lwork,
                                info_dev));
+  // the status and the smallest pivot go to pinned memory and are checked
+  // after the next synchronisation (check_overlap_factor): nothing that runs
+  // before it can fault on a bad factor, it only computes with it
+  launch_min_diag_sq(nbf, L, pmin_dev, stream);
+  PF_CUDA(cudaMemcpyAsync(ctx.pinned + ORTHO_PINNED, pmin_dev, sizeof(double), cudaMemcpyDeviceToHost, stream));
+  PF_CUDA(cudaMemcpyAsync(ctx.pinned + ORTHO_PINNED + 1, info_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  launch_identity(nbf, X, stream);
+  const double one = 1.0;
+  PF_CUBLAS(cublasDtrsm(cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nbf, nbf,
+                        &one, L, nbf, X, nbf));
+}
+
+// The overlap factorisation's outcome (after a synchronisation that follows
+// orthogonalizer()): a non-positive-definite S is PYFACC_ERR_LINDEP.
+void System::check_overlap_factor() {
   int info = 0;
-  std::vector<double> piv(nbf);
-  PF_CUDA(cudaMemcpyAsync(&info, info_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
-  PF_CUDA(cudaMemcpy2DAsync(piv.data(), sizeof(double), L, (size_t)(nbf + 1) * sizeof(double), sizeof(double), nbf,
-                            cudaMemcpyDeviceToHost, stream));
-  PF_CUDA(cudaStreamSynchronize(stream));
+  std::memcpy(&info, ctx.pinned + ORTHO_PINNED + 1, sizeof(int));
+  const double pmin = ctx.pinned[ORTHO_PINNED];
   if (info > 0) throw Error(PYFACC_ERR_LINDEP, "overlap matrix is not positive definite");
   if (info < 0) throw Error(PYFACC_ERR_CUDA, "overlap factorisation failed");
   // Cholesky pivots L_ii^2 bound the smallest eigenvalue of S from above;
   // coincident atoms give a pivot at round-off level without a negative
   // one.  la.f90:40-44 warns below an eigenvalue of 1e-8 and goes on into
   // 1/sqrt of it; here a pivot below 1e-10 (S_ii = 1) is reported.
-  double pmin = 1e300;
-  for (double d : piv) pmin = std::min(pmin, d * d);
   if (!(pmin >= LINDEP_PIVOT))
     throw Error(PYFACC_ERR_LINDEP, "overlap matrix is numerically singular (smallest Cholesky pivot " +
                                        std::to_string(pmin) + "; coincident atoms?)");
-  launch_identity(nbf, X, stream);
-  const double one = 1.0;
-  PF_CUBLAS(cublasDtrsm(cublas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, nbf, nbf,
-                        &one, L, nbf, X, nbf));
 }
 
 // Eigenpairs of F' = X^T F X (= R F R^T, symmetric) given directly, C = X C'.
@@ -298,7 +304,7 @@ bool System::purify_core(int nocc, double scale, double* Pm, double* Pp) {
   // back-transform are queued before it is read, so they run while the host
   // waits (after a failed purification the eigensolver fallback overwrites
   // Pm, and the caller does not use Pp)
-  double* ctl_pinned = ctx.pinned + 128;
+  double* ctl_pinned = ctx.pinned + PURIFY_PINNED;
   PF_CUDA(cudaMemcpyAsync(ctl_pinned, pstate + 8, 8 * sizeof(double), cudaMemcpyDeviceToHost, stream));
   PF_CUDA(cudaEventRecord(ctx.ready, stream));
   if (Pp) PF_CUDA(cudaMemcpyAsync(Pp, Xa, bytes, cudaMemcpyDeviceToDevice, stream));
@@ -404,17 +410,26 @@ void System::run_scf() {
   PF_CUDA(cudaEventCreate(&d0));
   PF_CUDA(cudaEventCreate(&d1));
   bool diag_pending = false;
+  // one-electron matrices, the overlap factor and the starting density are
+  // queued without a synchronisation; their timings and the factor's status
+  // are read at the first one (the first iteration's readback)
+  cudaEvent_t q1, q2;
+  PF_CUDA(cudaEventCreate(&q1));
+  PF_CUDA(cudaEventCreate(&q2));
   PF_CUDA(cudaEventRecord(t0, stream));
-  PF_CUDA(cudaEventRecord(a0, stream));
   one_electron();
-  PF_CUDA(cudaEventRecord(a1, stream));
-  PF_CUDA(cudaStreamSynchronize(stream));
-  st.ms_1e = elapsed(a0, a1);
-  PF_CUDA(cudaEventRecord(a0, stream));
+  PF_CUDA(cudaEventRecord(q1, stream));
   orthogonalizer();
-  PF_CUDA(cudaEventRecord(a1, stream));
-  PF_CUDA(cudaStreamSynchronize(stream));
-  const float ms_orth = elapsed(a0, a1);
+  PF_CUDA(cudaEventRecord(q2, stream));
+  float ms_orth = 0.0f;
+  bool ortho_checked = false;
+  auto ortho_check = [&]() {
+    if (ortho_checked) return;
+    check_overlap_factor();
+    st.ms_1e = elapsed(t0, q1);
+    ms_orth = elapsed(q1, q2);
+    ortho_checked = true;
+  };
   orbitals_ready = false;
   purify_steps = purify_fallbacks = 0;
   purify_ms = 0.0;
@@ -426,17 +441,17 @@ void System::run_scf() {
   const bool orth_diis = opt.diis_size > 0;
   bool pp_ok[2] = {false, false};
   if (opt.guess == PYFACC_GUESS_CORE) {
-    // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144)
+    // core-Hamiltonian guess (rscf.f90:113-114, uscf.f90:140-144): it uses
+    // the factor, so its status is read first
+    PF_CUDA(cudaStreamSynchronize(stream));
+    ortho_check();
     for (int s = 0; s < nsp; ++s) pp_ok[s] = density_step(H, nocc[s], pscale, P[s], Cm[s], eps_dev + s * nbf, Pp[s]);
   } else {
-    const std::vector<double> occ = atomic_occupations();
+    // atomic occupations on the diagonal (occ_dev, uploaded with the system)
     const double ne = (double)(nalpha + nbeta);
-    std::vector<double> Dh(n2, 0.0);
     for (int s = 0; s < nsp; ++s) {
       const double f = uhf ? (s == 0 ? nalpha : nbeta) / ne : 1.0;
-      for (int i = 0; i < nbf; ++i) Dh[(size_t)i * nbf + i] = f * occ[i];
-      PF_CUDA(cudaMemcpyAsync(P[s], Dh.data(), n2 * sizeof(double), cudaMemcpyHostToDevice, stream));
-      PF_CUDA(cudaStreamSynchronize(stream));
+      launch_set_diag(nbf, occ_dev, f, P[s], stream);
     }
   }
   for (int s = 0; s < nsp; ++s) launch_zero(Pbuilt[s], n2 * sizeof(double), stream);
@@ -574,6 +589,7 @@ void System::run_scf() {
     PF_CUDA(cudaEventSynchronize(ctx.ready));
     double red[8 + 64];
     std::memcpy(red, ctx.pinned, nred * sizeof(double));
+    ortho_check();
     if (diag_pending) {  // the previous iteration's density step, timed now
       ms_diag += elapsed(d0, d1);
       diag_pending = false;
@@ -699,6 +715,7 @@ void System::run_scf() {
   }
   PF_CUDA(cudaEventRecord(t1, stream));
   PF_CUDA(cudaStreamSynchronize(stream));
+  ortho_check();  // (no iteration ran)
   st.ms_total = elapsed(t0, t1);
   st.ms_fock = ms_fock;
   st.ms_diag = ms_diag;
@@ -728,6 +745,8 @@ void System::run_scf() {
   cudaEventDestroy(a1);
   cudaEventDestroy(d0);
   cudaEventDestroy(d1);
+  cudaEventDestroy(q1);
+  cudaEventDestroy(q2);
 }
 
 // Analytic gradient of the converged SCF:

@@ -81,6 +81,8 @@ struct System {
   float* dmax = nullptr;
   std::vector<double*> diis_F, diis_E;
   double* eps_dev = nullptr;
+  double* occ_dev = nullptr;   // atomic-occupation starting density (diagonal)
+  double* pmin_dev = nullptr;  // smallest Cholesky pivot^2 of S
   int* info_dev = nullptr;
   unsigned long long* stats_dev = nullptr;
   const double** ptrs_dev = nullptr;
@@ -127,7 +129,8 @@ struct System {
   void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
           bool dynamic = false, double thresh = -1.0, double fp32_thresh = -1.0);
   void eri_tensor(double* eri);
-  void orthogonalizer();
+  void orthogonalizer();  // queued; its LINDEP status is read by check_overlap_factor after a later sync
+  void check_overlap_factor();
   void diagonalize(const double* Fm, double* C, double* eps);
   void density_from(const double* C, int nocc, double scale, double* Pm);
   // P = scale * projector onto the nocc lowest eigenvectors of F (TC2
