@@ -330,12 +330,17 @@ void launch_min_diag_sq(int n, const double* L, double* out, cudaStream_t s);   
 void launch_identity(int n, double* A, cudaStream_t s);                  // A = I (n x n)             // A = A + A^T
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_antisym(int n, const double* B, double* E, cudaStream_t s);  // E = B - B^T (n x n)
+void launch_diff(long long n, const double* x, const double* y, double* out, cudaStream_t s);  // out = x - y
+void launch_fock_half(int n, const double* H, const double* Jh, double kf, const double* Kh, double* F,
+                      cudaStream_t s);  // F = H + Jh + Jh^T - kf (Kh + Kh^T)
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
                  cudaStream_t s);                                          // F = H + J - kf K
 // Blocks of the DIIS / energy reductions (their partial sums are combined
 // in a fixed order: the results do not depend on scheduling).
 constexpr int RED_BLOCKS = 64;
 constexpr int MAX_DIIS = 64;  // largest Pulay subspace (diis_size)
+// System::jk output forms
+constexpr int JK_FULL = 0, JK_HALF = 1, JK_ADD = 2;
 // part: scratch of RED_BLOCKS x max(m, 3) doubles
 void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, double* part,
                      cudaStream_t s);

@@ -1874,6 +1874,35 @@ void launch_axpby(long long n, double a, const double* x, double b, double* y, c
   count_launch();
 }
 
+// F = H + (Jh + Jh^T) - kf (Kh + Kh^T) from the unsymmetrised halves
+__global__ void fock_half_kernel(int n, const double* __restrict__ H, const double* __restrict__ J, double kf,
+                                 const double* __restrict__ K, double* __restrict__ F) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || j >= n) return;
+  const size_t ij = (size_t)i * n + j, ji = (size_t)j * n + i;
+  F[ij] = H[ij] + (J[ij] + J[ji]) - kf * (K[ij] + K[ji]);
+}
+void launch_fock_half(int n, const double* H, const double* J, double kf, const double* K, double* F,
+                      cudaStream_t s) {
+  dim3 b(32, 8), g((n + 31) / 32, (n + 7) / 8);
+  fock_half_kernel<<<g, b, 0, s>>>(n, H, J, kf, K, F);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
+// out = x - y
+__global__ void diff_kernel(long long n, const double* __restrict__ x, const double* __restrict__ y,
+                            double* __restrict__ out) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = x[i] - y[i];
+}
+void launch_diff(long long n, const double* x, const double* y, double* out, cudaStream_t s) {
+  int g = (int)std::min<long long>((n + 255) / 256, 4096);
+  diff_kernel<<<std::max(g, 1), 256, 0, s>>>(n, x, y, out);
+  PF_CUDA(cudaGetLastError());
+  count_launch();
+}
+
 __global__ void fock_kernel(long long n, const double* __restrict__ H, const double* __restrict__ J, double kf,
                             const double* __restrict__ K, double* __restrict__ F) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)

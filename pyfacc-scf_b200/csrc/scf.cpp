@@ -55,11 +55,14 @@ void System::one_electron() {
 // density-weighted Schwarz test, the six class kernels (FP64 task lists, or
 // the FP64 and FP32 halves of the mixed lists), then J = Jh + Jh^T.
 void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-                bool dynamic, double thresh, double fp32_thresh) {
+                bool dynamic, double thresh, double fp32_thresh, int out) {
   if (thresh <= 0) thresh = opt.schwarz_thresh;
+  if (out == JK_ADD && reducer) throw Error(PYFACC_ERR_INVALID, "J/K cannot be added in place across shards");
   const size_t n2 = (size_t)nbf * nbf;
-  launch_zero(Jo, n2 * sizeof(double), stream);
-  for (int k = 0; k < nk; ++k) launch_zero(Ko[k], n2 * sizeof(double), stream);
+  if (out != JK_ADD) {
+    launch_zero(Jo, n2 * sizeof(double), stream);
+    for (int k = 0; k < nk; ++k) launch_zero(Ko[k], n2 * sizeof(double), stream);
+  }
   launch_dmax(ns, bf_off_dev, nfun_dev, nbf, Dj, Dk[0], nk > 1 ? Dk[1] : nullptr, dmax, stream);
   JkArgs a;
   a.Dj = Dj;
@@ -109,8 +112,10 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
     reduce(Jo, (long long)n2);
     for (int k = 0; k < nk; ++k) reduce(Ko[k], (long long)n2);
   }
-  launch_symmetrize_add(nbf, Jo, stream);
-  for (int k = 0; k < nk; ++k) launch_symmetrize_add(nbf, Ko[k], stream);
+  if (out == JK_FULL) {
+    launch_symmetrize_add(nbf, Jo, stream);
+    for (int k = 0; k < nk; ++k) launch_symmetrize_add(nbf, Ko[k], stream);
+  }
   st.n_fock++;
 }
 
@@ -505,38 +510,47 @@ void System::run_scf() {
     const double step_thresh = coarse_build ? std::max(coarse_screen, inc_thresh) : inc_thresh;
     restart = false;
     double* Kp[2] = {K[0], K[1]};
+    // Without a shard reducer J and K hold the unsymmetrised halves Jh, Kh
+    // (J = Jh + Jh^T): an incremental build adds into them in place and the
+    // Fock matrix is assembled from them (launch_fock_half).  With one, they
+    // are the full matrices summed over the shards.
+    const bool half = !reducer;
     if (full) {
       if (uhf) {
         launch_axpby((long long)n2, 1.0, P[0], 0.0, W3, stream);
         launch_axpby((long long)n2, 1.0, P[1], 1.0, W3, stream);
-        jk(W3, 2, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32);
+        jk(W3, 2, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32, half ? JK_HALF : JK_FULL);
       } else {
-        jk(P[0], 1, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32);
+        jk(P[0], 1, Pspin, J, Kp, opt.precision, mixed, full_thresh, t32, half ? JK_HALF : JK_FULL);
       }
       since_full = 0;
     } else {
       // dP = P - P_built; J += J[dP], K += K[dP]
       double* dP[2] = {Err[0], Err[1]};
-      for (int s = 0; s < nsp; ++s) {
-        launch_axpby((long long)n2, 1.0, P[s], 0.0, dP[s], stream);
-        launch_axpby((long long)n2, -1.0, Pbuilt[s], 1.0, dP[s], stream);
-      }
-      double* dK[2] = {W2, W3};
+      for (int s = 0; s < nsp; ++s) launch_diff((long long)n2, P[s], Pbuilt[s], dP[s], stream);
       const double* dPc[2] = {dP[0], dP[1]};
+      const double* dPj = dP[0];
       if (uhf) {
         launch_axpby((long long)n2, 1.0, dP[0], 0.0, Wm, stream);
         launch_axpby((long long)n2, 1.0, dP[1], 1.0, Wm, stream);
-        jk(Wm, 2, dPc, W1, dK, opt.precision, mixed, step_thresh, t32);
-      } else {
-        jk(dP[0], 1, dPc, W1, dK, opt.precision, mixed, step_thresh, t32);
+        dPj = Wm;
       }
-      launch_axpby((long long)n2, 1.0, W1, 1.0, J, stream);
-      for (int s = 0; s < nsp; ++s) launch_axpby((long long)n2, 1.0, dK[s], 1.0, K[s], stream);
+      if (half) {
+        jk(dPj, nsp, dPc, J, Kp, opt.precision, mixed, step_thresh, t32, JK_ADD);
+      } else {
+        double* dK[2] = {W2, W3};
+        jk(dPj, nsp, dPc, W1, dK, opt.precision, mixed, step_thresh, t32);
+        launch_axpby((long long)n2, 1.0, W1, 1.0, J, stream);
+        for (int s = 0; s < nsp; ++s) launch_axpby((long long)n2, 1.0, dK[s], 1.0, K[s], stream);
+      }
       since_full++;
     }
     for (int s = 0; s < nsp; ++s)
       PF_CUDA(cudaMemcpyAsync(Pbuilt[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
-    for (int s = 0; s < nsp; ++s) launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
+    for (int s = 0; s < nsp; ++s) {
+      if (half) launch_fock_half(nbf, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
+      else launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
+    }
     PF_CUDA(cudaEventRecord(a1, stream));
     // ---- DIIS error X^T (F P S - S P F) X and energy
     // R (F P S - S P F) R^T with R = L^{-1} the row-major view of X (the

@@ -126,8 +126,10 @@ struct System {
   // J = J[Dj], K[k] = K[Dk[k]] (precision 0 = fp64, 1 = mixed); screening by
   // Q_ab Q_cd max|D| with the density(ies) given.
   // fp32_thresh < 0: opt.fp32_thresh (mixed precision only)
+  // out: JK_FULL (zeroed, then J = Jh + Jh^T), JK_HALF (zeroed, left as Jh)
+  // or JK_ADD (added into an existing Jh; no reducer)
   void jk(const double* Dj, int nk, const double* const* Dk, double* Jo, double* const* Ko, int precision,
-          bool dynamic = false, double thresh = -1.0, double fp32_thresh = -1.0);
+          bool dynamic = false, double thresh = -1.0, double fp32_thresh = -1.0, int out = 0);
   void eri_tensor(double* eri);
   void orthogonalizer();  // queued; its LINDEP status is read by check_overlap_factor after a later sync
   void check_overlap_factor();
