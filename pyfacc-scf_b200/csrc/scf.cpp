@@ -811,8 +811,13 @@ void System::gradient(double* g_host) {
   g2.Pb = uhf ? Ps[1] : Pt;
   g2.dmax = opt.schwarz_thresh > 0 ? dmax : nullptr;
   g2.ns_ld = ns;
-  g2.thresh = opt.schwarz_thresh;
-  g2.prim_thresh = opt.schwarz_thresh * PRIM_QUARTET_REL_GRAD * grad_prim_cut_scale(basis);
+  // a mixed gradient screens its quartets at GRAD_SCREEN_MIXED (its FP32
+  // half already carries errors well above what that drops)
+  const bool gmix = opt.gradient_precision == PYFACC_PRECISION_MIXED ||
+                    (opt.gradient_precision < 0 && opt.precision == PYFACC_PRECISION_MIXED);
+  const double gthr = gmix ? std::max(opt.schwarz_thresh, GRAD_SCREEN_MIXED) : opt.schwarz_thresh;
+  g2.thresh = gthr;
+  g2.prim_thresh = gthr * PRIM_QUARTET_REL_GRAD * grad_prim_cut_scale(basis);
   g2.natoms_total = natoms;
   g2.uhf = uhf ? 1 : 0;
   g2.grad = grad_dev;
@@ -828,7 +833,7 @@ void System::gradient(double* g_host) {
                       (opt.gradient_precision < 0 && opt.precision == PYFACC_PRECISION_MIXED));
   const bool dyn_split = split && opt.shard_count <= 1;
   if (dyn_split)
-    launch_dyn_tasks(pd, dmax, ns, opt.schwarz_thresh,
+    launch_dyn_tasks(pd, dmax, ns, gthr,
                      opt.gradient_fp32_thresh > 0 ? opt.gradient_fp32_thresh : opt.fp32_thresh, dyn, stream);
   // the FP64 and FP32 halves run on different streams, which swap from
   // class to class (an FP64 gradient keeps its classes on one stream: its
