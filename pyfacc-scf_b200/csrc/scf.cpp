@@ -506,7 +506,9 @@ void System::run_scf() {
                             : std::min(COARSE_SCREEN_SPAN, std::max(1.0, err_prev / opt.coarse_err));
     const double coarse_screen = coarse_base * span;
     const double t32 = coarse_build ? t32_coarse : -1.0;
-    const double full_thresh = coarse_build ? coarse_screen : -1.0;
+    // a mixed full build (the restart after the coarse phase, periodic
+    // rebuilds) screens like the incremental ones
+    const double full_thresh = coarse_build ? coarse_screen : (mixed ? inc_thresh : -1.0);
     const double step_thresh = coarse_build ? std::max(coarse_screen, inc_thresh) : inc_thresh;
     restart = false;
     double* Kp[2] = {K[0], K[1]};
