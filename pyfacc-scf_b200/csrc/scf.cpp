@@ -80,6 +80,9 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
   if (opt.shard_count > 1) dynamic = false;  // shards use their static sub-lists
   const double t32 = fp32_thresh >= 0 ? fp32_thresh : opt.fp32_thresh;
   if (dynamic) launch_dyn_tasks(pd, dmax, ns, thresh, mixed ? t32 : 0.0, dyn, stream);
+  // an all-FP32 build (the coarse phase: t32 beyond every Q_ab Q_cd max|D|)
+  // has empty FP64 lists, whose kernels are not launched
+  const bool fp64_part = !(dynamic && mixed && t32 >= 1e299);
   // the FP64 and FP32 halves of a mixed build run on different streams,
   // which swap from class to class; an FP64 build alternates its classes
   // between the two streams (every launch only adds into J and K)
@@ -92,7 +95,7 @@ void System::jk(const double* Dj, int nk, const double* const* Dk, double* Jo, d
       const int qc = (bc == 0) ? 0 : (bc == 1 ? 1 + kc : 3 + kc);
       cudaStream_t s64 = (nth & 1) ? s32 : stream, s32c = (nth & 1) ? stream : s32;
       if (dynamic) {
-        launch_jk(pd, dyn.lists[2 * qc], bc, kc, false, nk, a, num_sms, mixed ? s64 : stream);
+        if (fp64_part) launch_jk(pd, dyn.lists[2 * qc], bc, kc, false, nk, a, num_sms, mixed ? s64 : stream);
         if (mixed) launch_jk(pd, dyn.lists[2 * qc + 1], bc, kc, true, nk, a, num_sms, s32c);
       } else if (mixed) {
         launch_jk(pd, tasks[bc][kc][1], bc, kc, false, nk, a, num_sms, stream);
