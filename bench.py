@@ -430,7 +430,7 @@ def run_ours(args):
         "dtype": "f64+f32 (mixed); f64 for the plain path",
         "data": "synthetic, seeded (geometry builder pyfacc.geometry.alkane)",
         "config": {"workload": WORKLOADS[wl]["label"], "precision": "mixed",
-                   "schwarz_thresh": 1e-12, "fp32_thresh": 1e-4, "scf": "dE<1e-10, DIIS err<1e-8",
+                   "schwarz_thresh": 1e-12, "fp32_thresh": 1e-3, "scf": "dE<1e-10, DIIS err<1e-8",
                    "coarse_err": 1e-3, "gradient_fp32_thresh": 1e-1,
                    "mixed_energy": "last incremental mixed build (no FP64 polish build)",
                    "l2": "flushed between steps (256 MiB write)",

@@ -57,7 +57,7 @@ typedef struct pyfacc_options {
   int boys_mode;            /* PYFACC_BOYS_* for the V matrix         (ACCURATE) */
   double schwarz_thresh;    /* skip quartets with Q_ab Q_cd D_max below (1e-12) */
   double fp32_thresh;       /* mixed: Q_ab Q_cd (max|D| of a single
-                               molecule's builds) below this run in FP32 (1e-4) */
+                               molecule's builds) below this run in FP32 (1e-3) */
   int incremental;          /* build G[dP] and add; -1 = on for MIXED   (-1)  */
   int rebuild_every;        /* full rebuild period of incremental builds (12) */
   int compute_gradient;     /* fill result->gradient after the SCF      (0)   */

@@ -90,7 +90,7 @@ void pyfacc_default_options(pyfacc_options* o) {
   o->precision = PYFACC_PRECISION_FP64;
   o->boys_mode = PYFACC_BOYS_ACCURATE;
   o->schwarz_thresh = 1e-12;
-  o->fp32_thresh = 1e-4;
+  o->fp32_thresh = 1e-3;
   o->incremental = -1;
   o->rebuild_every = 12;
   o->compute_gradient = 0;

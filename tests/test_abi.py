@@ -50,7 +50,7 @@ def test_default_options(engine):
     from pyfacc import _native as N
     o = N.default_options()
     assert o.eps_energy == 1e-10 and o.eps_diis == 1e-8 and o.max_iter == 100 and o.diis_size == 8
-    assert o.schwarz_thresh == 1e-12 and o.fp32_thresh == 1e-4 and o.shard_count == 1
+    assert o.schwarz_thresh == 1e-12 and o.fp32_thresh == 1e-3 and o.shard_count == 1
 
 
 def test_partition_balances_costs(engine):
