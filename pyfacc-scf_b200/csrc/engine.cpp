@@ -592,7 +592,7 @@ void System::alloc_matrices() {
   small = m; m += 48;
   pstate = m; m += 48;  // purification graph state (24 doubles used)
   dmax = reinterpret_cast<float*>(m);
-  const size_t red_bytes = (size_t)RED_BLOCKS * std::max(nd, 3) * sizeof(double);
+  const size_t red_bytes = (size_t)RED_BLOCKS * (nd + 3) * sizeof(double);
   small_buf.ensure(2 * nbf * sizeof(double) + 256 + sizeof(JkStats) + 256 + 64 * sizeof(double*) + 256 +
                    3 * natoms * sizeof(double) + 256 + 256 + red_bytes + 256 + nbf * sizeof(double) + 256 + 256);
   {

@@ -330,7 +330,7 @@ void launch_min_diag_sq(int n, const double* L, double* out, cudaStream_t s);   
 void launch_identity(int n, double* A, cudaStream_t s);                  // A = I (n x n)             // A = A + A^T
 void launch_axpby(long long n, double a, const double* x, double b, double* y, cudaStream_t s);  // y = a x + b y
 void launch_antisym(int n, const double* B, double* E, cudaStream_t s);  // E = B - B^T (n x n)
-void launch_diff(long long n, const double* x, const double* y, double* out, cudaStream_t s);  // out = x - y
+void launch_diff_update(long long n, const double* x, double* y, double* out, cudaStream_t s);  // out = x - y; y = x
 void launch_fock_half(int n, const double* H, const double* Jh, double kf, const double* Kh, double* F,
                       cudaStream_t s);  // F = H + Jh + Jh^T - kf (Kh + Kh^T)
 void launch_fock(long long n, const double* H, const double* J, double kf, const double* K, double* F,
@@ -346,14 +346,16 @@ constexpr int JK_FULL = 0, JK_HALF = 1, JK_ADD = 2;
 // < 1e-7 Ha/bohr on C40H82, C100H202, C30H61/STO-6G UHF, rna1 and gly30,
 // for 15-26% less gradient time
 constexpr double GRAD_SCREEN_MIXED = 1e-10;
-// part: scratch of RED_BLOCKS x max(m, 3) doubles
+// part: scratch of RED_BLOCKS x (m + 3) doubles
 void launch_dot_many(long long n, const double* x, int m, const double* const* ys, double* out, double* part,
                      cudaStream_t s);
 // out = sum_k c[k] src[k] (m host-side pointers and coefficients, any m >= 1)
 void launch_lincomb(long long n, int m, const double* const* src, const double* c, double* out, cudaStream_t s);
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb,
                        const double* Fa, const double* Fb, const double* Ea, const double* Eb,
-                       const double* Pa_old, const double* Pb_old, double* out, double* part, cudaStream_t s);
+                       const double* Pa_old, const double* Pb_old, double* out, double* part, cudaStream_t s,
+                       long long nd = 0, const double* x = nullptr, int m = 0, const double* const* ys = nullptr,
+                       double* out_dots = nullptr);  // with m > 0 also out_dots[k] = <x, ys[k]> (length nd)
 void launch_dmax(int ns, const int* bf_off, const int* nfun, int nbf, const double* A, const double* B,
                  const double* C, float* dmax, cudaStream_t s);
 void launch_zero(void* p, size_t bytes, cudaStream_t s);

@@ -1895,13 +1895,16 @@ void launch_fock_half(int n, const double* H, const double* J, double kf, const 
   count_launch();
 }
 
-// out = x - y
-__global__ void diff_kernel(long long n, const double* __restrict__ x, const double* __restrict__ y,
+// out = x - y, then y = x
+__global__ void diff_kernel(long long n, const double* __restrict__ x, double* __restrict__ y,
                             double* __restrict__ out) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    out[i] = x[i] - y[i];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    out[i] = v - y[i];
+    y[i] = v;
+  }
 }
-void launch_diff(long long n, const double* x, const double* y, double* out, cudaStream_t s) {
+void launch_diff_update(long long n, const double* x, double* y, double* out, cudaStream_t s) {
   int g = (int)std::min<long long>((n + 255) / 256, 4096);
   diff_kernel<<<std::max(g, 1), 256, 0, s>>>(n, x, y, out);
   PF_CUDA(cudaGetLastError());
@@ -1949,7 +1952,7 @@ __global__ void dot_many_kernel(long long n, const double* __restrict__ x, const
 // out[j] = sum_b part[j * nb + b] (or the max for the rows flagged in
 // max_rows), one warp per row, lanes in a fixed order
 __global__ void sum_parts_kernel(const double* __restrict__ part, int rows, int nb, unsigned max_rows,
-                                 double* __restrict__ out) {
+                                 double* __restrict__ out, int split = 1 << 30, double* __restrict__ out2 = nullptr) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
   for (int j = w; j < rows; j += blockDim.x >> 5) {
     const bool mx = (max_rows >> j) & 1u;
@@ -1960,7 +1963,10 @@ __global__ void sum_parts_kernel(const double* __restrict__ part, int rows, int 
       const double u = __shfl_xor_sync(0xffffffffu, v, o);
       v = mx ? fmax(v, u) : v + u;
     }
-    if (l == 0) out[j] = v;
+    if (l == 0) {
+      if (j < split) out[j] = v;
+      else out2[j - split] = v;
+    }
   }
 }
 
@@ -2013,8 +2019,18 @@ __global__ void scf_reduce_kernel(long long n, int uhf, const double* __restrict
                                   const double* __restrict__ Pb, const double* __restrict__ Fa,
                                   const double* __restrict__ Fb, const double* __restrict__ Ea,
                                   const double* __restrict__ Eb, const double* __restrict__ Pa_old,
-                                  const double* __restrict__ Pb_old, double* __restrict__ part) {
+                                  const double* __restrict__ Pb_old, double* __restrict__ part, long long nd,
+                                  const double* __restrict__ x, const double* const* ys) {
   __shared__ double sh[32];
+  if (blockIdx.y > 0) {  // the DIIS overlaps <x, ys[y-1]>: partials into row 2 + y
+    const double* y = ys[blockIdx.y - 1];
+    double acc = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += (long long)gridDim.x * blockDim.x)
+      acc += x[i] * y[i];
+    acc = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[(2 + blockIdx.y) * gridDim.x + blockIdx.x] = acc;
+    return;
+  }
   double e = 0.0, dp = 0.0;
   double emx = 0.0;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -2052,10 +2068,12 @@ __global__ void scf_reduce_kernel(long long n, int uhf, const double* __restrict
 }
 void launch_scf_reduce(long long n, int uhf, const double* H, const double* Pa, const double* Pb, const double* Fa,
                        const double* Fb, const double* Ea, const double* Eb, const double* Pa_old,
-                       const double* Pb_old, double* out, double* part, cudaStream_t s) {
-  scf_reduce_kernel<<<RED_BLOCKS, 256, 0, s>>>(n, uhf, H, Pa, Pb, Fa, Fb, Ea, Eb, Pa_old, Pb_old, part);
+                       const double* Pb_old, double* out, double* part, cudaStream_t s, long long nd,
+                       const double* x, int m, const double* const* ys, double* out_dots) {
+  scf_reduce_kernel<<<dim3(RED_BLOCKS, 1 + std::max(m, 0)), 256, 0, s>>>(n, uhf, H, Pa, Pb, Fa, Fb, Ea, Eb, Pa_old,
+                                                                         Pb_old, part, nd, x, ys);
   PF_CUDA(cudaGetLastError());
-  sum_parts_kernel<<<1, 96, 0, s>>>(part, 3, RED_BLOCKS, 2u, out);
+  sum_parts_kernel<<<1, 256, 0, s>>>(part, 3 + std::max(m, 0), RED_BLOCKS, 2u, out, 3, out_dots);
   PF_CUDA(cudaGetLastError());
   count_launches(2);
 }

@@ -530,9 +530,9 @@ void System::run_scf() {
       }
       since_full = 0;
     } else {
-      // dP = P - P_built; J += J[dP], K += K[dP]
+      // dP = P - P_built (and P_built = P); J += J[dP], K += K[dP]
       double* dP[2] = {Err[0], Err[1]};
-      for (int s = 0; s < nsp; ++s) launch_diff((long long)n2, P[s], Pbuilt[s], dP[s], stream);
+      for (int s = 0; s < nsp; ++s) launch_diff_update((long long)n2, P[s], Pbuilt[s], dP[s], stream);
       const double* dPc[2] = {dP[0], dP[1]};
       const double* dPj = dP[0];
       if (uhf) {
@@ -550,8 +550,9 @@ void System::run_scf() {
       }
       since_full++;
     }
-    for (int s = 0; s < nsp; ++s)
-      PF_CUDA(cudaMemcpyAsync(Pbuilt[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+    if (full)
+      for (int s = 0; s < nsp; ++s)
+        PF_CUDA(cudaMemcpyAsync(Pbuilt[s], P[s], n2 * sizeof(double), cudaMemcpyDeviceToDevice, stream));
     for (int s = 0; s < nsp; ++s) {
       if (half) launch_fock_half(nbf, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
       else launch_fock((long long)n2, H, J, uhf ? 1.0 : 0.5, K[s], F[s], stream);
@@ -593,11 +594,11 @@ void System::run_scf() {
       launch_dgemm(nbf, nbf, nbf, false, X, nbf, false, W1, nbf, Eo[s], nbf, 1.0, nullptr, nbf, 0.0, false, false,
                    stream);
     }
+    // energy, errors and (DIIS: F' and the error vector are in their slot)
+    // the overlaps of the new error vector with the stored ones, one launch
     launch_scf_reduce((long long)n2, uhf ? 1 : 0, H, P[0], uhf ? P[1] : nullptr, F[0], uhf ? F[1] : nullptr, Eo[0],
-                      uhf ? Eo[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, red_part, stream);
-    // ---- DIIS bookkeeping: F' and the error vector are in their slot;
-    // overlaps with the stored errors
-    if (ndiis > 0) launch_dot_many((long long)nsp * n2, diis_E[slot], ndiis, ptrs_dev, small + 8, red_part, stream);
+                      uhf ? Eo[1] : nullptr, it > 1 ? Pold[0] : nullptr, uhf ? Pold[1] : nullptr, small, red_part, stream,
+                      (long long)nsp * n2, ndiis > 0 ? diis_E[slot] : nullptr, ndiis, ptrs_dev, small + 8);
     // energy, errors and DIIS overlaps into pinned memory; the copy of P
     // for the next iteration's |dP| runs while the host waits
     const int nred = 8 + std::max(ndiis, 0);
