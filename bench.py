@@ -1,6 +1,6 @@
 #!/usr/bin/env python3
 """Benchmark: seconds per RHF energy + analytic gradient, mixed precision
-(FP32 quartets below a Schwarz bound of 1e-5, incremental dP Fock builds)
+(FP32 quartets below Q_ab Q_cd max|D| = 1e-3, incremental dP Fock builds)
 against the plain FP64 GPU path, on C40H82 / STO-3G (282 basis functions,
 all-anti geometry with sigma = 0.02 A seeded jitter); Fock builds per second.
 
