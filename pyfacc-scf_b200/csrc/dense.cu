@@ -206,11 +206,16 @@ constexpr int ST_ACC = 2, ST_CTL = 8;
 __global__ void tc2g_bounds_kernel(int n, const double* __restrict__ F, double* __restrict__ st) {
   __shared__ double smin[32], smax[32];
   double lo = 1e300, hi = -1e300;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  // one warp per row (coalesced reads of the row), lanes split the columns
+  const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int i = threadIdx.x >> 5; i < n; i += nw) {
+    const double* row = F + (size_t)i * n;
     double r = 0.0;
-    for (int j = 0; j < n; ++j)
-      if (j != i) r += fabs(F[(size_t)i * n + j]);
-    const double d = F[(size_t)i * n + i];
+    for (int j = lane; j < n; j += 32)
+      if (j != i) r += fabs(row[j]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+    const double d = row[i];
     lo = fmin(lo, d - r);
     hi = fmax(hi, d + r);
   }
@@ -257,7 +262,20 @@ __global__ void tc2g_init_kernel(int n, const double* __restrict__ F, double* __
     t1 += __shfl_xor_sync(0xffffffffu, t1, o);
     t2 += __shfl_xor_sync(0xffffffffu, t2, o);
   }
+  // one pair of atomics per block, not per warp (all blocks add to the
+  // same two words)
+  __shared__ double s1[32], s2[32];
+  const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if ((threadIdx.x & 31) == 0) {
+    s1[w] = t1;
+    s2[w] = t2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nw; ++k) {
+      t1 += s1[k];
+      t2 += s2[k];
+    }
     atomicAdd(st + ST_ACC + 0, t1);
     atomicAdd(st + ST_ACC + 1, t2);
   }
