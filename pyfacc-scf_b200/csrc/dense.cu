@@ -1,8 +1,9 @@
 // Dense FP64 work of the single-molecule SCF step on the FP64 tensor cores.
 //
 //  * dgemm_kernel: C = alpha op(A) op(B) + beta Y for row-major matrices,
-//    one block of eight warps per 16 x 16 output tile (2 x 2 tiles of
-//    mma.sync m8n8k4 f64), the k range split eight ways between the warps and
+//    one block of eight warps (symmetric outputs) or four (full ones) per
+//    16 x 16 output tile (2 x 2 tiles of mma.sync m8n8k4 f64), the k range
+//    split between the warps and
 //    the partial tiles added through shared memory; operands read from
 //    L2/L1 (the matrices of one molecule are a few MB at most and stay
 //    resident), 16 loads per lane in flight; optionally only the
@@ -140,11 +141,16 @@ __device__ __forceinline__ void tile_product(const GemmArgs& g, int i0, int j0, 
 // then warp 0 adds the other warps' partial tiles from shared memory.
 // Returns true on warp 0, whose acc holds the tile.
 constexpr int SPLITK = 8;
-template <bool TA, bool TB, bool ASYMA>
+// Full (not symmetric) products have twice the tiles of a symmetric one
+// (324 against 171 at n = 282): with eight warps a block, two blocks per SM
+// (registers) hold 296 of them and the rest form a second wave; with four
+// warps all fit at once.
+constexpr int SPLITK_FULL = 4;
+template <bool TA, bool TB, bool ASYMA, int WARPS = SPLITK>
 __device__ __forceinline__ bool block_tile(const GemmArgs& g, int i0, int j0, double (&acc)[2][2][2]) {
-  __shared__ double part[SPLITK - 1][8][32];
+  __shared__ double part[WARPS - 1][8][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int nchunk = (g.k + 15) >> 4, per = (nchunk + SPLITK - 1) / SPLITK;
+  const int nchunk = (g.k + 15) >> 4, per = (nchunk + WARPS - 1) / WARPS;
   const int kb = min(warp * per * 16, g.k), ke = min((warp + 1) * per * 16, g.k);
   tile_product<TA, TB, ASYMA>(g, i0, j0, kb, ke, acc);
   if (warp > 0) {
@@ -154,20 +160,20 @@ __device__ __forceinline__ bool block_tile(const GemmArgs& g, int i0, int j0, do
   __syncthreads();
   if (warp > 0) return false;
 #pragma unroll
-  for (int w = 0; w < SPLITK - 1; ++w)
+  for (int w = 0; w < WARPS - 1; ++w)
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc[q >> 2][(q >> 1) & 1][q & 1] += part[w][q][lane];
   return true;
 }
 
-template <bool TA, bool TB, bool SYM, bool ASYMA>
-__global__ void __launch_bounds__(32 * SPLITK) dgemm_kernel(const GemmArgs g) {
+template <bool TA, bool TB, bool SYM, bool ASYMA, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) dgemm_kernel(const GemmArgs g) {
   const int ntm = (g.m + 15) >> 4, ntn = (g.n + 15) >> 4;
   int ti, tj;
   if (!tile_of<SYM>(blockIdx.x, ntm, ntn, ti, tj)) return;
   const int i0 = ti << 4, j0 = tj << 4;
   double acc[2][2][2];
-  if (!block_tile<TA, TB, ASYMA>(g, i0, j0, acc)) return;
+  if (!block_tile<TA, TB, ASYMA, WARPS>(g, i0, j0, acc)) return;
   const int lane = threadIdx.x & 31, gr = lane >> 2, tq = lane & 3;
 #pragma unroll
   for (int r = 0; r < 2; ++r)
@@ -189,7 +195,8 @@ template <bool TA, bool TB, bool SYM, bool ASYMA>
 void gemm_launch(const GemmArgs& g, cudaStream_t s) {
   const int ntm = (g.m + 15) / 16, ntn = (g.n + 15) / 16;
   const long long tiles = SYM ? (long long)ntn * (ntn + 1) / 2 : (long long)ntm * ntn;
-  dgemm_kernel<TA, TB, SYM, ASYMA><<<(int)tiles, 32 * SPLITK, 0, s>>>(g);
+  constexpr int W = SYM ? SPLITK : SPLITK_FULL;
+  dgemm_kernel<TA, TB, SYM, ASYMA, W><<<(int)tiles, 32 * W, 0, s>>>(g);
 }
 
 // ---------------------------------------------------------------------------
